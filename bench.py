@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark of the LinRT rendering hot path on B200: Mpaths/s of the wavefront path tracer.
+
+Workload (one step): the seven-material open-box scene set (Cornell-style box open to a Hosek sky, a
+displaced level-6 icosphere of 81,920 triangles carrying each of the seven BSDFs in turn), 512x512
+pixels, 64 samples per pixel, max depth 8, Russian roulette from depth 3 -- 7 x 16.8M = 117.4M camera
+paths per step. Inputs are synthetic and seeded (scenes.py).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lrt|reference]
+
+N > 1 runs as one process per GPU under torch.distributed (NCCL): every rank renders its own replica
+with a disjoint sample range (no data-path collective), the timed region is bracketed by barriers and
+the max over ranks is reported. --impl reference times the reference's own CPU renderer (the unmodified
+sources built in oracle/_ref) on this host's cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ray-tracing_b200"))
+
+import scenes  # noqa: E402
+
+W, H = scenes.CONFIG1["width"], scenes.CONFIG1["height"]
+SPP, DEPTH, RR = scenes.CONFIG1["spp"], scenes.CONFIG1["max_depth"], scenes.CONFIG1["rr_depth"]
+MATERIALS = scenes.MATERIAL_NAMES
+METRIC = "Mpaths/s (path tracer, 7 materials x 512x512 x 64 spp, depth 8, Hosek sky)"
+WORKLOAD = "open_box_7_materials_512x512_64spp_depth8"
+PATHS_PER_STEP = len(MATERIALS) * W * H * SPP
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH, "rr_depth": RR,
+         "materials": MATERIALS, "triangles": 81920 + 12, "paths_per_step": PATHS_PER_STEP,
+         "l2": "flushed (256 MB write) between timed steps", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu_index), "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the unmodified reference sources); used by --impl reference and by the
+# cpu_baseline field
+
+def reference_worlds():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.reference_available():
+        return None, None
+    return oracle, [oracle.RefWorld(scenes.open_box(m)) for m in MATERIALS]
+
+
+def reference_pass(oracle, worlds, spp, sample_offset=0):
+    """one pass over the seven scenes at 512x512 x `spp` on all host cores; returns (paths, seconds)"""
+    secs = 0.0
+    for w in worlds:
+        _, _, s = w.render(scenes.render_params(W, H, spp, DEPTH, RR, sample_offset=sample_offset), 0)
+        secs += s
+    return len(worlds) * W * H * spp, secs
+
+
+def cpu_baseline(budget_s=15.0):
+    oracle, worlds = reference_worlds()
+    if worlds is None:
+        return None
+    spp, paths, secs = 1, 0, 0.0
+    while secs < budget_s:
+        p, s = reference_pass(oracle, worlds, spp, sample_offset=paths)
+        paths += p
+        secs += s
+        if secs < budget_s / 4:
+            spp *= 2
+    return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": oracle.hardware_concurrency(),
+            "kind": "reference",
+            "sample": "%d paths: the 7 scenes at 512x512 with %d..%d spp per pass (same scenes, depth, roulette), "
+                      "32x32 tiles on a thread pool of hardware_concurrency workers, built -O3 without -march"
+                      % (paths, 1, spp)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    oracle, worlds = reference_worlds()
+    if worlds is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference sources not built (oracle/_ref missing)"}))
+        return 0
+    spp = 1
+    for i in range(args.warmup):
+        reference_pass(oracle, worlds, spp, sample_offset=1000 + 8 * i)
+    times, paths = [], 0
+    for i in range(args.steps):
+        p, s = reference_pass(oracle, worlds, spp, sample_offset=8 * i)
+        times.append(s)
+        paths += p
+    total = sum(times)
+    value = paths / total / 1e6
+    cores = oracle.hardware_concurrency()
+    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config({"reference_spp_per_step": spp}),
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": cores, "kind": "reference",
+                             "sample": "each step: the 7 scenes at 512x512 x %d spp (%d paths) on %d threads"
+                                       % (spp, len(worlds) * W * H * spp, cores)},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+
+def run_lrt(args):
+    import torch
+    import lrt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    ctxs = []
+    for m in MATERIALS:
+        c = lrt.Context(local, stream.cuda_stream)
+        c.upload(scenes.open_box(m))
+        ctxs.append(c)
+    out = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    offset = rank * SPP  # replicas render disjoint sample ranges
+    params = scenes.render_params(W, H, SPP, DEPTH, RR, sample_offset=offset)
+
+    # algorithmic work per path (exact traversal counts; untimed pass at 8 spp)
+    for c in ctxs:
+        c.set_option("count_work", 1)
+        c.reset_stats()
+        c.render_dev(scenes.render_params(W, H, 8, DEPTH, RR, sample_offset=offset + 1 << 20), out.data_ptr())
+        c.set_option("count_work", 0)
+    st = [c.stats() for c in ctxs]
+    paths_c = sum(s["paths"] for s in st)
+    ext_rays = sum(s["extension_rays"] for s in st)
+    ext_bytes = sum(8 * s["nodes_visited"] + 48 * s["triangles_tested"] for s in st) + (32 + 16) * ext_rays
+    sh_rays = sum(s["shadow_rays"] for s in st)
+    sh_bytes = sum(8 * s["shadow_nodes_visited"] + 48 * s["shadow_triangles_tested"] for s in st) + 32 * sh_rays
+    work = {"extension_rays_per_path": ext_rays / paths_c, "shadow_rays_per_path": sh_rays / paths_c,
+            "extend_bytes_per_path": ext_bytes / paths_c, "shadow_bytes_per_path": sh_bytes / paths_c,
+            "nodes_per_extension_ray": sum(s["nodes_visited"] for s in st) / max(1, ext_rays),
+            "triangles_per_extension_ray": sum(s["triangles_tested"] for s in st) / max(1, ext_rays)}
+
+    def step():
+        for c in ctxs:
+            c.render_dev(params, out.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    for c in ctxs:
+        c.reset_stats()
+        c.set_option("stage_timing", 1)
+
+    clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0] if world == 1 else local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clock_info = clocks.stop()
+    total_ms = float(sum(step_ms))
+    st = [c.stats() for c in ctxs]
+    launches = int(sum(s["kernel_launches"] for s in st))
+    extend_ms = sum(s["stage_ms"]["extend"] for s in st)
+    extend_launches = sum(s["stage_launches"]["extend"] for s in st)
+    stage_ms = {k: sum(s["stage_ms"][k] for s in st) for k in abi_stage_names()}
+    for c in ctxs:
+        c.set_option("stage_timing", 0)
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # end to end: the public host-buffer call (lrt_render: render + device->host copy of the image)
+    host_img = np.zeros((H, W, 3), dtype=np.float32)
+    e2e_times = []
+    if dist:
+        dist.barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for c in ctxs:
+            c.render(params, host_img)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    paths_total = world * PATHS_PER_STEP * args.steps
+    value = paths_total / (total_ms / 1000.0) / 1e6
+    e2e_value = paths_total / e2e_total / 1e6
+    peak, peak_kind = measured_peaks()
+    timed_paths = PATHS_PER_STEP * args.steps
+    achieved = (work["extend_bytes_per_path"] * timed_paths / 1e9) / (extend_ms / 1000.0) if extend_ms > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "extend_traffic.json")
+    if os.path.exists(tpath) and extend_launches:
+        with open(tpath) as f:
+            tr = json.load(f)
+        # DRAM bytes per extension ray from an ncu capture, scaled to this run's average launch
+        traffic = tr["dram_bytes_per_extension_ray"] * work["extension_rays_per_path"] * timed_paths / extend_launches
+    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes.py)",
+            "config": config({"work_per_path": work, "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}}),
+            "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": len(MATERIALS) * 32,
+                    "d2h_bytes_per_step": len(MATERIALS) * W * H * 3 * 4,
+                    "path": "lrt_render (host output buffer; scene resident after lrt_scene_upload)"},
+            "roofline": {"kernel": "k_extend (closest-hit kd-tree traversal)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic,
+                         "algorithmic_bytes": "per extension ray 8*nodes + 48*triangles + 32 ray + 16 hit",
+                         "avg_launch_ms": extend_ms / max(1, extend_launches)},
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    for c in ctxs:
+        c.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def abi_stage_names():
+    import lrt_abi
+    return lrt_abi.STAGE_NAMES
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lrt", choices=["lrt", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_lrt(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,349 @@
+/*
+ * lrt.h — C ABI of liblrt, the B200 (sm_100a) rendering hot path of the LinRT CPU ray tracer.
+ *
+ * Every entry point returns an int status (LRT_OK = 0, negative LRT_ERR_* on failure); no C++
+ * exception crosses this boundary. lrt_last_error() gives the message of the last failure on a
+ * context. All device work of a context is ordered on the CUDA stream given to lrt_create(). A
+ * context is not thread-safe: use one per host thread, or serialise calls.
+ *
+ * Entry points that take host pointers copy them (host <-> device copies happen inside the call);
+ * the *_dev variants take device pointers that the caller owns.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   scene build + upload        src/core/scene.h:21-34, src/core/hittable_list.h:10-34,
+ *                               src/geometry/triangle_mesh.h:14-28,148-157, src/accelerator/sah_kdtree.h:35-57
+ *   lrt_trace                   scene::hit src/core/scene.h:36-38 -> hittable_list::hit src/core/hittable_list.h:19-34
+ *                               -> triangle_mesh::hit src/geometry/triangle_mesh.h:30-99 -> sah_kdtree::intersect
+ *                               src/accelerator/sah_kdtree.h:62-121; rectangle::hit src/geometry/rectangle.h:18-55;
+ *                               sphere::hit src/geometry/sphere.h:21-49
+ *   lrt_bsdf_evaluate           bsdf::sample/eval/pdf src/material/bsdf.h:55-89 and the eight BSDFs in src/material/
+ *   lrt_sky_eval                scene::eval_environment src/core/scene.h:61-70 -> env_emitter::eval
+ *                               src/emitter/env_emitter.h:71-88
+ *   lrt_render                  the tile loop of src/main.cpp:103-147 around path_integrator::radiance
+ *                               src/integrator/path/path_integrator.h:18-170
+ *   lrt_photon_trace            photon_gather::run src/integrator/photonmapper/photon_gather.h:15-61 with
+ *                               photon_tracer::trace_particle src/integrator/photonmapper/photon_tracer.h:23-96
+ *   lrt_photon_map_build        photon_map::build src/integrator/photonmapper/photon_map.h:26-33
+ *   lrt_photon_knn              photon_map::nearest/search src/integrator/photonmapper/photon_map.h:117-165
+ *   lrt_photon_irradiance       photon_map::estimate_irradiance src/integrator/photonmapper/photon_map.h:38-70
+ *   lrt_rough_transmittance_slice  rough_transmittance ctor src/material/func/rough_transmittance.h:15-24,67-185
+ *   lrt_fresnel_diffuse_reflectance fresnel_diffuse_reflectance src/material/func/fresnel.h:128-133
+ */
+#ifndef LRT_H
+#define LRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define LRT_OK                    0
+#define LRT_ERR_INVALID_ARGUMENT (-1)
+#define LRT_ERR_CUDA             (-2)
+#define LRT_ERR_OUT_OF_MEMORY    (-3)
+#define LRT_ERR_IO               (-4)
+#define LRT_ERR_RANGE            (-5)
+#define LRT_ERR_NO_SCENE         (-6)
+#define LRT_ERR_QUEUE_OVERFLOW   (-7)
+#define LRT_ERR_TIMEOUT          (-8)
+#define LRT_ERR_NO_DEVICE        (-9)
+#define LRT_ERR_DEVICE_CHECK     (-10)
+
+/* ---- BSDF flags (src/material/bsdf.h:18-28) ---- */
+#define LRT_BSDF_NONE        0u
+#define LRT_BSDF_DIFFUSE     (1u << 0)
+#define LRT_BSDF_SPECULAR    (1u << 1)
+#define LRT_BSDF_REFLECTIVE  (1u << 2)
+#define LRT_BSDF_TRANSPARENT (1u << 3)
+#define LRT_BSDF_GLOSSY      (1u << 4)
+#define LRT_BSDF_METALLIC    (1u << 5)
+#define LRT_BSDF_DIELECTRIC  (1u << 6)
+#define LRT_BSDF_REFRACTIVE  (1u << 7)
+
+/* measure (src/material/bsdf.h:9-16) */
+#define LRT_MEASURE_SOLID_ANGLE 1
+#define LRT_MEASURE_DISCRETE    5
+
+/* transport mode (src/material/bsdf.h:31-34) */
+#define LRT_MODE_RADIANCE   0
+#define LRT_MODE_IMPORTANCE 1
+
+/* material types: one per BSDF class in src/material/ */
+#define LRT_DIFFUSE          0  /* diffuse_bsdf.h */
+#define LRT_ROUGH_CONDUCTOR  1  /* rough_conductor_bsdf.h (alpha <= 0: smooth mirror) */
+#define LRT_DIELECTRIC       2  /* dielectric_bsdf.h */
+#define LRT_ROUGH_DIELECTRIC 3  /* rough_dielectric_bsdf.h */
+#define LRT_PLASTIC          4  /* plastic_bsdf.h */
+#define LRT_ROUGH_PLASTIC    5  /* rough_plastic_bsdf.h */
+#define LRT_COATING          6  /* coating_bsdf.h */
+#define LRT_ROUGH_COATING    7  /* rough_coating_bsdf.h */
+
+/* rough-transmittance table length in cos^(1/4) theta (ggx.dat theta samples) */
+#define LRT_TRANS_SAMPLES 100
+
+/*
+ * Material description. Field meaning follows the reference constructors:
+ *   diffuse:          diffuse_reflectance = albedo
+ *   rough_conductor:  eta, k, alpha, specular_reflectance
+ *   dielectric:       int_ior, ext_ior, specular_reflectance, specular_transmittance
+ *   rough_dielectric: int_ior, ext_ior, alpha, specular_reflectance, specular_transmittance
+ *   plastic:          int_ior, ext_ior, specular_reflectance, diffuse_reflectance, nonlinear
+ *   rough_plastic:    int_ior, ext_ior, alpha, specular_reflectance, diffuse_reflectance, nonlinear,
+ *                     trans_table = rough_transmittance(int/ext, alpha) sliced 1-D table,
+ *                     trans_internal_diffuse = rough_transmittance(ext/int, alpha).eval_diffuse()
+ *   coating:          int_ior, ext_ior, nested, specular_reflectance, sigma_a, thickness
+ *   rough_coating:    int_ior, ext_ior, alpha, nested, specular_reflectance, sigma_a, thickness,
+ *                     trans_table = rough_transmittance(int/ext, alpha) sliced 1-D table
+ * The tables come from lrt_rough_transmittance_slice() (or any caller holding the same data).
+ * A coating's nested material must have a smaller index than the coating and must not itself be
+ * a coating (the reference allows deeper nesting; the device path supports one level).
+ */
+typedef struct lrt_material_desc {
+    int32_t type;
+    int32_t nested;
+    int32_t nonlinear;
+    float int_ior;
+    float ext_ior;
+    float alpha;
+    float thickness;
+    float diffuse_reflectance[3];
+    float specular_reflectance[3];
+    float specular_transmittance[3];
+    float eta[3];
+    float k[3];
+    float sigma_a[3];
+    float trans_table[LRT_TRANS_SAMPLES];
+    float trans_internal_diffuse;
+} lrt_material_desc;
+
+/* objects of the linear object list (src/core/hittable_list.h); order is significant */
+#define LRT_OBJECT_MESH      0  /* triangle_mesh: one SAH kd-tree per mesh */
+#define LRT_OBJECT_RECTANGLE 1  /* rectangle: never carries a BSDF (rectangle.h:50) */
+#define LRT_OBJECT_SPHERE    2  /* sphere */
+
+typedef struct lrt_object_desc {
+    int32_t kind;
+    int32_t material;          /* index into materials, -1 = none */
+    uint32_t n_vertices;
+    uint32_t n_indices;        /* 3 per triangle */
+    const float* positions;    /* n_vertices * 3 */
+    const uint32_t* indices;   /* n_indices */
+    const float* corner_normals; /* n_indices * 3: one normal per triangle corner */
+    float corner[3];           /* rectangle */
+    float edge_u[3];
+    float edge_v[3];
+    float center[3];           /* sphere */
+    float radius;
+} lrt_object_desc;
+
+#define LRT_EMITTER_AREA 0  /* area_emitter over an object (area_emitter.h) */
+#define LRT_EMITTER_ENV  1  /* Hosek sky (env_emitter.h) */
+
+/*
+ * Emitter description. For LRT_EMITTER_ENV, hosek_config/hosek_radiance are the RGB model state
+ * (ArHosekSkyModelState configs[0..2] and radiances[0..2]) cooked by
+ * arhosek_rgb_skymodelstate_alloc_init(turbidity, albedo, asin(normalize(sun_direction).y)).
+ */
+typedef struct lrt_emitter_desc {
+    int32_t kind;
+    int32_t object;            /* area: index of the emitting object */
+    float radiance[3];         /* area */
+    float sun_direction[3];    /* env: normalised inside, as env_emitter.h:17 */
+    float turbidity;
+    float albedo;
+    float scale;
+    double hosek_config[3][9];
+    double hosek_radiance[3];
+} lrt_emitter_desc;
+
+/* pinhole camera (src/core/camera.h:20-44); aperture must be 0 */
+typedef struct lrt_camera_desc {
+    float origin[3];
+    float look_at[3];
+    float up[3];
+    float fov_degrees;
+    float aspect_ratio;
+} lrt_camera_desc;
+
+typedef struct lrt_scene_desc {
+    uint32_t n_objects;
+    const lrt_object_desc* objects;
+    uint32_t n_materials;
+    const lrt_material_desc* materials;
+    uint32_t n_emitters;
+    const lrt_emitter_desc* emitters;
+    lrt_camera_desc camera;
+} lrt_scene_desc;
+
+/* ---- queries ---- */
+
+/* one ray: origin, direction, t_min, t_max */
+typedef struct lrt_ray {
+    float origin[3];
+    float direction[3];
+    float t_min;
+    float t_max;
+} lrt_ray;
+
+typedef struct lrt_hit {
+    float t;
+    int32_t object;      /* -1 on miss */
+    int32_t prim;        /* triangle index inside the mesh; -1 for analytic shapes */
+    int32_t front_face;
+    float p[3];
+    float normal[3];     /* shading normal, facing the incoming ray (hit_record::normal) */
+} lrt_hit;
+
+typedef struct lrt_bsdf_query {
+    float wi[3];
+    float wo[3];
+    float u[2];
+    float lobe_sample;
+    int32_t front_face;
+    int32_t mode;          /* LRT_MODE_* */
+    uint32_t type_mask;
+    int32_t component;
+    int32_t measure;       /* for eval/pdf: LRT_MEASURE_* */
+} lrt_bsdf_query;
+
+typedef struct lrt_bsdf_result {
+    float sample_weight[3];
+    float sample_wo[3];
+    float sample_pdf;
+    float sample_eta;
+    uint32_t sampled_type;
+    int32_t sampled_component;
+    float eval[3];
+    float pdf;
+} lrt_bsdf_result;
+
+/* photon record (photon_map.h:16-22) */
+typedef struct lrt_photon {
+    float position[3];
+    float direction[3];
+    float normal[3];
+    float power[3];
+    uint32_t depth;
+} lrt_photon;
+
+#define LRT_GATHER_SURFACE 0
+#define LRT_GATHER_CAUSTIC 1
+
+typedef struct lrt_render_params {
+    uint32_t width;
+    uint32_t height;
+    uint32_t spp;
+    int32_t max_depth;       /* path_integrator.h:173 */
+    int32_t rr_depth;        /* path_integrator.h:19 */
+    uint32_t sample_offset;  /* first sample index (replicas render disjoint sample ranges) */
+    uint32_t row_begin;      /* render rows [row_begin, row_end); 0,0 = all rows */
+    uint32_t row_end;
+} lrt_render_params;
+
+/* per-stage device time of the wavefront renderer, accumulated while stage timing is on */
+#define LRT_STAGE_RAYGEN  0
+#define LRT_STAGE_EXTEND  1
+#define LRT_STAGE_SORT    2
+#define LRT_STAGE_SHADE   3
+#define LRT_STAGE_SHADOW  4
+#define LRT_STAGE_ACCUM   5
+#define LRT_STAGE_COUNT   6
+
+typedef struct lrt_render_stats {
+    uint64_t paths;              /* camera paths traced */
+    uint64_t extension_rays;     /* closest-hit rays traced */
+    uint64_t shadow_rays;        /* NEE shadow rays traced */
+    uint64_t nodes_visited;      /* kd nodes visited by extension rays (option count_work) */
+    uint64_t triangles_tested;   /* triangle tests of extension rays (option count_work) */
+    uint64_t shadow_nodes_visited;     /* the same for shadow rays */
+    uint64_t shadow_triangles_tested;
+    uint64_t shading_events;
+    uint64_t kernel_launches;
+    float stage_ms[LRT_STAGE_COUNT];
+    uint32_t stage_launches[LRT_STAGE_COUNT];
+} lrt_render_stats;
+
+/* ---- context ---- */
+typedef struct lrt_context lrt_context;
+
+int lrt_create(int device, void* cuda_stream, lrt_context** out);
+int lrt_destroy(lrt_context* ctx);
+const char* lrt_last_error(const lrt_context* ctx);
+const char* lrt_status_string(int status);
+
+/* host-side utilities (no device work) */
+int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha,
+                                  float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
+float lrt_fresnel_diffuse_reflectance(float eta);
+
+/* Host-only SAH kd-tree build over n primitive bounds (3 floats each in bmin/bmax): the tree
+ * sah_kdtree::build makes (src/accelerator/sah_kdtree.h:35-57,175-347), packed depth-first into
+ * 8-byte nodes (2 uint32 words each: interior = split bits, right<<2|axis; leaf = first, count<<2|3)
+ * with leaf references in leaf order. Returns LRT_ERR_RANGE (and the needed sizes) when the output
+ * arrays are too small. */
+int lrt_kdtree_build(const float* bmin, const float* bmax, uint32_t n, uint32_t* nodes_out,
+                     uint32_t max_nodes, uint32_t* refs_out, uint32_t max_refs, uint32_t* n_nodes,
+                     uint32_t* n_refs, uint32_t* depth);
+
+/* scene: builds the per-mesh SAH kd-trees on the host and uploads everything to the device */
+int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc);
+/* bytes the last upload copied host->device */
+uint64_t lrt_scene_device_bytes(const lrt_context* ctx);
+/* kd-tree of one mesh object: node count, leaf-list length, maximum depth */
+int lrt_mesh_tree_info(const lrt_context* ctx, uint32_t object, uint32_t* nodes, uint32_t* refs,
+                       uint32_t* depth);
+
+/* closest-hit queries (parity) */
+int lrt_trace(lrt_context* ctx, const lrt_ray* rays, uint32_t n, lrt_hit* hits);
+int lrt_trace_dev(lrt_context* ctx, const lrt_ray* rays_dev, uint32_t n, lrt_hit* hits_dev);
+
+/* BSDF sample + eval + pdf of material `material` for each query (parity) */
+int lrt_bsdf_evaluate(lrt_context* ctx, int32_t material, const lrt_bsdf_query* q, uint32_t n,
+                      lrt_bsdf_result* out);
+/* environment radiance for directions (n * 3 floats in, n * 3 out) */
+int lrt_sky_eval(lrt_context* ctx, const float* directions, uint32_t n, float* rgb);
+/* sampler values for (pixel, sample) pairs: n_dims floats per pair (parity; src/core/sampler.h:12-27) */
+int lrt_sampler_values(lrt_context* ctx, const uint32_t* pixel_sample, uint32_t n, uint32_t n_dims,
+                       float* values);
+/* camera rays of (pixel, sample) pairs exactly as src/main.cpp:121-132 forms them (parity) */
+int lrt_camera_rays(lrt_context* ctx, uint32_t width, uint32_t height, const uint32_t* pixel_sample,
+                    uint32_t n, lrt_ray* rays);
+/* scene::sample_emitter_direction at (point, u2) and scene::pdf_emitter_direction at (point, dir)
+ * (src/core/scene.h:73-108). sample_out: 16 floats per query = ok, direction[3], point[3], 0,0,0,
+ * pdf, distance, radiance[3], emitter index. */
+int lrt_emitter_query(lrt_context* ctx, const float* points, const float* u2, const float* dirs,
+                      uint32_t n, float* sample_out, float* pdf_out);
+
+/* path-traced image: rgb is width*height*3 floats, row-major from row 0 (as src/main.cpp) */
+int lrt_render(lrt_context* ctx, const lrt_render_params* params, float* rgb);
+int lrt_render_dev(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev);
+/* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
+int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
+int lrt_render_stats_reset(lrt_context* ctx);
+int lrt_set_option(lrt_context* ctx, const char* name, int64_t value);
+
+/* photons: particles [0, ...) traced in index order until `requested` photons are stored */
+int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t max_depth,
+                     int32_t rr_depth, lrt_photon* photons_out, uint32_t* n_out, uint64_t* shot_out);
+/* photons of particles [first, first+count), with per-particle photon counts (parity) */
+int lrt_photon_trace_particles(lrt_context* ctx, int32_t kind, uint32_t first, uint32_t count,
+                               int32_t max_depth, int32_t rr_depth, uint32_t max_per_particle,
+                               lrt_photon* photons_out, uint32_t* counts_out);
+int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photons, uint32_t n,
+                         float scale);
+/* k nearest photons within squared radius r2 (photon_map.h:117-165). Indices refer to the array
+ * given to lrt_photon_map_build; each query's results are sorted by (d2, index) descending as the
+ * reference pops its max-heap. */
+int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t n, float r2,
+                   uint32_t k, uint32_t* idx_out, float* d2_out, uint32_t* count_out);
+int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, const float* normals,
+                          uint32_t n, float radius, int32_t max_depth, uint32_t k, float* rgb_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LRT_H */

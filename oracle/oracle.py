@@ -1,0 +1,229 @@
+"""TEST INFRASTRUCTURE: ctypes loader of the reference oracle (oracle/_ref/liblrt_ref.so, the
+unmodified reference compiled by oracle/Makefile) and of the C restatement (oracle/build/liblrt_oracle.so).
+
+Only tests/, the smoke check and the CPU-baseline leg of bench.py use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "ray-tracing_b200"))
+import lrt_abi as abi  # noqa: E402
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(ORACLE_DIR, "_ref")
+REF_LIB = os.path.join(REF_DIR, "liblrt_ref.so")
+GGX_PATH = os.path.join(REF_DIR, "third_party", "data", "ggx.dat")
+RESTATEMENT_LIB = os.path.join(ORACLE_DIR, "build", "liblrt_oracle.so")
+
+_ref = None
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_LIB) and os.path.exists(GGX_PATH)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not reference_available():
+            raise FileNotFoundError("reference oracle not built: run `make -C oracle ref` (needs the reference sources)")
+        lib = C.CDLL(REF_LIB)
+        vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int32, C.c_float
+        P = C.POINTER
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_world_create.restype = vp
+        lib.ref_world_create.argtypes = [P(abi.SceneDesc), C.c_char_p]
+        lib.ref_world_destroy.argtypes = [vp]
+        lib.ref_trace.restype = C.c_int64
+        lib.ref_trace.argtypes = [vp, P(abi.Ray), u32, P(abi.Hit), P(C.c_uint64)]
+        lib.ref_bsdf_query.argtypes = [vp, i32, P(abi.BsdfQuery), u32, P(abi.BsdfResult)]
+        lib.ref_bsdf_flags.restype = u32
+        lib.ref_bsdf_flags.argtypes = [vp, i32]
+        lib.ref_sky_eval.argtypes = [vp, P(f32), u32, P(f32)]
+        lib.ref_emitter_sample.argtypes = [vp, P(f32), P(f32), u32, P(f32)]
+        lib.ref_emitter_pdf.argtypes = [vp, P(f32), P(f32), u32, P(f32)]
+        lib.ref_sampler_values.argtypes = [P(u32), u32, u32, P(f32)]
+        lib.ref_camera_rays.argtypes = [vp, u32, u32, P(u32), u32, P(abi.Ray)]
+        lib.ref_render.restype = C.c_double
+        lib.ref_render.argtypes = [vp, P(abi.RenderParams), u32, P(f32), P(f32)]
+        lib.ref_trace_particles.argtypes = [vp, i32, u32, u32, i32, i32, u32, P(abi.Photon), P(u32)]
+        lib.ref_photon_gather.restype = u32
+        lib.ref_photon_gather.argtypes = [vp, i32, u32, i32, i32, P(abi.Photon), P(C.c_uint64), P(C.c_double)]
+        lib.ref_photon_map_create.restype = vp
+        lib.ref_photon_map_create.argtypes = [P(abi.Photon), u32, f32]
+        lib.ref_photon_map_destroy.argtypes = [vp]
+        lib.ref_photon_map_knn.argtypes = [vp, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
+        lib.ref_photon_map_irradiance.argtypes = [vp, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
+        lib.ref_rough_transmittance.restype = i32
+        lib.ref_rough_transmittance.argtypes = [C.c_char_p, f32, f32, P(f32), P(f32)]
+        lib.ref_rough_transmittance_eval.restype = f32
+        lib.ref_rough_transmittance_eval.argtypes = [C.c_char_p, f32, f32, f32]
+        lib.ref_fresnel_diffuse_reflectance.restype = f32
+        lib.ref_fresnel_diffuse_reflectance.argtypes = [f32]
+        lib.ref_hosek_state.argtypes = [P(f32), f32, f32, P(C.c_double), P(C.c_double)]
+        lib.ref_hardware_concurrency.restype = u32
+        _ref = lib
+    return _ref
+
+
+def _p(a, t=C.c_float):
+    return abi.ptr(a, t)
+
+
+class RefWorld:
+    """Reference objects built from the same scene description as the GPU library."""
+
+    def __init__(self, scene):
+        self.holder = abi.SceneHolder(scene)
+        lib = ref_lib()
+        self.handle = lib.ref_world_create(C.byref(self.holder.desc), REF_DIR.encode())
+        if not self.handle:
+            raise RuntimeError("reference scene construction failed: %s" % lib.ref_last_error().decode())
+
+    def close(self):
+        if self.handle:
+            ref_lib().ref_world_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
+        hits = np.zeros(len(rays), dtype=abi.HIT_DTYPE)
+        tests = C.c_uint64(0)
+        mism = ref_lib().ref_trace(self.handle, _p(rays, abi.Ray), len(rays), _p(hits, abi.Hit), C.byref(tests))
+        assert mism == 0, "harness object loop disagrees with scene::hit on %d rays" % mism
+        return hits, tests.value
+
+    def bsdf(self, material: int, queries: np.ndarray):
+        queries = np.ascontiguousarray(queries, dtype=abi.BSDF_QUERY_DTYPE)
+        out = np.zeros(len(queries), dtype=abi.BSDF_RESULT_DTYPE)
+        ref_lib().ref_bsdf_query(self.handle, material, _p(queries, abi.BsdfQuery), len(queries),
+                                 _p(out, abi.BsdfResult))
+        return out
+
+    def bsdf_flags(self, material: int) -> int:
+        return ref_lib().ref_bsdf_flags(self.handle, material)
+
+    def sky(self, dirs: np.ndarray):
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32)
+        out = np.zeros((len(dirs), 3), dtype=np.float32)
+        ref_lib().ref_sky_eval(self.handle, _p(dirs), len(dirs), _p(out))
+        return out
+
+    def emitter_sample(self, points, u2):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        u2 = np.ascontiguousarray(u2, dtype=np.float32)
+        out = np.zeros((len(points), 16), dtype=np.float32)
+        ref_lib().ref_emitter_sample(self.handle, _p(points), _p(u2), len(points), _p(out))
+        return out
+
+    def emitter_pdf(self, points, dirs):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32)
+        out = np.zeros(len(points), dtype=np.float32)
+        ref_lib().ref_emitter_pdf(self.handle, _p(points), _p(dirs), len(points), _p(out))
+        return out
+
+    def camera_rays(self, width, height, pixel_sample):
+        ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
+        rays = np.zeros(len(ps), dtype=abi.RAY_DTYPE)
+        ref_lib().ref_camera_rays(self.handle, width, height, _p(ps, C.c_uint32), len(ps), _p(rays, abi.Ray))
+        return rays
+
+    def render(self, params: abi.RenderParams, threads: int = 0, want_sq: bool = False):
+        img = np.zeros((params.height, params.width, 3), dtype=np.float32)
+        sq = np.zeros_like(img) if want_sq else None
+        secs = ref_lib().ref_render(self.handle, C.byref(params), threads, _p(img),
+                                    _p(sq) if sq is not None else None)
+        return img, sq, secs
+
+    def trace_particles(self, kind, first, count, max_depth, rr_depth, max_per=64):
+        photons = np.zeros(count * max_per, dtype=abi.PHOTON_DTYPE)
+        counts = np.zeros(count, dtype=np.uint32)
+        ref_lib().ref_trace_particles(self.handle, kind, first, count, max_depth, rr_depth, max_per,
+                                      _p(photons, abi.Photon), _p(counts, C.c_uint32))
+        return photons.reshape(count, max_per), counts
+
+    def photon_gather(self, kind, requested, max_depth, rr_depth):
+        photons = np.zeros(requested, dtype=abi.PHOTON_DTYPE)
+        shot = C.c_uint64(0)
+        secs = C.c_double(0)
+        n = ref_lib().ref_photon_gather(self.handle, kind, requested, max_depth, rr_depth,
+                                        _p(photons, abi.Photon), C.byref(shot), C.byref(secs))
+        return photons[:n], shot.value, secs.value
+
+
+class RefPhotonMap:
+    def __init__(self, photons: np.ndarray, scale: float = 1.0):
+        self.photons = np.ascontiguousarray(photons, dtype=abi.PHOTON_DTYPE)
+        self.handle = ref_lib().ref_photon_map_create(_p(self.photons, abi.Photon), len(self.photons), scale)
+
+    def knn(self, points, r2, k):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        n = len(points)
+        idx = np.full((n, k), 0xFFFFFFFF, dtype=np.uint32)
+        d2 = np.zeros((n, k), dtype=np.float32)
+        cnt = np.zeros(n, dtype=np.uint32)
+        ref_lib().ref_photon_map_knn(self.handle, _p(points), n, r2, k, _p(idx, C.c_uint32), _p(d2),
+                                     _p(cnt, C.c_uint32))
+        return idx, d2, cnt
+
+    def irradiance(self, points, normals, radius, max_depth, k):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        normals = np.ascontiguousarray(normals, dtype=np.float32)
+        out = np.zeros((len(points), 3), dtype=np.float32)
+        ref_lib().ref_photon_map_irradiance(self.handle, _p(points), _p(normals), len(points), radius, max_depth,
+                                            k, _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            if self.handle:
+                ref_lib().ref_photon_map_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def sampler_values(pixel_sample, n_dims):
+    ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
+    out = np.zeros((len(ps), n_dims), dtype=np.float32)
+    ref_lib().ref_sampler_values(_p(ps, C.c_uint32), len(ps), n_dims, _p(out))
+    return out
+
+
+def rough_transmittance(eta, alpha, ggx_path=GGX_PATH):
+    table = np.zeros(abi.TRANS_SAMPLES, dtype=np.float32)
+    diffuse = C.c_float(0)
+    n = ref_lib().ref_rough_transmittance(ggx_path.encode(), eta, alpha, _p(table), C.byref(diffuse))
+    if n < 0:
+        raise RuntimeError(ref_lib().ref_last_error().decode())
+    assert n == abi.TRANS_SAMPLES
+    return table, np.float32(diffuse.value)
+
+
+def fresnel_diffuse_reflectance(eta):
+    return np.float32(ref_lib().ref_fresnel_diffuse_reflectance(eta))
+
+
+def hosek_state(sun_direction, turbidity, albedo):
+    sd = np.asarray(sun_direction, dtype=np.float32)
+    cfg = np.zeros(27, dtype=np.float64)
+    rad = np.zeros(3, dtype=np.float64)
+    ref_lib().ref_hosek_state(_p(sd), turbidity, albedo, _p(cfg, C.c_double), _p(rad, C.c_double))
+    return cfg.reshape(3, 9), rad
+
+
+def hardware_concurrency() -> int:
+    return int(ref_lib().ref_hardware_concurrency())

@@ -1,0 +1,915 @@
+// lrt_api.cu — liblrt: context, scene upload, parity kernels and the wavefront path tracer, behind
+// the C ABI of include/lrt.h. sm_100a only; no CPU fallback: every entry point that computes runs its
+// CUDA kernels or returns an error.
+//
+// Wavefront path tracer (one render = a sequence of waves; a wave = all samples of a pixel range):
+//   raygen      camera rays of every (pixel, sample) slot of the wave        main.cpp:121-132
+//   extend      closest hit of every active path + append to the shading      path_integrator.h:31
+//               queue of its material type (warp-aggregated match/ballot)
+//   shade       miss/emission + MIS, NEE light sample + BSDF eval/pdf (emits  path_integrator.h:32-166
+//               a shadow ray), BSDF sample, Russian roulette; survivors are
+//               compacted into the next queue
+//   shadow      closest-emitter query of each shadow ray; unoccluded rays add path_integrator.h:113-125
+//               their precomputed NEE contribution
+//   accumulate  per-pixel sum over the wave's samples in sample order         main.cpp:133-136
+// Every stage reads its queue length on the device, so the grid sizes are fixed (SM count x resident
+// blocks, grid-stride loops) and no host round trip happens inside a wave.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lrt_context.cuh"
+#include "lrt_scene.cuh"
+
+using namespace lrt;
+
+namespace {
+
+template <typename T>
+cudaError_t upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t s, uint64_t& bytes) {
+    const size_t n = std::max<size_t>(1, v.size()) * sizeof(T);
+    cudaError_t e = buf.ensure(n);
+    if(e != cudaSuccess) return e;
+    if(!v.empty()) {
+        e = cudaMemcpyAsync(buf.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+        bytes += v.size() * sizeof(T);
+    }
+    return e;
+}
+
+// ================================ parity kernels ================================
+
+__global__ void k_trace(DeviceScene s, const lrt_ray* rays, uint32_t n, lrt_hit* hits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const lrt_ray in = rays[i];
+    const Ray r{load3(in.origin), load3(in.direction)};
+    HitInfo h;
+    TraceCount cnt{0, 0};
+    lrt_hit out;
+    memset(&out, 0, sizeof(out));
+    out.object = -1;
+    out.prim = -1;
+    if(scene_hit<false>(s, r, in.t_min, in.t_max, h, cnt)) {
+        out.t = h.t;
+        out.object = h.object;
+        out.prim = h.prim;
+        out.front_face = h.front_face ? 1 : 0;
+        store3(out.p, h.p);
+        store3(out.normal, h.normal);
+    }
+    hits[i] = out;
+}
+
+__global__ void k_bsdf(DeviceScene s, int32_t mid, const lrt_bsdf_query* q, uint32_t n, lrt_bsdf_result* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const lrt_bsdf_query in = q[i];
+    const BsdfCtx c{in.mode, in.type_mask, in.component, in.lobe_sample};
+    BRec r{};
+    r.wi = load3(in.wi);
+    r.wo = mk(0.0f);
+    r.front_face = in.front_face != 0;
+    const f3 w = bsdf_sample(s.materials, s.tables, mid, c, r, in.u[0], in.u[1]);
+    lrt_bsdf_result o;
+    store3(o.sample_weight, w);
+    store3(o.sample_wo, r.wo);
+    o.sample_pdf = r.pdf;
+    o.sample_eta = r.eta;
+    o.sampled_type = r.sampled_type;
+    o.sampled_component = r.sampled_component;
+    BRec e{};
+    e.wi = load3(in.wi);
+    e.wo = load3(in.wo);
+    e.front_face = in.front_face != 0;
+    e.eta = 1.0f;
+    const int meas = in.measure == LRT_MEASURE_DISCRETE ? kDiscrete : kSolidAngle;
+    store3(o.eval, bsdf_eval(s.materials, s.tables, mid, c, e, meas));
+    o.pdf = bsdf_pdf(s.materials, s.tables, mid, c, e, meas);
+    out[i] = o;
+}
+
+__global__ void k_sky(DeviceScene s, const float* dirs, uint32_t n, float* rgb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    store3(rgb + 3ull * i, eval_environment(s, load3(dirs + 3ull * i)));
+}
+
+__global__ void k_sampler(const uint32_t* table, const uint32_t* ps, uint32_t n, uint32_t dims, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const uint32_t(*t)[32] = reinterpret_cast<const uint32_t(*)[32]>(table);
+    Sampler smp = sampler_start(ps[2 * i], ps[2 * i + 1]);
+    for(uint32_t d = 0; d < dims; ++d) out[static_cast<size_t>(i) * dims + d] = sampler_next_1d(t, smp);
+}
+
+// emitter sampling parity: same record layout as the reference harness (16 floats)
+__global__ void k_emitter(DeviceScene s, const float* points, const float* u2, const float* dirs, uint32_t n, float* out,
+                          float* pdf_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const f3 p = load3(points + 3ull * i);
+    DirectSample ds{};
+    ds.distance = kInf;
+    const bool ok = sample_emitter_direction(s, p, u2[2 * i], u2[2 * i + 1], ds);
+    float* o = out + 16ull * i;
+    o[0] = ok ? 1.0f : 0.0f;
+    store3(o + 1, ds.direction);
+    store3(o + 4, ds.point);
+    o[7] = o[8] = o[9] = 0.0f;
+    o[10] = ds.pdf;
+    o[11] = ds.distance;
+    store3(o + 12, ds.radiance);
+    o[15] = ok ? static_cast<float>(ds.emitter) : -1.0f;
+    pdf_out[i] = pdf_emitter_direction(s, p, load3(dirs + 3ull * i));
+}
+
+__global__ void k_camera(DeviceScene s, uint32_t width, uint32_t height, const uint32_t* ps, uint32_t n, lrt_ray* rays) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const uint32_t pixel = ps[2 * i];
+    Sampler smp = sampler_start(pixel, ps[2 * i + 1]);
+    const F2 off = sampler_next_2d(sobol_table(s), smp);
+    const float u = (static_cast<float>(pixel % width) + off.x) / static_cast<float>(width - 1);
+    const float v = (static_cast<float>(pixel / width) + off.y) / static_cast<float>(height - 1);
+    const Ray r = camera_ray(s.cam, u, v);
+    lrt_ray out;
+    store3(out.origin, r.o);
+    store3(out.direction, r.d);
+    out.t_min = 0.001f;
+    out.t_max = kInf;
+    rays[i] = out;
+}
+
+// ================================ wavefront path tracer ================================
+
+struct WaveArgs {
+    DeviceScene s;
+    float4* o;       // ray origin
+    float4* d;       // ray direction
+    float4* tp;      // throughput rgb, eta
+    float4* L;       // radiance rgb
+    float2* misc;    // solid-angle pdf, have_pdf (0/1)
+    uint2* id;       // pixel index, sample index
+    float4* hit_p;   // hit point, object index bits
+    float4* hit_n;   // shading normal, front_face
+    uint32_t* q0;    // active queue (even bounces read q0)
+    uint32_t* q1;
+    uint32_t* keyed; // kKeys segments of `capacity`
+    float4* sh_o;    // shadow origin, tmax
+    float4* sh_d;    // shadow direction, light index bits
+    float4* sh_c;    // contribution rgb, path id bits
+    BounceCounters* counters;
+    unsigned long long* work;  // [0] nodes, [1] triangles, [2] shading events, [3] extension rays, [4] shadow rays
+    float* sum;      // per-pixel running sums (3 floats per pixel of the wave)
+    uint32_t capacity;
+    uint32_t width, height;
+    uint32_t pixel_begin;    // first pixel of the wave (row-major over the image)
+    uint32_t n_pixels;
+    uint32_t sample_begin;   // first sample index of the wave
+    uint32_t n_samples;      // samples per pixel in this wave
+    int32_t max_depth, rr_depth;
+};
+
+__global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
+    const uint32_t n = a.n_pixels * a.n_samples;
+    if(blockIdx.x == 0 && threadIdx.x == 0) a.counters[0].active = n;
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const uint32_t pix = a.pixel_begin + slot / a.n_samples;
+        const uint32_t sample = a.sample_begin + slot % a.n_samples;
+        Sampler smp = sampler_start(pix, sample);
+        const F2 off = sampler_next_2d(sobol_table(a.s), smp);
+        const float u = (static_cast<float>(pix % a.width) + off.x) / static_cast<float>(a.width - 1);
+        const float v = (static_cast<float>(pix / a.width) + off.y) / static_cast<float>(a.height - 1);
+        const Ray r = camera_ray(a.s.cam, u, v);
+        a.o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+        a.d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
+        a.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        a.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        a.misc[slot] = make_float2(0.0f, 0.0f);
+        a.id[slot] = make_uint2(pix, sample);
+        a.q0[slot] = slot;
+    }
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
+    const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
+    BounceCounters& bc = a.counters[depth];
+    const uint32_t n = bc.active;
+    TraceCount cnt{0, 0};
+    uint32_t rays = 0;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t pid = queue[i];
+        const float4 o = a.o[pid];
+        const float4 d = a.d[pid];
+        HitInfo h;
+        const bool hit = scene_hit<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, kInf, h, cnt);
+        ++rays;
+        int key = 0;
+        if(hit) {
+            const int32_t mat = a.s.objects[h.object].material;
+            key = mat < 0 ? 1 : 2 + a.s.materials[mat].type;
+            a.hit_p[pid] = make_float4(h.p.x, h.p.y, h.p.z, __int_as_float(h.object));
+            a.hit_n[pid] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.front_face ? 1.0f : 0.0f);
+        }
+        const uint32_t slot = warp_append_keyed(bc.key_count, key);
+        a.keyed[static_cast<size_t>(key) * a.capacity + slot] = pid;
+    }
+    if(kCount) {
+        add_count(&a.work[0], cnt.nodes);
+        add_count(&a.work[1], cnt.tris);
+        add_count(&a.work[3], rays);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
+    __shared__ uint32_t prefix[kKeys + 1];
+    BounceCounters& bc = a.counters[depth];
+    if(threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for(int k = 0; k < kKeys; ++k) {
+            prefix[k] = acc;
+            acc += bc.key_count[k];
+        }
+        prefix[kKeys] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = prefix[kKeys];
+    uint32_t* next = (depth & 1) ? a.q0 : a.q1;
+    BounceCounters& nc = a.counters[depth + 1];
+    const DeviceScene& s = a.s;
+    uint32_t shading = 0;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int key = 0;
+        while(key + 1 < kKeys && prefix[key + 1] <= i) ++key;
+        const uint32_t pid = a.keyed[static_cast<size_t>(key) * a.capacity + (i - prefix[key])];
+        const float4 o4 = a.o[pid], d4 = a.d[pid], tp4 = a.tp[pid], L4 = a.L[pid];
+        const float2 misc = a.misc[pid];
+        const f3 ro{o4.x, o4.y, o4.z};
+        const f3 rd{d4.x, d4.y, d4.z};
+        f3 throughput{tp4.x, tp4.y, tp4.z};
+        float eta = tp4.w;
+        f3 result{L4.x, L4.y, L4.z};
+        const bool have_pdf = misc.y != 0.0f;
+        const float sa_pdf = misc.x;
+
+        if(key == 0) {  // miss: environment + MIS (path_integrator.h:32-45); rec.p of a miss is (0,0,0)
+            const f3 Le = eval_environment(s, rd);
+            if(!have_pdf) {
+                result += throughput * Le;
+            } else {
+                const float light_pdf = pdf_emitter_direction(s, mk(0.0f), rd);
+                const float w = power_heuristic(sa_pdf, light_pdf);
+                result += throughput * w * Le;
+            }
+            a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
+            continue;
+        }
+        const float4 hp = a.hit_p[pid], hn = a.hit_n[pid];
+        const f3 p{hp.x, hp.y, hp.z};
+        const f3 normal{hn.x, hn.y, hn.z};
+        const bool front_face = hn.w != 0.0f;
+        const ObjRec& obj = s.objects[__float_as_int(hp.w)];
+        if(obj.emitter >= 0 && front_face) {  // path_integrator.h:47-59
+            const f3 outgoing = -normalize(rd);
+            const f3 Le = area_emitted(s.emitters[obj.emitter], normal, outgoing);
+            if(!is_zero(Le)) {
+                if(!have_pdf) {
+                    result += throughput * Le;
+                } else {
+                    const float light_pdf = pdf_emitter_direction(s, ro, rd);
+                    const float w = power_heuristic(sa_pdf, light_pdf);
+                    result += throughput * w * Le;
+                }
+            }
+        }
+        if(key == 1) {
+            a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
+            continue;
+        }
+        ++shading;
+        const int32_t mid = obj.material;
+        const Onb basis = onb_from_normal(normal);
+        BRec rec{};
+        rec.wi = to_local(basis, -normalize(rd));
+        rec.wo = mk(0.0f);
+        rec.front_face = front_face;
+        rec.eta = 1.0f;
+        const uint2 ident = a.id[pid];
+        Sampler smp = sampler_start(ident.x, ident.y);
+        smp.dimension = 2u + 6u * static_cast<uint32_t>(depth);
+        // path_integrator.h:80-83: light (2), lobe (1), bsdf (2), roulette (1)
+        const F2 light_uv = sampler_next_2d(sobol_table(s), smp);
+        BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+        ctx.lobe_sample = sampler_next_1d(sobol_table(s), smp);
+        const F2 bsdf_uv = sampler_next_2d(sobol_table(s), smp);
+        const float rr_u = sampler_next_1d(sobol_table(s), smp);
+
+        const MatRec& mat = s.materials[mid];
+        if((mat.flags & (kDiffuse | kGlossy)) != 0) {  // NEE (path_integrator.h:86-128)
+            DirectSample light{};
+            light.distance = kInf;
+            if(sample_emitter_direction(s, p, light_uv.x, light_uv.y, light)) {
+                const f3 shadow_origin = p + normal * 1e-4f;
+                f3 shadow_dir = light.direction;
+                float tmax = kInf;
+                bool have_target = true;
+                if(!isinf(light.distance)) {
+                    const f3 to_light = light.point - shadow_origin;
+                    const float dist = length(to_light);
+                    if(dist < 1e-6f) {
+                        have_target = false;
+                    } else {
+                        shadow_dir = to_light / dist;
+                        tmax = dist * (1.0f - 1e-4f);
+                    }
+                }
+                if(have_target) {
+                    rec.wo = to_local(basis, shadow_dir);
+                    const f3 f_cos = bsdf_eval(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                    if(!is_zero(f_cos)) {
+                        const float bsdf_pdf_v = bsdf_pdf(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                        const float light_pdf = pdf_emitter_direction(s, p, shadow_dir);
+                        if(light_pdf > 0.0f) {
+                            const float w = power_heuristic(light_pdf, bsdf_pdf_v);
+                            const f3 contrib = throughput * f_cos * light.radiance * (w / light_pdf);
+                            const uint32_t si = warp_append(&bc.shadow);
+                            a.sh_o[si] = make_float4(shadow_origin.x, shadow_origin.y, shadow_origin.z, tmax);
+                            a.sh_d[si] = make_float4(shadow_dir.x, shadow_dir.y, shadow_dir.z, __int_as_float(light.emitter));
+                            a.sh_c[si] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(pid));
+                        }
+                    }
+                }
+            }
+        }
+        if(depth == a.max_depth - 1) {
+            a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
+            continue;
+        }
+        const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, rec, bsdf_uv.x, bsdf_uv.y);
+        bool alive = !is_zero(weight);
+        f3 new_dir = rd;
+        if(alive) {
+            new_dir = to_world(basis, rec.wo);
+            throughput *= weight;
+            eta *= rec.eta;
+            if(depth >= a.rr_depth) {
+                const float q = smin(max3(throughput) * eta * eta, 0.95f);
+                if(rr_u >= q) {
+                    alive = false;
+                } else {
+                    throughput /= q;
+                }
+            }
+        }
+        a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
+        if(alive) {
+            const bool have = measure_of(rec.sampled_type) == kSolidAngle && rec.pdf > 0.0f;
+            a.o[pid] = make_float4(p.x, p.y, p.z, 0.0f);
+            a.d[pid] = make_float4(new_dir.x, new_dir.y, new_dir.z, 0.0f);
+            a.tp[pid] = make_float4(throughput.x, throughput.y, throughput.z, eta);
+            a.misc[pid] = make_float2(rec.pdf, have ? 1.0f : 0.0f);
+            const uint32_t ni = warp_append(&nc.active);
+            next[ni] = pid;
+        }
+    }
+    if(a.work) add_count(&a.work[2], shading);
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs a, int depth) {
+    const uint32_t n = a.counters[depth].shadow;
+    TraceCount cnt{0, 0};
+    uint32_t rays = 0;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = a.sh_o[i], d = a.sh_d[i], c = a.sh_c[i];
+        const int32_t light = __float_as_int(d.w);
+        const int32_t e = scene_hit_emitter<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, o.w, cnt);
+        ++rays;
+        const bool blocked = e != -2 && e != light;
+        if(!blocked) {
+            const uint32_t pid = __float_as_uint(c.w);
+            float4 L = a.L[pid];
+            L.x += c.x;
+            L.y += c.y;
+            L.z += c.z;
+            a.L[pid] = L;
+        }
+    }
+    if(kCount) {
+        add_count(&a.work[5], cnt.nodes);
+        add_count(&a.work[6], cnt.tris);
+        add_count(&a.work[4], rays);
+    }
+}
+
+// sum the wave's samples per pixel in sample order; the last wave of a pixel divides by spp
+__global__ void __launch_bounds__(kBlock) k_accumulate(WaveArgs a, float* rgb, uint32_t spp, int first_wave,
+                                                       int last_wave) {
+    for(uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x; pl < a.n_pixels; pl += gridDim.x * blockDim.x) {
+        f3 acc = first_wave ? mk(0.0f) : load3(a.sum + 3ull * pl);
+        for(uint32_t s = 0; s < a.n_samples; ++s) {
+            const float4 L = a.L[static_cast<size_t>(pl) * a.n_samples + s];
+            acc += f3{L.x, L.y, L.z};
+        }
+        if(last_wave) {
+            store3(rgb + 3ull * (a.pixel_begin + pl), acc / static_cast<float>(spp));
+        } else {
+            store3(a.sum + 3ull * pl, acc);
+        }
+    }
+}
+
+int ensure_wave(lrt_context* ctx, uint32_t cap) {
+    WaveState& w = ctx->wave;
+    if(w.capacity >= cap) return LRT_OK;
+    const size_t c = cap;
+    LRT_CUDA(ctx, w.o.ensure(c * 16));
+    LRT_CUDA(ctx, w.d.ensure(c * 16));
+    LRT_CUDA(ctx, w.tp.ensure(c * 16));
+    LRT_CUDA(ctx, w.L.ensure(c * 16));
+    LRT_CUDA(ctx, w.misc.ensure(c * 8));
+    LRT_CUDA(ctx, w.id.ensure(c * 8));
+    LRT_CUDA(ctx, w.hit_p.ensure(c * 16));
+    LRT_CUDA(ctx, w.hit_n.ensure(c * 16));
+    LRT_CUDA(ctx, w.q0.ensure(c * 4));
+    LRT_CUDA(ctx, w.q1.ensure(c * 4));
+    LRT_CUDA(ctx, w.keyed.ensure(c * 4 * kKeys));
+    LRT_CUDA(ctx, w.sh_o.ensure(c * 16));
+    LRT_CUDA(ctx, w.sh_d.ensure(c * 16));
+    LRT_CUDA(ctx, w.sh_c.ensure(c * 16));
+    LRT_CUDA(ctx, w.sum.ensure(c * 12));
+    w.capacity = cap;
+    return LRT_OK;
+}
+
+void record_stage(lrt_context* ctx, int stage, bool begin) {
+    if(!ctx->stage_timing) return;
+    cudaEvent_t ev;
+    if(cudaEventCreate(&ev) != cudaSuccess) return;
+    cudaEventRecord(ev, ctx->stream);
+    ctx->events.push_back(ev);
+    ctx->event_stage.push_back(begin ? stage : -1 - stage);
+}
+
+void collect_stage_times(lrt_context* ctx) {
+    for(size_t i = 0; i + 1 < ctx->events.size(); i += 2) {
+        float ms = 0.0f;
+        if(cudaEventElapsedTime(&ms, ctx->events[i], ctx->events[i + 1]) == cudaSuccess) {
+            const int stage = ctx->event_stage[i];
+            if(stage >= 0 && stage < LRT_STAGE_COUNT) {
+                ctx->stats.stage_ms[stage] += ms;
+                ctx->stats.stage_launches[stage] += 1;
+            }
+        }
+    }
+    for(cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+    ctx->events.clear();
+    ctx->event_stage.clear();
+}
+
+int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(!p || p->width < 2 || p->height < 2 || p->spp == 0 || p->max_depth < 1 || p->max_depth > 1024) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT,
+                    "render parameters out of range (width, height >= 2; spp >= 1; 1 <= max_depth <= 1024)");
+    }
+    const uint32_t row_begin = p->row_end > p->row_begin ? p->row_begin : 0u;
+    const uint32_t row_end = p->row_end > p->row_begin ? std::min(p->row_end, p->height) : p->height;
+    if(row_begin >= row_end) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "empty row range");
+    if(static_cast<uint64_t>(p->width) * p->height > 0x3fffffffull) return fail(ctx, LRT_ERR_RANGE, "image too large");
+    const uint32_t cap = ctx->wave_capacity;
+    int st = ensure_wave(ctx, cap);
+    if(st != LRT_OK) return st;
+    const size_t counters_bytes = sizeof(BounceCounters) * (p->max_depth + 1);
+    LRT_CUDA(ctx, ctx->counters.ensure(counters_bytes));
+    WaveState& w = ctx->wave;
+    WaveArgs a{};
+    a.s = ctx->ds;
+    a.o = w.o.as<float4>();
+    a.d = w.d.as<float4>();
+    a.tp = w.tp.as<float4>();
+    a.L = w.L.as<float4>();
+    a.misc = w.misc.as<float2>();
+    a.id = w.id.as<uint2>();
+    a.hit_p = w.hit_p.as<float4>();
+    a.hit_n = w.hit_n.as<float4>();
+    a.q0 = w.q0.as<uint32_t>();
+    a.q1 = w.q1.as<uint32_t>();
+    a.keyed = w.keyed.as<uint32_t>();
+    a.sh_o = w.sh_o.as<float4>();
+    a.sh_d = w.sh_d.as<float4>();
+    a.sh_c = w.sh_c.as<float4>();
+    a.counters = ctx->counters.as<BounceCounters>();
+    a.sum = w.sum.as<float>();
+    a.capacity = cap;
+    a.width = p->width;
+    a.height = p->height;
+    a.max_depth = p->max_depth;
+    a.rr_depth = p->rr_depth;
+    unsigned long long* work = nullptr;
+    if(ctx->count_work) {
+        LRT_CUDA(ctx, ctx->scratch_b.ensure(64));
+        work = ctx->scratch_b.as<unsigned long long>();
+        LRT_CUDA(ctx, cudaMemsetAsync(work, 0, 64, ctx->stream));
+    }
+    a.work = work;
+
+    const bool cnt = ctx->count_work;
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
+    const int g_extend = grid_for(ctx, cnt ? (const void*)k_extend<true> : (const void*)k_extend<false>, kBlock);
+    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const int g_shadow = grid_for(ctx, cnt ? (const void*)k_shadow<true> : (const void*)k_shadow<false>, kBlock);
+    const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
+
+    // wave plan: a pixel range x a sample range, at most `cap` slots
+    const uint32_t spp = p->spp;
+    const uint32_t samples_per_wave = std::min(spp, cap);
+    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
+    const uint32_t pix0 = row_begin * p->width;
+    const uint32_t pix1 = row_end * p->width;
+    uint64_t launches = 0;
+    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
+        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
+        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
+            const uint32_t ns = std::min(samples_per_wave, spp - sb);
+            a.pixel_begin = pb;
+            a.n_pixels = np;
+            a.sample_begin = p->sample_offset + sb;
+            a.n_samples = ns;
+            LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
+            record_stage(ctx, LRT_STAGE_RAYGEN, true);
+            k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
+            record_stage(ctx, LRT_STAGE_RAYGEN, false);
+            launches += 1;
+            for(int depth = 0; depth < p->max_depth; ++depth) {
+                record_stage(ctx, LRT_STAGE_EXTEND, true);
+                if(cnt) {
+                    k_extend<true><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                } else {
+                    k_extend<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                }
+                record_stage(ctx, LRT_STAGE_EXTEND, false);
+                record_stage(ctx, LRT_STAGE_SHADE, true);
+                k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+                record_stage(ctx, LRT_STAGE_SHADE, false);
+                record_stage(ctx, LRT_STAGE_SHADOW, true);
+                if(cnt) {
+                    k_shadow<true><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                } else {
+                    k_shadow<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                }
+                record_stage(ctx, LRT_STAGE_SHADOW, false);
+                launches += 3;
+            }
+            record_stage(ctx, LRT_STAGE_ACCUM, true);
+            k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
+            record_stage(ctx, LRT_STAGE_ACCUM, false);
+            launches += 1;
+            LRT_CUDA(ctx, cudaGetLastError());
+        }
+    }
+    ctx->stats.paths += static_cast<uint64_t>(pix1 - pix0) * spp;
+    ctx->stats.kernel_launches += launches;
+    if(ctx->stage_timing || cnt) {
+        LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        collect_stage_times(ctx);
+        if(cnt) {
+            unsigned long long h[7];
+            LRT_CUDA(ctx, cudaMemcpy(h, work, sizeof(h), cudaMemcpyDeviceToHost));
+            ctx->stats.nodes_visited += h[0];
+            ctx->stats.triangles_tested += h[1];
+            ctx->stats.shading_events += h[2];
+            ctx->stats.extension_rays += h[3];
+            ctx->stats.shadow_rays += h[4];
+            ctx->stats.shadow_nodes_visited += h[5];
+            ctx->stats.shadow_triangles_tested += h[6];
+        }
+    }
+    return LRT_OK;
+}
+
+}  // namespace
+
+// ======================================= C ABI =======================================
+
+extern "C" {
+
+const char* lrt_status_string(int status) {
+    switch(status) {
+    case LRT_OK: return "LRT_OK";
+    case LRT_ERR_INVALID_ARGUMENT: return "LRT_ERR_INVALID_ARGUMENT";
+    case LRT_ERR_CUDA: return "LRT_ERR_CUDA";
+    case LRT_ERR_OUT_OF_MEMORY: return "LRT_ERR_OUT_OF_MEMORY";
+    case LRT_ERR_IO: return "LRT_ERR_IO";
+    case LRT_ERR_RANGE: return "LRT_ERR_RANGE";
+    case LRT_ERR_NO_SCENE: return "LRT_ERR_NO_SCENE";
+    case LRT_ERR_QUEUE_OVERFLOW: return "LRT_ERR_QUEUE_OVERFLOW";
+    case LRT_ERR_TIMEOUT: return "LRT_ERR_TIMEOUT";
+    case LRT_ERR_NO_DEVICE: return "LRT_ERR_NO_DEVICE";
+    case LRT_ERR_DEVICE_CHECK: return "LRT_ERR_DEVICE_CHECK";
+    default: return "LRT_ERR_UNKNOWN";
+    }
+}
+
+int lrt_create(int device, void* cuda_stream, lrt_context** out) {
+    if(!out) return LRT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if(cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return LRT_ERR_NO_DEVICE;
+    }
+    if(device < 0 || device >= count) return LRT_ERR_INVALID_ARGUMENT;
+    auto ctx = std::make_unique<lrt_context>();
+    ctx->device = device;
+    if(cudaSetDevice(device) != cudaSuccess) return LRT_ERR_CUDA;
+    cudaDeviceProp prop;
+    if(cudaGetDeviceProperties(&prop, device) != cudaSuccess) return LRT_ERR_CUDA;
+    if(prop.major < 10) return LRT_ERR_NO_DEVICE;  // built for sm_100a only
+    ctx->sm_count = prop.multiProcessorCount;
+    if(cuda_stream) {
+        ctx->stream = static_cast<cudaStream_t>(cuda_stream);
+    } else {
+        if(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return LRT_ERR_CUDA;
+        ctx->own_stream = true;
+    }
+    uint32_t table[kSobolDims][32];
+    sobol_direction_table(table);
+    if(ctx->sobol.ensure(sizeof(table)) != cudaSuccess) return LRT_ERR_OUT_OF_MEMORY;
+    if(cudaMemcpy(ctx->sobol.ptr, table, sizeof(table), cudaMemcpyHostToDevice) != cudaSuccess) return LRT_ERR_CUDA;
+    *out = ctx.release();
+    return LRT_OK;
+}
+
+int lrt_destroy(lrt_context* ctx) {
+    if(!ctx) return LRT_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for(cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+    if(ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return LRT_OK;
+}
+
+const char* lrt_last_error(const lrt_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha, float* table_out, float* diffuse_out) {
+    if(!ggx_path || !table_out || !diffuse_out) return LRT_ERR_INVALID_ARGUMENT;
+    std::string err;
+    return rough_transmittance_slice(ggx_path, eta, alpha, table_out, diffuse_out, err);
+}
+
+float lrt_fresnel_diffuse_reflectance(float eta) { return fresnel_diffuse_reflectance(eta); }
+
+int lrt_kdtree_build(const float* bmin, const float* bmax, uint32_t n, uint32_t* nodes_out, uint32_t max_nodes,
+                     uint32_t* refs_out, uint32_t max_refs, uint32_t* n_nodes, uint32_t* n_refs, uint32_t* depth) {
+    if((n && (!bmin || !bmax)) || !n_nodes || !n_refs) return LRT_ERR_INVALID_ARGUMENT;
+    PackedTree t;
+    build_kdtree(bmin, bmax, n, t);
+    *n_nodes = static_cast<uint32_t>(t.nodes.size());
+    *n_refs = static_cast<uint32_t>(t.refs.size());
+    if(depth) *depth = t.depth;
+    if(t.nodes.size() > max_nodes || t.refs.size() > max_refs || !nodes_out || (!refs_out && !t.refs.empty())) {
+        return LRT_ERR_RANGE;
+    }
+    for(size_t i = 0; i < t.nodes.size(); ++i) {
+        nodes_out[2 * i] = t.nodes[i].x;
+        nodes_out[2 * i + 1] = t.nodes[i].y;
+    }
+    std::copy(t.refs.begin(), t.refs.end(), refs_out);
+    return LRT_OK;
+}
+
+int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    ctx->has_scene = false;
+    std::string err;
+    const int st = build_host_scene(desc, ctx->host, err);
+    if(st != LRT_OK) return fail(ctx, st, "%s", err.c_str());
+    HostScene& h = ctx->host;
+    uint64_t bytes = 0;
+    cudaStream_t s = ctx->stream;
+    LRT_CUDA(ctx, upload(ctx->nodes, h.nodes, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->tris, h.tris, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->ref_prim, h.ref_prim, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->normals, h.normals, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->objects, h.objects, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->materials, h.materials, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->tables, h.tables, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->emitters, h.emitters, s, bytes));
+    // emission CDF (floats) followed by its emitter indices
+    std::vector<float> emission(h.emission_cdf);
+    emission.resize(2 * h.emission_cdf.size() + 1);
+    for(size_t i = 0; i < h.emission_index.size(); ++i) {
+        memcpy(&emission[h.emission_cdf.size() + i], &h.emission_index[i], 4);
+    }
+    LRT_CUDA(ctx, upload(ctx->emission, emission, s, bytes));
+    LRT_CUDA(ctx, cudaStreamSynchronize(s));
+    DeviceScene& ds = ctx->ds;
+    ds.nodes = ctx->nodes.as<uint2>();
+    ds.tris = ctx->tris.as<float4>();
+    ds.ref_prim = ctx->ref_prim.as<uint32_t>();
+    ds.normals = ctx->normals.as<float4>();
+    ds.objects = ctx->objects.as<ObjRec>();
+    ds.materials = ctx->materials.as<MatRec>();
+    ds.tables = ctx->tables.as<float>();
+    ds.emitters = ctx->emitters.as<EmitRec>();
+    ds.sobol = ctx->sobol.as<uint32_t>();
+    ds.emission_cdf = ctx->emission.as<float>();
+    ds.emission_index = reinterpret_cast<const int32_t*>(ctx->emission.as<float>() + h.emission_cdf.size());
+    ds.n_objects = static_cast<int32_t>(h.objects.size());
+    ds.n_materials = static_cast<int32_t>(h.materials.size());
+    ds.n_emitters = static_cast<int32_t>(h.emitters.size());
+    ds.n_infinite = h.n_infinite;
+    ds.n_emission = static_cast<int32_t>(h.emission_cdf.size());
+    ds.emission_power = h.emission_power;
+    ds.cam = h.cam;
+    ctx->scene_bytes = bytes;
+    ctx->has_scene = true;
+    return LRT_OK;
+}
+
+uint64_t lrt_scene_device_bytes(const lrt_context* ctx) { return ctx ? ctx->scene_bytes : 0; }
+
+int lrt_mesh_tree_info(const lrt_context* ctx, uint32_t object, uint32_t* nodes, uint32_t* refs, uint32_t* depth) {
+    if(!ctx || !ctx->has_scene || object >= ctx->host.mesh_info.size()) return LRT_ERR_INVALID_ARGUMENT;
+    const MeshTreeInfo& m = ctx->host.mesh_info[object];
+    if(nodes) *nodes = m.nodes;
+    if(refs) *refs = m.refs;
+    if(depth) *depth = m.depth;
+    return LRT_OK;
+}
+
+int lrt_trace_dev(lrt_context* ctx, const lrt_ray* rays_dev, uint32_t n, lrt_hit* hits_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n == 0) return LRT_OK;
+    if(!rays_dev || !hits_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    k_trace<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, rays_dev, n, hits_dev);
+    LRT_CUDA(ctx, cudaGetLastError());
+    return LRT_OK;
+}
+
+int lrt_trace(lrt_context* ctx, const lrt_ray* rays, uint32_t n, lrt_hit* hits) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(n == 0) return LRT_OK;
+    if(!rays || !hits) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(sizeof(lrt_ray) * static_cast<size_t>(n) + sizeof(lrt_hit) * static_cast<size_t>(n)));
+    lrt_ray* dr = ctx->scratch_a.as<lrt_ray>();
+    lrt_hit* dh = reinterpret_cast<lrt_hit*>(dr + n);
+    LRT_CUDA(ctx, cudaMemcpyAsync(dr, rays, sizeof(lrt_ray) * n, cudaMemcpyHostToDevice, ctx->stream));
+    const int st = lrt_trace_dev(ctx, dr, n, dh);
+    if(st != LRT_OK) return st;
+    LRT_CUDA(ctx, cudaMemcpyAsync(hits, dh, sizeof(lrt_hit) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_bsdf_evaluate(lrt_context* ctx, int32_t material, const lrt_bsdf_query* q, uint32_t n, lrt_bsdf_result* out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(material < 0 || material >= ctx->ds.n_materials) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "material out of range");
+    if(n == 0) return LRT_OK;
+    if(!q || !out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t qb = sizeof(lrt_bsdf_query) * n, rb = sizeof(lrt_bsdf_result) * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(qb + rb));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, q, qb, cudaMemcpyHostToDevice, ctx->stream));
+    k_bsdf<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, material, reinterpret_cast<lrt_bsdf_query*>(base), n,
+                                                      reinterpret_cast<lrt_bsdf_result*>(base + qb));
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(out, base + qb, rb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_sky_eval(lrt_context* ctx, const float* directions, uint32_t n, float* rgb) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n == 0) return LRT_OK;
+    if(!directions || !rgb) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t b = sizeof(float) * 3 * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(2 * b));
+    float* base = ctx->scratch_a.as<float>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, directions, b, cudaMemcpyHostToDevice, ctx->stream));
+    k_sky<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, base, n, base + 3ull * n);
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(rgb, base + 3ull * n, b, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_sampler_values(lrt_context* ctx, const uint32_t* pixel_sample, uint32_t n, uint32_t n_dims, float* values) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(n == 0 || n_dims == 0) return LRT_OK;
+    if(!pixel_sample || !values) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t ib = sizeof(uint32_t) * 2 * n, ob = sizeof(float) * static_cast<size_t>(n) * n_dims;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(ib + ob));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, pixel_sample, ib, cudaMemcpyHostToDevice, ctx->stream));
+    k_sampler<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->sobol.as<uint32_t>(), reinterpret_cast<uint32_t*>(base), n,
+                                                         n_dims, reinterpret_cast<float*>(base + ib));
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(values, base + ib, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_emitter_query(lrt_context* ctx, const float* points, const float* u2, const float* dirs, uint32_t n,
+                      float* sample_out, float* pdf_out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n == 0) return LRT_OK;
+    if(!points || !u2 || !dirs || !sample_out || !pdf_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t pb = 12ull * n, ub = 8ull * n, ob = 64ull * n, fb = 4ull * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(2 * pb + ub + ob + fb));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, points, pb, cudaMemcpyHostToDevice, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(base + pb, dirs, pb, cudaMemcpyHostToDevice, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(base + 2 * pb, u2, ub, cudaMemcpyHostToDevice, ctx->stream));
+    float* o = reinterpret_cast<float*>(base + 2 * pb + ub);
+    float* pdf = reinterpret_cast<float*>(base + 2 * pb + ub + ob);
+    k_emitter<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, reinterpret_cast<float*>(base),
+                                                         reinterpret_cast<float*>(base + 2 * pb),
+                                                         reinterpret_cast<float*>(base + pb), n, o, pdf);
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(sample_out, o, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(pdf_out, pdf, fb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_camera_rays(lrt_context* ctx, uint32_t width, uint32_t height, const uint32_t* pixel_sample, uint32_t n,
+                    lrt_ray* rays) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n == 0) return LRT_OK;
+    if(!pixel_sample || !rays || width < 2 || height < 2) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "bad arguments");
+    const size_t ib = 8ull * n, ob = sizeof(lrt_ray) * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(ib + ob));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, pixel_sample, ib, cudaMemcpyHostToDevice, ctx->stream));
+    k_camera<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, width, height, reinterpret_cast<uint32_t*>(base), n,
+                                                        reinterpret_cast<lrt_ray*>(base + ib));
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(rays, base + ib, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_render_dev(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null output");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    return render_impl(ctx, params, rgb_dev);
+}
+
+int lrt_render(lrt_context* ctx, const lrt_render_params* params, float* rgb) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!rgb || !params) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(params->width) * params->height;
+    LRT_CUDA(ctx, ctx->out_rgb.ensure(bytes));
+    LRT_CUDA(ctx, cudaMemsetAsync(ctx->out_rgb.ptr, 0, bytes, ctx->stream));
+    const int st = render_impl(ctx, params, ctx->out_rgb.as<float>());
+    if(st != LRT_OK) return st;
+    LRT_CUDA(ctx, cudaMemcpyAsync(rgb, ctx->out_rgb.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out) {
+    if(!ctx || !out) return LRT_ERR_INVALID_ARGUMENT;
+    *out = ctx->stats;
+    return LRT_OK;
+}
+
+int lrt_render_stats_reset(lrt_context* ctx) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    ctx->stats = lrt_render_stats{};
+    return LRT_OK;
+}
+
+int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
+    if(!ctx || !name) return LRT_ERR_INVALID_ARGUMENT;
+    if(strcmp(name, "stage_timing") == 0) {
+        ctx->stage_timing = value != 0;
+    } else if(strcmp(name, "count_work") == 0) {
+        ctx->count_work = value != 0;
+    } else if(strcmp(name, "photon_tree_device") == 0) {
+        ctx->photon_tree_device = value != 0;
+    } else if(strcmp(name, "wave_capacity") == 0) {
+        if(value < 1024 || value > (1ll << 26)) return fail(ctx, LRT_ERR_RANGE, "wave_capacity must be in [1024, 2^26]");
+        ctx->wave_capacity = static_cast<uint32_t>(value);
+    } else {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "unknown option %s", name);
+    }
+    return LRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// lrt_context.cuh — the context object behind the C ABI and small device/launch helpers shared by
+// the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "lrt.h"
+#include "lrt_host.h"
+#include "lrt_math.cuh"
+#include "lrt_types.h"
+
+namespace lrt {
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if(ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if(n <= bytes) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if(e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+constexpr int kKeys = 10;  // shading keys: 0 miss, 1 hit without BSDF, 2 + material type
+constexpr int kBlock = 128;
+constexpr int kMaxPhotonMaps = 4;
+constexpr uint32_t kMaxKnn = 128;
+
+// per-bounce device counters of one wave
+struct BounceCounters {
+    uint32_t active;  // paths entering this bounce
+    uint32_t shadow;  // shadow rays emitted by this bounce
+    uint32_t key_count[kKeys];
+    uint32_t pad[4];
+};
+
+struct WaveState {
+    uint32_t capacity = 0;
+    DevBuf o, d, tp, L, misc, id, hit_p, hit_n, q0, q1, keyed, sh_o, sh_d, sh_c, sum;
+};
+
+// photon map in tree order: positions carry the caller's index in w (bits)
+struct PhotonNode {
+    int32_t a;      // interior: left child; leaf: first photon
+    int32_t b;      // interior: right child; leaf: photon count
+    int32_t axis;   // 0..2, or 3 for a leaf
+    float split;
+};
+
+struct PhotonMap {
+    uint32_t n = 0;
+    float scale = 1.0f;
+    DevBuf pos;     // float4 x, y, z, caller index
+    DevBuf dir;     // float4 direction, depth (as float)
+    DevBuf nrm;     // float4 normal
+    DevBuf pow;     // float4 power
+    DevBuf nodes;   // PhotonNode
+    uint32_t n_nodes = 0;
+    uint32_t depth = 0;
+};
+
+}  // namespace lrt
+
+struct lrt_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 0;
+    std::string error;
+    // scene
+    bool has_scene = false;
+    lrt::HostScene host;
+    lrt::DeviceScene ds{};
+    lrt::DevBuf nodes, tris, ref_prim, normals, objects, materials, tables, emitters, emission, sobol;
+    uint64_t scene_bytes = 0;
+    // render
+    lrt::WaveState wave;
+    lrt::DevBuf out_rgb, scratch_a, scratch_b, counters;
+    lrt_render_stats stats{};
+    bool stage_timing = false;
+    bool count_work = false;
+    uint32_t wave_capacity = 1u << 21;
+    std::vector<cudaEvent_t> events;
+    std::vector<int> event_stage;
+    // photons
+    bool photon_tree_device = false;  // false: reference-identical tree built on the host
+    lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
+    lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg;
+};
+
+namespace lrt {
+
+inline int fail(lrt_context* ctx, int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if(ctx) ctx->error = buf;
+    return code;
+}
+
+#define LRT_CUDA(ctx, call)                                                                                   \
+    do {                                                                                                      \
+        cudaError_t e_ = (call);                                                                              \
+        if(e_ != cudaSuccess) {                                                                               \
+            return ::lrt::fail(ctx, e_ == cudaErrorMemoryAllocation ? LRT_ERR_OUT_OF_MEMORY : LRT_ERR_CUDA,   \
+                               "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);          \
+        }                                                                                                     \
+    } while(0)
+
+inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+inline int grid_for(lrt_context* ctx, const void* kernel, int block) {
+    int per_sm = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    return ctx->sm_count * per_sm;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ const uint32_t (*sobol_table(const DeviceScene& s))[32] {
+    return reinterpret_cast<const uint32_t(*)[32]>(s.sobol);
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// warp-aggregated append: one atomic per warp (ballot + popc), slot per lane
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter) {
+    const uint32_t mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+// warp-aggregated append into one of several queues: lanes with equal keys share one atomic
+__device__ __forceinline__ uint32_t warp_append_keyed(uint32_t* counters, int key) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counters + key, static_cast<uint32_t>(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane_id()) - 1u));
+}
+
+// warp reduce then one atomic per warp
+__device__ __forceinline__ void add_count(unsigned long long* dst, uint32_t v) {
+    const uint32_t mask = __activemask();
+    unsigned long long x = v;
+    for(int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(mask, x, off);
+    if(lane_id() == static_cast<uint32_t>(__ffs(mask) - 1) && x) atomicAdd(dst, x);
+}
+#endif
+
+}  // namespace lrt

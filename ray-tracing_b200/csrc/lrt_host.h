@@ -1,0 +1,57 @@
+// lrt_host.h — host-side scene assembly (no CUDA calls): SAH kd-tree build, device record packing,
+// rough-transmittance slicing, Fdr quadrature, camera and emitter precomputation.
+#pragma once
+
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "lrt.h"
+#include "lrt_types.h"
+
+namespace lrt {
+
+struct MeshTreeInfo {
+    uint32_t nodes;  // reachable nodes after packing
+    uint32_t refs;   // leaf references after packing
+    uint32_t depth;  // deepest leaf (root = 1)
+};
+
+struct HostScene {
+    std::vector<uint2> nodes;
+    std::vector<float4> tris;
+    std::vector<uint32_t> ref_prim;
+    std::vector<float4> normals;
+    std::vector<ObjRec> objects;
+    std::vector<MatRec> materials;
+    std::vector<float> tables;
+    std::vector<EmitRec> emitters;
+    std::vector<MeshTreeInfo> mesh_info;  // per object (zeros for analytic shapes)
+    CamRec cam{};
+    int32_t n_infinite = 0;
+    // scene::sample_emitter_ray's luminance CDF over emitters with positive power (scene.h:21-34)
+    std::vector<float> emission_cdf;
+    std::vector<int32_t> emission_index;
+    float emission_power = 0.0f;
+    float bounding_radius = 0.0f;  // scene::bounding_sphere_radius (scene.h:41-45)
+    bool has_delta_bsdf = false;   // scene::has_delta_bsdf (scene.h:48-57)
+};
+
+// Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message.
+int build_host_scene(const lrt_scene_desc* desc, HostScene& out, std::string& error);
+
+// SAH kd-tree over triangle AABBs, the tree sah_kdtree::build produces (src/accelerator/sah_kdtree.h:35-57,
+// 175-347), packed depth-first into 8-byte nodes with leaf references in leaf order.
+struct PackedTree {
+    std::vector<uint2> nodes;
+    std::vector<uint32_t> refs;  // triangle index per leaf reference
+    uint32_t depth = 0;
+};
+void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out);
+
+int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& error);
+float fresnel_diffuse_reflectance(float eta);
+void sobol_direction_table(uint32_t table[16][32]);
+
+}  // namespace lrt

@@ -1,0 +1,743 @@
+// lrt_photon.cu — photon tracing, the GPU-built balanced photon kd-tree and the k-nearest-photon
+// gather / irradiance estimate of the LinRT photon mapper.
+//
+//   photon trace   photon_tracer::trace_particle (photon_tracer.h:23-96) per particle index, one
+//                  thread per particle; a counting pass and a storing pass at prefix-sum offsets give
+//                  the photons in particle-index order, cut exactly as photon_gather::process_result
+//                  cuts them with one worker (photon_gather.h:65-101)
+//   map build      the tree photon_map::build_range describes (photon_map.h:83-114): a node over
+//                  [start, start+count) is a leaf when count <= 8, otherwise it splits at the median
+//                  (start + count/2) on the largest-extent axis of its photons. The topology depends
+//                  only on the count; the device computes, level by level, each node's bounds and
+//                  axis, sorts every node range on its axis (CUB segmented radix sort) and reads the
+//                  split at the median.
+//   k-NN gather    photon_map::nearest/search (photon_map.h:117-165): near child first, the far child
+//                  when delta^2 <= the limit taken at node entry, a max-heap of (d2, index) that pops
+//                  its maximum for every candidate with d2 <= limit once full
+//   irradiance     photon_map::estimate_irradiance (photon_map.h:38-70) over the neighbours in heap
+//                  pop order
+#include <cub/device/device_segmented_radix_sort.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "lrt_context.cuh"
+#include "lrt_scene.cuh"
+
+using namespace lrt;
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// photon trace
+
+struct EmitterRay {
+    Ray ray;
+    f3 weight;
+};
+
+// area_emitter::sample_ray (area_emitter.h:93-122)
+__device__ __forceinline__ bool area_sample_ray(const DeviceScene& s, const EmitRec& e, float sx, float sy, float dx,
+                                                float dy, EmitterRay& out) {
+    if(e.area <= 0.0f) return false;
+    f3 p, n;
+    float pdf_area = 0.0f;
+    shape_sample_position(s.objects[e.object], sx, sy, p, n, pdf_area);
+    if(pdf_area <= 0.0f) return false;
+    const float cos_theta = sqrtf(dx);
+    const float sin_theta = sqrtf(1.0f - dx);
+    const float phi = 2.0f * kPi * dy;
+    const f3 local{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    const Onb frame = onb_from_normal(n);
+    out.ray = Ray{p, to_world(frame, local)};
+    out.weight = load3(e.radiance) * (kPi * e.area);  // power()
+    return true;
+}
+
+// scene::sample_emitter_ray (scene.h:113-142)
+__device__ __forceinline__ bool sample_emitter_ray(const DeviceScene& s, F2 spatial, F2 directional, EmitterRay& out) {
+    if(s.emission_power <= 0.0f || s.n_emission <= 0) return false;
+    const float target = spatial.x * s.emission_power;
+    int32_t bin = 0;  // std::upper_bound: first bin with cdf > target
+    while(bin < s.n_emission && !(target < s.emission_cdf[bin])) ++bin;
+    if(bin >= s.n_emission) bin = s.n_emission - 1;
+    const float prev = bin == 0 ? 0.0f : s.emission_cdf[bin - 1];
+    const float span = s.emission_cdf[bin] - prev;
+    if(span <= 0.0f) return false;
+    const float selection_pdf = span / s.emission_power;
+    const float u = (target - prev) / span;
+    const EmitRec& e = s.emitters[s.emission_index[bin]];
+    if(e.kind != LRT_EMITTER_AREA) return false;  // env_emitter::sample_ray returns false
+    if(!area_sample_ray(s, e, u, spatial.y, directional.x, directional.y, out)) return false;
+    out.weight /= selection_pdf;
+    return true;
+}
+
+struct PhotonOut {
+    lrt_photon* out;    // destination (nullptr: count only)
+    uint64_t base;      // index of this particle's first photon in `out`
+    uint64_t limit;     // photons at index >= limit are dropped
+    uint32_t count;     // photons emitted by the particle
+};
+
+__device__ __forceinline__ void emit_photon(PhotonOut& o, f3 p, f3 dir, f3 n, f3 power, int depth) {
+    const uint64_t slot = o.base + o.count;
+    ++o.count;
+    if(!o.out || slot >= o.limit) return;
+    lrt_photon ph;
+    store3(ph.position, p);
+    store3(ph.direction, dir);
+    store3(ph.normal, n);
+    store3(ph.power, power);
+    ph.depth = static_cast<uint32_t>(static_cast<uint16_t>(depth));
+    o.out[slot] = ph;
+}
+
+// photon_tracer::trace_particle + store_if_accepted (photon_tracer.h:23-96)
+__device__ void trace_particle(const DeviceScene& s, int kind, uint32_t index, int max_depth, int rr_depth,
+                               PhotonOut& out) {
+    const uint32_t(*table)[32] = sobol_table(s);
+    Sampler smp = sampler_start(0u, index);
+    // sample_emitter_ray(next_2d(), next_2d(), ...): the right argument (directional) draws first
+    const F2 directional = sampler_next_2d(table, smp);
+    const F2 spatial = sampler_next_2d(table, smp);
+    EmitterRay er;
+    if(!sample_emitter_ray(s, spatial, directional, er)) return;
+    Ray current = er.ray;
+    f3 throughput = mk(1.0f);
+    bool delta = false;
+    TraceCount cnt{0, 0};
+    for(int depth = 1; !is_zero(throughput) && depth <= max_depth;) {
+        HitInfo rec;
+        if(!scene_hit<false>(s, current, 0.001f, kInf, rec, cnt)) break;
+        const int32_t mid = s.objects[rec.object].material;
+        if(mid < 0) break;
+        const MatRec& mat = s.materials[mid];
+        const bool smooth = (mat.flags & kDiffuse) != 0 || (mat.flags & kGlossy) != 0;
+        if(smooth && depth > 1 && (kind == LRT_GATHER_CAUSTIC ? delta : !delta)) {
+            emit_photon(out, rec.p, normalize(current.d), rec.normal, throughput * er.weight, depth);
+        }
+        const Onb basis = onb_from_normal(rec.normal);
+        BsdfCtx ctx = ctx_default(LRT_MODE_IMPORTANCE);
+        ctx.lobe_sample = sampler_next_1d(table, smp);
+        BRec br{};
+        br.wi = to_local(basis, -normalize(current.d));
+        br.wo = mk(0.0f);
+        br.front_face = rec.front_face;
+        br.eta = 1.0f;
+        const F2 u = sampler_next_2d(table, smp);
+        const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, br, u.x, u.y);
+        if(is_zero(weight)) break;
+        const f3 outgoing = to_world(basis, br.wo);
+        const f3 incoming = to_world(basis, br.wi);
+        if(dot(rec.normal, incoming) * br.wi.z <= 0.0f || dot(rec.normal, outgoing) * br.wo.z <= 0.0f) break;
+        throughput *= weight;
+        delta = (br.sampled_type & kSpecular) != 0;
+        current = Ray{rec.p, outgoing};
+        if(depth++ >= rr_depth) {
+            const float survival = smin(max3(throughput), 0.95f);
+            if(sampler_next_1d(table, smp) >= survival) break;
+            throughput /= survival;
+        }
+    }
+}
+
+// one slot of max_per photons per particle (parity entry point)
+__global__ void k_particles_slots(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
+                                  uint32_t max_per, lrt_photon* out, uint32_t* counts) {
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        PhotonOut o{out, static_cast<uint64_t>(i) * max_per, static_cast<uint64_t>(i) * max_per + max_per, 0};
+        trace_particle(s, kind, first + i, max_depth, rr_depth, o);
+        counts[i] = o.count;
+    }
+}
+
+// counting pass
+__global__ void k_particles_count(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
+                                  uint32_t* counts) {
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        PhotonOut o{nullptr, 0, 0, 0};
+        trace_particle(s, kind, first + i, max_depth, rr_depth, o);
+        counts[i] = o.count;
+    }
+}
+
+// storing pass: particle i writes at offsets[i] (absolute photon index), dropping indices >= limit
+__global__ void k_particles_store(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
+                                  const uint64_t* offsets, uint64_t limit, lrt_photon* out) {
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        PhotonOut o{out, offsets[i], limit, 0};
+        if(offsets[i] >= limit) continue;
+        trace_particle(s, kind, first + i, max_depth, rr_depth, o);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// photon map build, reference-identical (host): photon_map::build_range (photon_map.h:83-114) with the
+// same std::nth_element. The split of a node is read from photons[mid] after both children have been
+// built, i.e. after the right child has re-partitioned its range, exactly as the reference does; that
+// value is generally not the median the node was partitioned on, and the search inherits the effect.
+struct HostPhoton {
+    float p[3];
+    uint32_t index;
+};
+
+int32_t build_range_host(std::vector<HostPhoton>& ph, int32_t start, int32_t count, std::vector<PhotonNode>& nodes,
+                         uint32_t depth, uint32_t& max_depth) {
+    const int32_t index = static_cast<int32_t>(nodes.size());
+    nodes.push_back(PhotonNode{start, count, 3, 0.0f});
+    max_depth = std::max(max_depth, depth);
+    if(count <= 8) return index;
+    float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+    for(int32_t i = 0; i < count; ++i) {
+        for(int a = 0; a < 3; ++a) {
+            lo[a] = smin(lo[a], ph[start + i].p[a]);
+            hi[a] = smax(hi[a], ph[start + i].p[a]);
+        }
+    }
+    const float extent[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    int axis = 0;
+    if(extent[1] > extent[axis]) axis = 1;
+    if(extent[2] > extent[axis]) axis = 2;
+    const int32_t mid = start + count / 2;
+    std::nth_element(ph.begin() + start, ph.begin() + mid, ph.begin() + start + count,
+                     [axis](const HostPhoton& a, const HostPhoton& b) { return a.p[axis] < b.p[axis]; });
+    const int32_t left = build_range_host(ph, start, mid - start, nodes, depth + 1, max_depth);
+    const int32_t right = build_range_host(ph, mid, start + count - mid, nodes, depth + 1, max_depth);
+    nodes[index] = PhotonNode{left, right, axis, ph[mid].p[axis]};
+    return index;
+}
+
+__global__ void k_photon_gather_attrs(const lrt_photon* in, const uint32_t* order, uint32_t n, float4* pos, float4* dir,
+                                      float4* nrm, float4* pw) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const uint32_t src = order[i];
+    const lrt_photon& p = in[src];
+    pos[i] = make_float4(p.position[0], p.position[1], p.position[2], __uint_as_float(src));
+    dir[i] = make_float4(p.direction[0], p.direction[1], p.direction[2], __int_as_float(static_cast<int>(p.depth)));
+    nrm[i] = make_float4(p.normal[0], p.normal[1], p.normal[2], 0.0f);
+    pw[i] = make_float4(p.power[0], p.power[1], p.power[2], 0.0f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// photon map build on the device (option photon_tree_device): same topology, every node range sorted
+// on its axis, split = the median value. A valid partition, so the search finds the exact k nearest
+// photons within the radius; the reference's tree can miss some of them (see above).
+
+struct HostNode {
+    int32_t start, count, left, right, depth;
+};
+
+int build_topology(int32_t start, int32_t count, int32_t depth, std::vector<HostNode>& nodes) {
+    const int32_t index = static_cast<int32_t>(nodes.size());
+    nodes.push_back(HostNode{start, count, -1, -1, depth});
+    if(count <= 8) return index;
+    const int32_t mid = start + count / 2;
+    const int32_t left = build_topology(start, mid - start, depth + 1, nodes);
+    const int32_t right = build_topology(mid, start + count - mid, depth + 1, nodes);
+    nodes[index].left = left;
+    nodes[index].right = right;
+    return index;
+}
+
+__global__ void k_photon_positions(const lrt_photon* in, uint32_t n, float4* pos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    pos[i] = make_float4(in[i].position[0], in[i].position[1], in[i].position[2], __uint_as_float(i));
+}
+
+// one block per node: bounds of its photons -> largest-extent axis (photon_map.h:94-100); then the sort keys
+__global__ void __launch_bounds__(256) k_node_axis(const float4* pos, const int2* segs, const int32_t* seg_node,
+                                                   PhotonNode* nodes, float* keys, uint32_t* vals) {
+    __shared__ float lo[3][256];
+    __shared__ float hi[3][256];
+    __shared__ int axis_s;
+    const int2 seg = segs[blockIdx.x];
+    float l0 = kInf, l1 = kInf, l2 = kInf, h0 = -kInf, h1 = -kInf, h2 = -kInf;
+    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) {
+        const float4 p = pos[i];
+        l0 = smin(l0, p.x); l1 = smin(l1, p.y); l2 = smin(l2, p.z);
+        h0 = smax(h0, p.x); h1 = smax(h1, p.y); h2 = smax(h2, p.z);
+    }
+    lo[0][threadIdx.x] = l0; lo[1][threadIdx.x] = l1; lo[2][threadIdx.x] = l2;
+    hi[0][threadIdx.x] = h0; hi[1][threadIdx.x] = h1; hi[2][threadIdx.x] = h2;
+    __syncthreads();
+    for(int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if(threadIdx.x < stride) {
+            for(int a = 0; a < 3; ++a) {
+                lo[a][threadIdx.x] = smin(lo[a][threadIdx.x], lo[a][threadIdx.x + stride]);
+                hi[a][threadIdx.x] = smax(hi[a][threadIdx.x], hi[a][threadIdx.x + stride]);
+            }
+        }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) {
+        const f3 extent = f3{hi[0][0], hi[1][0], hi[2][0]} - f3{lo[0][0], lo[1][0], lo[2][0]};
+        int axis = 0;
+        if(extent.y > comp(extent, axis)) axis = 1;
+        if(extent.z > comp(extent, axis)) axis = 2;
+        axis_s = axis;
+        nodes[seg_node[blockIdx.x]].axis = axis;
+    }
+    __syncthreads();
+    const int axis = axis_s;
+    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) {
+        const float4 p = pos[i];
+        keys[i] = axis == 0 ? p.x : (axis == 1 ? p.y : p.z);
+        vals[i] = static_cast<uint32_t>(i);
+    }
+}
+
+// reorder each node range by the sorted permutation and read the split at the median (photon_map.h:102-110)
+__global__ void __launch_bounds__(256) k_node_permute(const float4* pos, float4* out, const int2* segs,
+                                                      const int32_t* seg_node, const uint32_t* perm, PhotonNode* nodes) {
+    const int2 seg = segs[blockIdx.x];
+    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) out[i] = pos[perm[i]];
+    if(threadIdx.x == 0) {
+        PhotonNode& nd = nodes[seg_node[blockIdx.x]];
+        const int mid = seg.x + (seg.y - seg.x) / 2;
+        const float4 p = pos[perm[mid]];
+        nd.split = nd.axis == 0 ? p.x : (nd.axis == 1 ? p.y : p.z);
+    }
+}
+
+__global__ void k_photon_attrs(const lrt_photon* in, const float4* pos, uint32_t n, float4* dir, float4* nrm, float4* pw) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const lrt_photon& p = in[__float_as_uint(pos[i].w)];
+    dir[i] = make_float4(p.direction[0], p.direction[1], p.direction[2], __int_as_float(static_cast<int>(p.depth)));
+    nrm[i] = make_float4(p.normal[0], p.normal[1], p.normal[2], 0.0f);
+    pw[i] = make_float4(p.power[0], p.power[1], p.power[2], 0.0f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// k-NN gather
+
+struct MapView {
+    const float4* pos;
+    const float4* dir;
+    const float4* nrm;
+    const float4* pw;
+    const PhotonNode* nodes;
+    uint32_t n;
+    float scale;
+};
+
+// (d2, index) pairs compared as std::pair
+__device__ __forceinline__ bool pair_less(float da, uint32_t ia, float db, uint32_t ib) {
+    return da < db || (!(db < da) && ia < ib);
+}
+
+struct KnnHeap {
+    float d[kMaxKnn];
+    uint32_t i[kMaxKnn];
+    uint32_t size;
+
+    __device__ __forceinline__ void pop() {  // remove the maximum
+        --size;
+        if(size == 0) return;
+        const float dl = d[size];
+        const uint32_t il = i[size];
+        uint32_t k = 0;
+        while(true) {
+            uint32_t c = 2 * k + 1;
+            if(c >= size) break;
+            if(c + 1 < size && pair_less(d[c], i[c], d[c + 1], i[c + 1])) ++c;
+            if(!pair_less(dl, il, d[c], i[c])) break;
+            d[k] = d[c];
+            i[k] = i[c];
+            k = c;
+        }
+        d[k] = dl;
+        i[k] = il;
+    }
+    __device__ __forceinline__ void push(float dv, uint32_t iv) {
+        uint32_t k = size++;
+        while(k > 0) {
+            const uint32_t parent = (k - 1) / 2;
+            if(!pair_less(d[parent], i[parent], dv, iv)) break;
+            d[k] = d[parent];
+            i[k] = i[parent];
+            k = parent;
+        }
+        d[k] = dv;
+        i[k] = iv;
+    }
+};
+
+__device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2, uint32_t k, KnnHeap& heap) {
+    heap.size = 0;
+    if(m.n == 0 || k == 0) return;
+    int32_t stack[64];
+    int top = 0;
+    stack[top++] = 0;
+    while(top > 0) {
+        const PhotonNode nd = m.nodes[stack[--top]];
+        float limit = r2;
+        if(heap.size == k) limit = smin(limit, heap.d[0]);
+        if(nd.axis == 3) {
+            for(int32_t j = 0; j < nd.b; ++j) {
+                const uint32_t pi = static_cast<uint32_t>(nd.a + j);
+                const float4 p4 = __ldg(m.pos + pi);
+                const float distance = length_squared(f3{p4.x, p4.y, p4.z} - point);
+                if(distance > limit) continue;
+                if(heap.size == k) heap.pop();
+                heap.push(distance, pi);
+                if(heap.size == k) limit = smin(r2, heap.d[0]);
+            }
+            continue;
+        }
+        const float delta = comp(point, nd.axis) - nd.split;
+        const int32_t near = delta <= 0.0f ? nd.a : nd.b;
+        const int32_t far = delta <= 0.0f ? nd.b : nd.a;
+        if(delta * delta <= limit && top < 64) stack[top++] = far;
+        if(top < 64) stack[top++] = near;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_knn(MapView m, const float* points, uint32_t n, float r2, uint32_t k,
+                                                uint32_t* idx_out, float* d2_out, uint32_t* cnt_out) {
+    for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        KnnHeap heap;
+        knn_search(m, load3(points + 3ull * q), r2, k, heap);
+        const uint32_t found = heap.size;
+        cnt_out[q] = found;
+        for(uint32_t j = 0; j < found; ++j) {  // max-heap pop order
+            idx_out[static_cast<size_t>(q) * k + j] = __float_as_uint(m.pos[heap.i[0]].w);
+            d2_out[static_cast<size_t>(q) * k + j] = heap.d[0];
+            heap.pop();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_irradiance(MapView m, const float* points, const float* normals, uint32_t n,
+                                                       float radius, int32_t max_depth, uint32_t k, float* rgb) {
+    for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        f3 sum = mk(0.0f);
+        if(m.n > 0 && radius > 0.0f && k > 0) {
+            const float squared_radius = radius * radius;
+            KnnHeap heap;
+            knn_search(m, load3(points + 3ull * q), squared_radius, k, heap);
+            const float inverse_squared_radius = 1.0f / squared_radius;
+            const f3 normal = load3(normals + 3ull * q);
+            while(heap.size > 0) {
+                const uint32_t pi = heap.i[0];
+                const float d2 = heap.d[0];
+                heap.pop();
+                const float4 dir = m.dir[pi];
+                if(__float_as_int(dir.w) > max_depth) continue;
+                const float4 pn = m.nrm[pi];
+                const f3 photon_normal{pn.x, pn.y, pn.z};
+                const f3 incoming = -f3{dir.x, dir.y, dir.z};
+                const float incoming_dot_photon = dot(photon_normal, incoming);
+                const float incoming_dot_shading = dot(normal, incoming);
+                if(incoming_dot_shading <= 0.0f || dot(photon_normal, normal) <= 1e-1f || incoming_dot_photon <= 1e-2f) {
+                    continue;
+                }
+                const float square = 1.0f - d2 * inverse_squared_radius;
+                const float weight = (incoming_dot_shading / incoming_dot_photon) * (square * square);
+                const float4 pw = m.pw[pi];
+                sum += f3{pw.x, pw.y, pw.z} * fabsf(weight);
+            }
+            sum = sum * (m.scale * 3.0f * (1.0f / kPi) * inverse_squared_radius);
+        }
+        store3(rgb + 3ull * q, sum);
+    }
+}
+
+MapView view_of(const PhotonMap& pm) {
+    return MapView{pm.pos.as<float4>(), pm.dir.as<float4>(), pm.nrm.as<float4>(), pm.pow.as<float4>(),
+                   pm.nodes.as<PhotonNode>(), pm.n, pm.scale};
+}
+
+bool unsuccessful(uint64_t needed, uint64_t stored, uint64_t shot) {
+    return stored < needed && (stored == 0 || stored < shot / 1024);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_photon_trace_particles(lrt_context* ctx, int32_t kind, uint32_t first, uint32_t count, int32_t max_depth,
+                               int32_t rr_depth, uint32_t max_per, lrt_photon* photons_out, uint32_t* counts_out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(count == 0) return LRT_OK;
+    if(!photons_out || !counts_out || max_per == 0 || (kind != LRT_GATHER_SURFACE && kind != LRT_GATHER_CAUSTIC)) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "bad photon trace arguments");
+    }
+    const size_t pb = sizeof(lrt_photon) * static_cast<size_t>(count) * max_per, cb = 4ull * count;
+    LRT_CUDA(ctx, ctx->ph_out.ensure(pb));
+    LRT_CUDA(ctx, ctx->ph_counts.ensure(cb));
+    LRT_CUDA(ctx, cudaMemsetAsync(ctx->ph_out.ptr, 0, pb, ctx->stream));
+    k_particles_slots<<<blocks_for(count), kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, count, max_depth, rr_depth,
+                                                                    max_per, ctx->ph_out.as<lrt_photon>(),
+                                                                    ctx->ph_counts.as<uint32_t>());
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(photons_out, ctx->ph_out.ptr, pb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(counts_out, ctx->ph_counts.ptr, cb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t max_depth, int32_t rr_depth,
+                     lrt_photon* photons_out, uint32_t* n_out, uint64_t* shot_out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(!n_out || !shot_out || (kind != LRT_GATHER_SURFACE && kind != LRT_GATHER_CAUSTIC)) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "bad photon trace arguments");
+    }
+    *n_out = 0;
+    *shot_out = 0;
+    if(requested == 0 || max_depth < 1) return LRT_OK;  // photon_gather.h:20-22
+    if(!photons_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photon buffer");
+    // work items of `granularity` particles as with one worker (photon_gather.h:26-28)
+    const uint64_t granularity = std::max<uint64_t>(1, requested / 16);
+    const uint64_t batches_per_launch = std::max<uint64_t>(1, (1ull << 21) / granularity);
+    const uint64_t chunk = std::min<uint64_t>(granularity * batches_per_launch, 1ull << 24);
+    LRT_CUDA(ctx, ctx->ph_out.ensure(sizeof(lrt_photon) * static_cast<size_t>(requested)));
+    LRT_CUDA(ctx, ctx->ph_counts.ensure(4 * chunk));
+    LRT_CUDA(ctx, ctx->ph_offsets.ensure(8 * chunk));
+    std::vector<uint32_t> counts(chunk);
+    std::vector<uint64_t> offsets(chunk);
+    uint64_t stored = 0, shot = 0, returned = 0, next = 0;
+    bool done = false;
+    const int grid = grid_for(ctx, (const void*)k_particles_count, kBlock);
+    while(!done) {
+        if(next + chunk > 0xffffffffull) return fail(ctx, LRT_ERR_RANGE, "particle index space exhausted");
+        const uint32_t first = static_cast<uint32_t>(next);
+        const uint32_t n = static_cast<uint32_t>(chunk);
+        k_particles_count<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, n, max_depth, rr_depth,
+                                                            ctx->ph_counts.as<uint32_t>());
+        LRT_CUDA(ctx, cudaGetLastError());
+        LRT_CUDA(ctx, cudaMemcpyAsync(counts.data(), ctx->ph_counts.ptr, 4 * chunk, cudaMemcpyDeviceToHost, ctx->stream));
+        LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        // walk the work items in order: generate_work's stop test, then process_result's cut
+        uint64_t taken = 0;  // particles of this launch that store
+        for(uint64_t b = 0; b < batches_per_launch && !done; ++b) {
+            if(returned >= requested || (shot > 100000 && unsuccessful(requested, stored, shot))) {
+                done = true;
+                break;
+            }
+            uint64_t counted = 0, batch_photons = 0;
+            bool full = false;
+            for(uint64_t j = 0; j < granularity; ++j) {
+                const uint64_t i = b * granularity + j;
+                batch_photons += counts[i];
+                offsets[i] = stored;
+                if(full) continue;
+                ++counted;
+                if(counts[i] > 0 && stored >= requested) {
+                    full = true;
+                    continue;
+                }
+                const uint64_t room = requested - stored;
+                if(counts[i] > room) {
+                    stored = requested;
+                    full = true;
+                } else {
+                    stored += counts[i];
+                }
+                taken = i + 1;
+            }
+            shot += counted;
+            returned += batch_photons;
+        }
+        if(taken > 0) {
+            LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_offsets.ptr, offsets.data(), 8 * taken, cudaMemcpyHostToDevice, ctx->stream));
+            k_particles_store<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, static_cast<uint32_t>(taken), max_depth,
+                                                                rr_depth, ctx->ph_offsets.as<uint64_t>(), requested,
+                                                                ctx->ph_out.as<lrt_photon>());
+            LRT_CUDA(ctx, cudaGetLastError());
+            LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        next += chunk;
+    }
+    if(stored > 0) {
+        LRT_CUDA(ctx, cudaMemcpyAsync(photons_out, ctx->ph_out.ptr, sizeof(lrt_photon) * stored, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    *n_out = static_cast<uint32_t>(stored);
+    *shot_out = shot;
+    return LRT_OK;
+}
+
+int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photons, uint32_t n, float scale) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
+    if(n > 0 && !photons) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photons");
+    if(n >= (1u << 30)) return fail(ctx, LRT_ERR_RANGE, "too many photons");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    PhotonMap& pm = ctx->maps[map];
+    pm.n = n;
+    pm.scale = scale;
+    pm.n_nodes = 0;
+    if(n == 0) return LRT_OK;
+    cudaStream_t s = ctx->stream;
+    if(!ctx->photon_tree_device) {
+        std::vector<HostPhoton> ph(n);
+        for(uint32_t i = 0; i < n; ++i) {
+            ph[i] = HostPhoton{{photons[i].position[0], photons[i].position[1], photons[i].position[2]}, i};
+        }
+        std::vector<PhotonNode> nodes;
+        nodes.reserve(n / 4 + 16);
+        uint32_t max_depth = 0;
+        build_range_host(ph, 0, static_cast<int32_t>(n), nodes, 1, max_depth);
+        std::vector<uint32_t> order(n);
+        for(uint32_t i = 0; i < n; ++i) order[i] = ph[i].index;
+        LRT_CUDA(ctx, pm.pos.ensure(16ull * n));
+        LRT_CUDA(ctx, pm.dir.ensure(16ull * n));
+        LRT_CUDA(ctx, pm.nrm.ensure(16ull * n));
+        LRT_CUDA(ctx, pm.pow.ensure(16ull * n));
+        LRT_CUDA(ctx, pm.nodes.ensure(sizeof(PhotonNode) * nodes.size()));
+        LRT_CUDA(ctx, ctx->ph_tmp.ensure(sizeof(lrt_photon) * static_cast<size_t>(n)));
+        LRT_CUDA(ctx, ctx->ph_vals.ensure(4ull * n));
+        LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_tmp.ptr, photons, sizeof(lrt_photon) * static_cast<size_t>(n),
+                                      cudaMemcpyHostToDevice, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_vals.ptr, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(pm.nodes.ptr, nodes.data(), sizeof(PhotonNode) * nodes.size(), cudaMemcpyHostToDevice, s));
+        k_photon_gather_attrs<<<blocks_for(n), kBlock, 0, s>>>(ctx->ph_tmp.as<lrt_photon>(), ctx->ph_vals.as<uint32_t>(), n,
+                                                               pm.pos.as<float4>(), pm.dir.as<float4>(), pm.nrm.as<float4>(),
+                                                               pm.pow.as<float4>());
+        LRT_CUDA(ctx, cudaGetLastError());
+        LRT_CUDA(ctx, cudaStreamSynchronize(s));
+        pm.n_nodes = static_cast<uint32_t>(nodes.size());
+        pm.depth = max_depth;
+        return LRT_OK;
+    }
+    // topology (depends only on n) in the reference's depth-first node order
+    std::vector<HostNode> topo;
+    topo.reserve(n / 4 + 16);
+    build_topology(0, static_cast<int32_t>(n), 0, topo);
+    std::vector<PhotonNode> nodes(topo.size());
+    int32_t max_level = 0;
+    for(size_t i = 0; i < topo.size(); ++i) {
+        const HostNode& h = topo[i];
+        if(h.left < 0) {
+            nodes[i] = PhotonNode{h.start, h.count, 3, 0.0f};
+        } else {
+            nodes[i] = PhotonNode{h.left, h.right, 0, 0.0f};
+            max_level = std::max(max_level, h.depth);
+        }
+    }
+    pm.depth = static_cast<uint32_t>(max_level + 1);
+    LRT_CUDA(ctx, pm.pos.ensure(16ull * n));
+    LRT_CUDA(ctx, pm.dir.ensure(16ull * n));
+    LRT_CUDA(ctx, pm.nrm.ensure(16ull * n));
+    LRT_CUDA(ctx, pm.pow.ensure(16ull * n));
+    LRT_CUDA(ctx, pm.nodes.ensure(sizeof(PhotonNode) * nodes.size()));
+    LRT_CUDA(ctx, ctx->ph_tmp.ensure(sizeof(lrt_photon) * static_cast<size_t>(n)));
+    LRT_CUDA(ctx, ctx->ph_keys.ensure(8ull * n));
+    LRT_CUDA(ctx, ctx->ph_vals.ensure(8ull * n));
+    LRT_CUDA(ctx, ctx->scratch_b.ensure(16ull * n));
+    LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_tmp.ptr, photons, sizeof(lrt_photon) * static_cast<size_t>(n),
+                                  cudaMemcpyHostToDevice, s));
+    LRT_CUDA(ctx, cudaMemcpyAsync(pm.nodes.ptr, nodes.data(), sizeof(PhotonNode) * nodes.size(), cudaMemcpyHostToDevice, s));
+    k_photon_positions<<<blocks_for(n), kBlock, 0, s>>>(ctx->ph_tmp.as<lrt_photon>(), n, pm.pos.as<float4>());
+    LRT_CUDA(ctx, cudaGetLastError());
+    // per level: the interior nodes as sort segments
+    std::vector<std::vector<int32_t>> levels(max_level + 1);
+    for(size_t i = 0; i < topo.size(); ++i) {
+        if(topo[i].left >= 0) levels[topo[i].depth].push_back(static_cast<int32_t>(i));
+    }
+    float* keys_in = ctx->ph_keys.as<float>();
+    float* keys_out = keys_in + n;
+    uint32_t* vals_in = ctx->ph_vals.as<uint32_t>();
+    uint32_t* vals_out = vals_in + n;
+    float4* pos = pm.pos.as<float4>();
+    float4* pos_tmp = ctx->scratch_b.as<float4>();
+    for(int32_t level = 0; level <= max_level; ++level) {
+        const std::vector<int32_t>& ids = levels[level];
+        if(ids.empty()) continue;
+        const int32_t nseg = static_cast<int32_t>(ids.size());
+        std::vector<int2> segs(nseg);
+        std::vector<int32_t> begin(nseg), end(nseg);
+        for(int32_t j = 0; j < nseg; ++j) {
+            const HostNode& h = topo[ids[j]];
+            segs[j] = make_int2(h.start, h.start + h.count);
+            begin[j] = h.start;
+            end[j] = h.start + h.count;
+        }
+        const size_t seg_bytes = sizeof(int2) * nseg + 3 * sizeof(int32_t) * nseg;
+        LRT_CUDA(ctx, ctx->ph_seg.ensure(seg_bytes));
+        char* sb = ctx->ph_seg.as<char>();
+        int2* d_segs = reinterpret_cast<int2*>(sb);
+        int32_t* d_node = reinterpret_cast<int32_t*>(sb + sizeof(int2) * nseg);
+        int32_t* d_begin = d_node + nseg;
+        int32_t* d_end = d_begin + nseg;
+        LRT_CUDA(ctx, cudaMemcpyAsync(d_segs, segs.data(), sizeof(int2) * nseg, cudaMemcpyHostToDevice, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(d_node, ids.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(d_begin, begin.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(d_end, end.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
+        k_node_axis<<<nseg, 256, 0, s>>>(pos, d_segs, d_node, pm.nodes.as<PhotonNode>(), keys_in, vals_in);
+        LRT_CUDA(ctx, cudaGetLastError());
+        size_t temp = 0;
+        LRT_CUDA(ctx, cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp, keys_in, keys_out, vals_in, vals_out,
+                                                               static_cast<int>(n), nseg, d_begin, d_end, 0, 32, s));
+        LRT_CUDA(ctx, ctx->ph_cub.ensure(temp));
+        LRT_CUDA(ctx, cub::DeviceSegmentedRadixSort::SortPairs(ctx->ph_cub.ptr, temp, keys_in, keys_out, vals_in,
+                                                               vals_out, static_cast<int>(n), nseg, d_begin, d_end, 0,
+                                                               32, s));
+        LRT_CUDA(ctx, cudaMemcpyAsync(pos_tmp, pos, 16ull * n, cudaMemcpyDeviceToDevice, s));
+        k_node_permute<<<nseg, 256, 0, s>>>(pos, pos_tmp, d_segs, d_node, vals_out, pm.nodes.as<PhotonNode>());
+        LRT_CUDA(ctx, cudaGetLastError());
+        LRT_CUDA(ctx, cudaMemcpyAsync(pos, pos_tmp, 16ull * n, cudaMemcpyDeviceToDevice, s));
+        LRT_CUDA(ctx, cudaStreamSynchronize(s));  // the segment arrays are rewritten next level
+    }
+    k_photon_attrs<<<blocks_for(n), kBlock, 0, s>>>(ctx->ph_tmp.as<lrt_photon>(), pos, n, pm.dir.as<float4>(),
+                                                     pm.nrm.as<float4>(), pm.pow.as<float4>());
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaStreamSynchronize(s));
+    pm.n_nodes = static_cast<uint32_t>(nodes.size());
+    return LRT_OK;
+}
+
+int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t n, float r2, uint32_t k,
+                   uint32_t* idx_out, float* d2_out, uint32_t* count_out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
+    if(k > kMaxKnn) return fail(ctx, LRT_ERR_RANGE, "k must be at most %u", kMaxKnn);
+    if(n == 0) return LRT_OK;
+    if(!points || !idx_out || !d2_out || !count_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t pb = 12ull * n, ib = 4ull * n * k, cb = 4ull * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(pb + 2 * ib + cb));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, points, pb, cudaMemcpyHostToDevice, ctx->stream));
+    uint32_t* di = reinterpret_cast<uint32_t*>(base + pb);
+    float* dd = reinterpret_cast<float*>(base + pb + ib);
+    uint32_t* dc = reinterpret_cast<uint32_t*>(base + pb + 2 * ib);
+    const int grid = grid_for(ctx, (const void*)k_knn, kBlock);
+    k_knn<<<grid, kBlock, 0, ctx->stream>>>(view_of(ctx->maps[map]), reinterpret_cast<float*>(base), n, r2, k, di, dd, dc);
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(idx_out, di, ib, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(d2_out, dd, ib, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(count_out, dc, cb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, const float* normals, uint32_t n,
+                          float radius, int32_t max_depth, uint32_t k, float* rgb_out) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
+    if(k > kMaxKnn) return fail(ctx, LRT_ERR_RANGE, "k must be at most %u", kMaxKnn);
+    if(n == 0) return LRT_OK;
+    if(!points || !normals || !rgb_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t pb = 12ull * n;
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(3 * pb));
+    float* base = ctx->scratch_a.as<float>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, points, pb, cudaMemcpyHostToDevice, ctx->stream));
+    LRT_CUDA(ctx, cudaMemcpyAsync(base + 3ull * n, normals, pb, cudaMemcpyHostToDevice, ctx->stream));
+    const int grid = grid_for(ctx, (const void*)k_irradiance, kBlock);
+    k_irradiance<<<grid, kBlock, 0, ctx->stream>>>(view_of(ctx->maps[map]), base, base + 3ull * n, n, radius, max_depth, k,
+                                                   base + 6ull * n);
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(rgb_out, base + 6ull * n, pb, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,485 @@
+// lrt_scene.cuh — device-side scene queries: kd-tree traversal with Moller-Trumbore triangle tests,
+// analytic shapes, the linear object list, emitters (area lights and the Hosek sky) and the camera.
+//
+// Traversal restates sah_kdtree::intersect (src/accelerator/sah_kdtree.h:62-121) over 8-byte nodes:
+// same front-to-back order, same [mint, maxt] intervals, same early exit, so the same leaves and
+// triangles are tested in the same order and the closest hit (ties: the later triangle wins,
+// triangle_mesh.h:77) is bit-identical.
+#pragma once
+
+#include "lrt_bsdf.cuh"
+#include "lrt_math.cuh"
+#include "lrt_types.h"
+
+namespace lrt {
+
+constexpr float kInf = __builtin_huge_valf();
+constexpr int kStackSize = 48;  // sah_kdtree.h:80 (depth limit <= 48 keeps the stack within bounds)
+
+struct Ray {
+    f3 o;
+    f3 d;
+};
+
+// per-ray traversal counters (algorithmic-bytes accounting); compiled out unless requested
+struct TraceCount {
+    uint32_t nodes;
+    uint32_t tris;
+};
+
+struct HitInfo {
+    float t;
+    int32_t object;     // -1 miss
+    int32_t prim;       // triangle within the mesh, -1 analytic
+    bool front_face;
+    f3 p;
+    f3 normal;          // hit_record::normal (faces the ray)
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint2 ld_node(const uint2* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ld_tri(const float4* p) { return __ldg(p); }
+#endif
+
+// Moller-Trumbore as triangle_mesh::hit_triangle (triangle_mesh.h:43-99), on a leaf record
+// (p0 | degenerate, edge1, edge2). Returns true and updates closest/u/v when accepted.
+__device__ __forceinline__ bool hit_tri_record(const float4* rec, const Ray& r, float t0, float t1, float& closest,
+                                               float& out_u, float& out_v) {
+    const float4 a = ld_tri(rec);
+    const float4 b = ld_tri(rec + 1);
+    const float4 c = ld_tri(rec + 2);
+    if(a.w != 0.0f) return false;  // cross(edge1, edge2).length_squared() <= 0
+    const f3 p0{a.x, a.y, a.z};
+    const f3 edge1{b.x, b.y, b.z};
+    const f3 edge2{c.x, c.y, c.z};
+    const f3 pvec = cross(r.d, edge2);
+    const float det = dot(edge1, pvec);
+    if(fabsf(det) < 1e-8f) return false;
+    const float inv_det = 1.0f / det;
+    const f3 tvec = r.o - p0;
+    const float u = dot(tvec, pvec) * inv_det;
+    if(u < 0.0f || u > 1.0f) return false;
+    const f3 qvec = cross(tvec, edge1);
+    const float v = dot(r.d, qvec) * inv_det;
+    if(v < 0.0f || u + v > 1.0f) return false;
+    const float t = dot(edge2, qvec) * inv_det;
+    if(t < t0 || t > t1) return false;
+    closest = t;
+    out_u = u;
+    out_v = v;
+    return true;
+}
+
+struct MeshHit {
+    float t;
+    float u, v;
+    uint32_t ref;  // leaf reference of the last accepted triangle
+};
+
+// sah_kdtree::intersect over one mesh's tree with the triangle_mesh::hit leaf callback.
+template <bool kCount>
+__device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o, const Ray& r, float t_min, float t_max,
+                                           MeshHit& h, TraceCount& cnt) {
+    const uint2* nodes = s.nodes + o.node_base;
+    const float4* tris = s.tris + 3ull * o.ref_base;
+    float closest = t_max;
+    bool hit_any = false;
+    const float inv_d[3] = {1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
+    struct Item {
+        uint32_t node;
+        float mint, maxt;
+    };
+    Item stack[kStackSize];
+    int top = 0;
+    float mint = t_min;
+    float maxt = closest;
+    uint32_t node = 0;
+    while(true) {
+        if(closest < mint) break;
+        const uint2 n = ld_node(nodes + node);
+        if(kCount) ++cnt.nodes;
+        if((n.y & 3u) == kLeafTag) {
+            const uint32_t count = n.y >> 2;
+            const uint32_t first = n.x;
+            float limit = smin(maxt, closest);
+            for(uint32_t i = 0; i < count; ++i) {
+                if(kCount) ++cnt.tris;
+                float u, v;
+                if(hit_tri_record(tris + 3ull * (first + i), r, mint, limit, closest, u, v)) {
+                    hit_any = true;
+                    h.t = closest;
+                    h.u = u;
+                    h.v = v;
+                    h.ref = first + i;
+                }
+                limit = smin(maxt, closest);
+            }
+            if(top == 0) break;
+            --top;
+            node = stack[top].node;
+            mint = stack[top].mint;
+            maxt = stack[top].maxt;
+            continue;
+        }
+        const uint32_t axis = n.y & 3u;
+        const float split = __uint_as_float(n.x);
+        const float o_a = comp(r.o, axis);
+        const float d_a = comp(r.d, axis);
+        const float t_plane = (split - o_a) * (axis == 0 ? inv_d[0] : (axis == 1 ? inv_d[1] : inv_d[2]));
+        const bool left_of_split = o_a < split || (o_a == split && d_a <= 0.0f);
+        const uint32_t right = n.y >> 2;
+        const uint32_t first_child = left_of_split ? node + 1 : right;
+        const uint32_t second_child = left_of_split ? right : node + 1;
+        if(t_plane > maxt || t_plane <= 0.0f) {
+            node = first_child;
+        } else if(t_plane < mint) {
+            node = second_child;
+        } else {
+            if(top < kStackSize) {
+                stack[top].node = second_child;
+                stack[top].mint = t_plane;
+                stack[top].maxt = maxt;
+                ++top;
+            }
+            node = first_child;
+            maxt = t_plane;
+        }
+    }
+    return hit_any;
+}
+
+// rectangle::hit (src/geometry/rectangle.h:18-55)
+__device__ __forceinline__ bool hit_rectangle(const ObjRec& o, const Ray& r, float t_min, float t_max, float& t_out,
+                                              f3& p_out) {
+    const f3 normal = load3(o.normal);
+    const float denom = dot(normal, r.d);
+    if(fabsf(denom) < 1e-8f) return false;
+    const f3 corner = load3(o.corner);
+    const float t = dot(corner - r.o, normal) / denom;
+    if(t < t_min || t > t_max) return false;
+    const f3 p = r.o + t * r.d;
+    const f3 d = p - corner;
+    const f3 eu = load3(o.edge_u);
+    const f3 ev = load3(o.edge_v);
+    const float uu = dot(eu, eu);
+    const float vv = dot(ev, ev);
+    const float uv = dot(eu, ev);
+    const float du = dot(d, eu);
+    const float dv = dot(d, ev);
+    const float det = uu * vv - uv * uv;
+    if(fabsf(det) < 1e-12f) return false;
+    const float u = (vv * du - uv * dv) / det;
+    const float v = (uu * dv - uv * du) / det;
+    if(u < 0.0f || u > 1.0f || v < 0.0f || v > 1.0f) return false;
+    t_out = t;
+    p_out = p;
+    return true;
+}
+
+// sphere::hit (src/geometry/sphere.h:21-49)
+__device__ __forceinline__ bool hit_sphere(const ObjRec& o, const Ray& r, float t_min, float t_max, float& t_out) {
+    const f3 center = load3(o.center);
+    const f3 oc = r.o - center;
+    const float a = length_squared(r.d);
+    const float half_b = dot(oc, r.d);
+    const float c = length_squared(oc) - o.radius * o.radius;
+    const float discriminant = half_b * half_b - a * c;
+    if(discriminant < 0.0f) return false;
+    const float sqrtd = sqrtf(discriminant);
+    float root = (-half_b - sqrtd) / a;
+    if(root < t_min || root > t_max) {
+        root = (-half_b + sqrtd) / a;
+        if(root < t_min || root > t_max) return false;
+    }
+    t_out = root;
+    return true;
+}
+
+// The full hit record of the object list's closest hit (hittable_list::hit, hittable_list.h:19-34,
+// then the record each shape writes).
+template <bool kCount>
+__device__ __forceinline__ bool scene_hit(const DeviceScene& s, const Ray& r, float t_min, float t_max, HitInfo& out,
+                                          TraceCount& cnt) {
+    float closest_so_far = t_max;
+    int32_t best = -1;
+    MeshHit best_mesh{};
+    for(int32_t i = 0; i < s.n_objects; ++i) {
+        const ObjRec& o = s.objects[i];
+        if(o.kind == LRT_OBJECT_MESH) {
+            MeshHit mh;
+            if(trace_mesh<kCount>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+                closest_so_far = mh.t;
+                best = i;
+                best_mesh = mh;
+            }
+        } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+            float t;
+            f3 p;
+            if(hit_rectangle(o, r, t_min, closest_so_far, t, p)) {
+                closest_so_far = t;
+                best = i;
+            }
+        } else {
+            float t;
+            if(hit_sphere(o, r, t_min, closest_so_far, t)) {
+                closest_so_far = t;
+                best = i;
+            }
+        }
+    }
+    out.object = best;
+    out.prim = -1;
+    if(best < 0) return false;
+    const ObjRec& o = s.objects[best];
+    const float t = closest_so_far;
+    out.t = t;
+    out.p = r.o + t * r.d;
+    if(o.kind == LRT_OBJECT_MESH) {
+        // triangle_mesh.h:80-96: face normal from the geometric cross product, then the interpolated
+        // shading normal flipped toward the ray.
+        const uint32_t ref = o.ref_base + best_mesh.ref;
+        const uint32_t tri = __ldg(s.ref_prim + ref);
+        out.prim = static_cast<int32_t>(tri);
+        const float4 b = ld_tri(s.tris + 3ull * ref + 1);
+        const float4 c = ld_tri(s.tris + 3ull * ref + 2);
+        const f3 geometric = cross(f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z});
+        const f3 outward = geometric / length(geometric);
+        out.front_face = dot(r.d, outward) < 0.0f;
+        out.normal = out.front_face ? outward : -outward;
+        const float u = best_mesh.u;
+        const float v = best_mesh.v;
+        const float b0 = 1.0f - u - v;
+        const float4* cn = s.normals + 3ull * (o.tri_base + tri);
+        const float4 n0 = __ldg(cn), n1 = __ldg(cn + 1), n2 = __ldg(cn + 2);
+        f3 shading = b0 * f3{n0.x, n0.y, n0.z} + u * f3{n1.x, n1.y, n1.z} + v * f3{n2.x, n2.y, n2.z};
+        if(length_squared(shading) > 0.0f) {
+            shading = shading / length(shading);
+            if(dot(r.d, shading) > 0.0f) shading = -shading;
+            out.normal = shading;
+        }
+    } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+        const f3 normal = load3(o.normal);
+        out.front_face = dot(r.d, normal) < 0.0f;
+        out.normal = out.front_face ? normal : -normal;
+    } else {
+        const f3 outward = (out.p - load3(o.center)) / o.radius;
+        out.front_face = dot(r.d, outward) < 0.0f;
+        out.normal = out.front_face ? outward : -outward;
+    }
+    return true;
+}
+
+// Shadow-ray query with the closest-hit semantics the path integrator needs
+// (path_integrator.h:113-115): returns the emitter index of the closest object within [t_min, t_max],
+// -1 for a non-emitting object, -2 for no hit.
+template <bool kCount>
+__device__ __forceinline__ int32_t scene_hit_emitter(const DeviceScene& s, const Ray& r, float t_min, float t_max,
+                                                     TraceCount& cnt) {
+    float closest_so_far = t_max;
+    int32_t best = -1;
+    for(int32_t i = 0; i < s.n_objects; ++i) {
+        const ObjRec& o = s.objects[i];
+        if(o.kind == LRT_OBJECT_MESH) {
+            MeshHit mh;
+            if(trace_mesh<kCount>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+                closest_so_far = mh.t;
+                best = i;
+            }
+        } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+            float t;
+            f3 p;
+            if(hit_rectangle(o, r, t_min, closest_so_far, t, p)) {
+                closest_so_far = t;
+                best = i;
+            }
+        } else {
+            float t;
+            if(hit_sphere(o, r, t_min, closest_so_far, t)) {
+                closest_so_far = t;
+                best = i;
+            }
+        }
+    }
+    if(best < 0) return -2;
+    return s.objects[best].emitter;
+}
+
+// ---- sky: env_emitter::eval (env_emitter.h:71-88) + ArHosekSkyModel_GetRadianceInternal (double) ----
+__device__ __forceinline__ double hosek_radiance(const double* cfg, double theta, double gamma) {
+    const double cos_gamma = cos(gamma);
+    const double expM = exp(cfg[4] * gamma);
+    const double rayM = cos_gamma * cos_gamma;
+    const double mieM = (1.0 + cos_gamma * cos_gamma) / pow((1.0 + cfg[8] * cfg[8] - 2.0 * cfg[8] * cos_gamma), 1.5);
+    const double zenith = sqrt(cos(theta));
+    return (1.0 + cfg[0] * exp(cfg[1] / (cos(theta) + 0.01))) *
+           (cfg[2] + cfg[3] * expM + cfg[5] * rayM + cfg[6] * mieM + cfg[7] * zenith);
+}
+
+__device__ __forceinline__ f3 env_eval(const EmitRec& e, f3 direction) {
+    const f3 dir = normalize(direction);
+    if(dir.y <= 0.0f) return mk(1.0f);
+    const float theta = acosf(sclamp(dir.y, 0.0f, 1.0f));
+    const float gamma = acosf(sclamp(dot(dir, load3(e.sun)), -1.0f, 1.0f));
+    const f3 c{static_cast<float>(hosek_radiance(e.cfg[0], theta, gamma) * e.rad[0]),
+               static_cast<float>(hosek_radiance(e.cfg[1], theta, gamma) * e.rad[1]),
+               static_cast<float>(hosek_radiance(e.cfg[2], theta, gamma) * e.rad[2])};
+    return c * e.scale;
+}
+
+// scene::eval_environment (scene.h:62-70)
+__device__ __forceinline__ f3 eval_environment(const DeviceScene& s, f3 direction) {
+    f3 emitted = mk(0.0f);
+    for(int32_t i = 0; i < s.n_emitters; ++i) {
+        if(s.emitters[i].kind == LRT_EMITTER_ENV) emitted += env_eval(s.emitters[i], direction);
+    }
+    return emitted;
+}
+
+struct DirectSample {
+    f3 direction;
+    f3 point;
+    f3 radiance;
+    float pdf;
+    float distance;
+    int32_t emitter;
+};
+
+// hittable::sample_position of the emitter's shape (rectangle.h:65-69, sphere.h:60-67)
+__device__ __forceinline__ void shape_sample_position(const ObjRec& o, float sx, float sy, f3& p, f3& n, float& pdf) {
+    if(o.kind == LRT_OBJECT_RECTANGLE) {
+        p = load3(o.corner) + sx * load3(o.edge_u) + sy * load3(o.edge_v);
+        n = load3(o.normal);
+        pdf = 1.0f / o.area;
+    } else {
+        const float z = 1.0f - 2.0f * sy;
+        const float ring = sqrtf(smax(0.0f, 1.0f - z * z));
+        const float phi = 2.0f * kPi * sx;
+        n = f3{ring * cosf(phi), ring * sinf(phi), z};
+        p = load3(o.center) + o.radius * n;
+        pdf = 1.0f / o.area;
+    }
+}
+
+// area_emitter::sample (area_emitter.h:17-49)
+__device__ __forceinline__ bool area_sample(const DeviceScene& s, const EmitRec& e, f3 shading_point, float sx,
+                                            float sy, DirectSample& out) {
+    if(e.area <= 0.0f) return false;
+    f3 p, n;
+    float pdf_area = 0.0f;
+    shape_sample_position(s.objects[e.object], sx, sy, p, n, pdf_area);
+    const f3 to_light = p - shading_point;
+    const float dist2 = length_squared(to_light);
+    if(dist2 < 1e-8f) return false;
+    const float dist = sqrtf(dist2);
+    const f3 direction = to_light / dist;
+    const float cos_light = dot(n, -direction);
+    if(cos_light <= 0.0f) return false;
+    out.point = p;
+    out.direction = direction;
+    out.distance = dist;
+    out.pdf = pdf_area * dist2 / cos_light;
+    out.radiance = load3(e.radiance);
+    return true;
+}
+
+// env_emitter::sample (env_emitter.h:33-53)
+__device__ __forceinline__ bool env_sample(const EmitRec& e, float sx, float sy, DirectSample& out) {
+    if(!e.sun_active) return false;
+    const float cos_theta = (1.0f - sx) + sx * e.cos_cutoff;
+    const float sin_theta = sqrtf(smax(0.0f, 1.0f - cos_theta * cos_theta));
+    const float phi = 2.0f * kPi * sy;
+    const f3 local{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    const f3 a0 = load3(e.frame[0]), a1 = load3(e.frame[1]), a2 = load3(e.frame[2]);
+    out.direction = a0 * local.x + a1 * local.y + a2 * local.z;
+    out.pdf = e.cone_pdf;
+    out.radiance = env_eval(e, out.direction);
+    out.distance = kInf;
+    return true;
+}
+
+// scene::sample_emitter_direction (scene.h:73-93): uniform 1/n light pick on sample.x
+__device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f3 shading_point, float sx, float sy,
+                                                         DirectSample& out) {
+    const int32_t count = s.n_emitters;
+    if(count <= 0) return false;
+    const float scaled = sx * static_cast<float>(count);
+    int32_t index = static_cast<int32_t>(scaled);
+    if(index >= count) index = count - 1;
+    const float rx = scaled - static_cast<float>(index);
+    const EmitRec& e = s.emitters[index];
+    out.distance = kInf;
+    out.pdf = 0.0f;
+    const bool ok = e.kind == LRT_EMITTER_ENV ? env_sample(e, rx, sy, out) : area_sample(s, e, shading_point, rx, sy, out);
+    if(!ok) return false;
+    out.emitter = index;
+    out.pdf *= 1.0f / static_cast<float>(count);
+    return out.pdf > 0.0f;
+}
+
+// area_emitter::pdf (area_emitter.h:51-72): re-intersects the light shape
+__device__ __forceinline__ float area_pdf(const DeviceScene& s, const EmitRec& e, f3 shading_point, f3 direction) {
+    if(e.area <= 0.0f) return 0.0f;
+    const f3 dir = normalize(direction);
+    const Ray r{shading_point, dir};
+    const ObjRec& o = s.objects[e.object];
+    float t;
+    f3 normal;
+    if(o.kind == LRT_OBJECT_RECTANGLE) {
+        f3 p;
+        if(!hit_rectangle(o, r, 0.001f, kInf, t, p)) return 0.0f;
+        normal = load3(o.normal);
+        if(!(dot(r.d, normal) < 0.0f)) return 0.0f;  // !rec.front_face
+    } else {
+        if(!hit_sphere(o, r, 0.001f, kInf, t)) return 0.0f;
+        const f3 p = r.o + t * r.d;
+        normal = (p - load3(o.center)) / o.radius;
+        if(!(dot(r.d, normal) < 0.0f)) return 0.0f;
+    }
+    const float cos_light = dot(normal, -dir);
+    if(cos_light <= 0.0f) return 0.0f;
+    return t * t / (e.area * cos_light);
+}
+
+// env_emitter::pdf (env_emitter.h:55-69)
+__device__ __forceinline__ float env_pdf(const EmitRec& e, f3 direction) {
+    if(!e.sun_active) return 0.0f;
+    const f3 dir = normalize(direction);
+    if(dot(dir, load3(e.sun)) + 1e-5f < e.cos_cutoff) return 0.0f;
+    return e.cone_pdf;
+}
+
+// scene::pdf_emitter_direction (scene.h:96-108)
+__device__ __forceinline__ float pdf_emitter_direction(const DeviceScene& s, f3 shading_point, f3 direction) {
+    const int32_t count = s.n_emitters;
+    if(count <= 0) return 0.0f;
+    const float selection = 1.0f / static_cast<float>(count);
+    float sum = 0.0f;
+    for(int32_t i = 0; i < count; ++i) {
+        const EmitRec& e = s.emitters[i];
+        const float p = e.kind == LRT_EMITTER_ENV ? env_pdf(e, direction) : area_pdf(s, e, shading_point, direction);
+        sum += selection * p;
+    }
+    return sum;
+}
+
+// area_emitter::emitted (area_emitter.h:79-85)
+__device__ __forceinline__ f3 area_emitted(const EmitRec& e, f3 normal, f3 outgoing) {
+    if(dot(normal, outgoing) <= 0.0f) return mk(0.0f);
+    return load3(e.radiance);
+}
+
+// camera::get_ray for a pinhole (camera.h:53-60)
+__device__ __forceinline__ Ray camera_ray(const CamRec& c, float s, float t) {
+    const f3 origin = load3(c.origin);
+    const f3 target = load3(c.llc) + s * load3(c.horizontal) + t * load3(c.vertical) - origin;
+    return Ray{origin, normalize(target)};
+}
+
+LRT_HD float power_heuristic(float pdf_strategy, float pdf_other) {
+    const float a = pdf_strategy * pdf_strategy;
+    const float b = pdf_other * pdf_other;
+    const float sum = a + b;
+    return sum > 0.0f ? a / sum : 0.0f;
+}
+
+}  // namespace lrt

@@ -1,0 +1,277 @@
+"""Python host binding of liblrt (ctypes over the C ABI in include/lrt.h).
+
+This is the host-side mirror of the reference's integrator/scene interfaces for tests and benchmarks:
+``Context.upload(scene)`` replaces building LinRT::scene, ``Context.render(...)`` replaces the tile loop
+of src/main.cpp around path_integrator::radiance, and the query methods expose the per-function parity
+entry points (traversal, BSDFs, sky, sampler, emitters, photons).
+
+The library is loaded from this directory (``liblrt.so``, built by ``make -C csrc``). There is no CPU
+fallback: a missing library or a missing GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+import lrt_abi as abi
+from lrt_abi import ptr
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblrt.so")
+
+# every entry point include/lrt.h declares (checked by the CPU test suite)
+EXPORTS = [
+    "lrt_create", "lrt_destroy", "lrt_last_error", "lrt_status_string", "lrt_rough_transmittance_slice",
+    "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_scene_upload", "lrt_scene_device_bytes",
+    "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_bsdf_evaluate", "lrt_sky_eval",
+    "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
+    "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
+    "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
+]
+
+
+class LrtError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (abi.STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError("liblrt.so is not built (run `make -C %s`)" % os.path.join(HERE, "csrc"))
+        L = C.CDLL(LIB_PATH)
+        vp, u32, i32, f32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_float, C.c_uint64
+        P = C.POINTER
+        L.lrt_create.argtypes = [C.c_int, vp, P(vp)]
+        L.lrt_destroy.argtypes = [vp]
+        L.lrt_last_error.restype = C.c_char_p
+        L.lrt_last_error.argtypes = [vp]
+        L.lrt_status_string.restype = C.c_char_p
+        L.lrt_status_string.argtypes = [C.c_int]
+        L.lrt_rough_transmittance_slice.argtypes = [C.c_char_p, f32, f32, P(f32), P(f32)]
+        L.lrt_fresnel_diffuse_reflectance.restype = f32
+        L.lrt_fresnel_diffuse_reflectance.argtypes = [f32]
+        L.lrt_kdtree_build.argtypes = [P(f32), P(f32), u32, P(u32), u32, P(u32), u32, P(u32), P(u32), P(u32)]
+        L.lrt_scene_upload.argtypes = [vp, P(abi.SceneDesc)]
+        L.lrt_scene_device_bytes.restype = u64
+        L.lrt_scene_device_bytes.argtypes = [vp]
+        L.lrt_mesh_tree_info.argtypes = [vp, u32, P(u32), P(u32), P(u32)]
+        L.lrt_trace.argtypes = [vp, P(abi.Ray), u32, P(abi.Hit)]
+        L.lrt_trace_dev.argtypes = [vp, vp, u32, vp]
+        L.lrt_bsdf_evaluate.argtypes = [vp, i32, P(abi.BsdfQuery), u32, P(abi.BsdfResult)]
+        L.lrt_sky_eval.argtypes = [vp, P(f32), u32, P(f32)]
+        L.lrt_sampler_values.argtypes = [vp, P(u32), u32, u32, P(f32)]
+        L.lrt_camera_rays.argtypes = [vp, u32, u32, P(u32), u32, P(abi.Ray)]
+        L.lrt_emitter_query.argtypes = [vp, P(f32), P(f32), P(f32), u32, P(f32), P(f32)]
+        L.lrt_render.argtypes = [vp, P(abi.RenderParams), P(f32)]
+        L.lrt_render_dev.argtypes = [vp, P(abi.RenderParams), vp]
+        L.lrt_render_stats_get.argtypes = [vp, P(abi.RenderStats)]
+        L.lrt_render_stats_reset.argtypes = [vp]
+        L.lrt_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
+        L.lrt_photon_trace.argtypes = [vp, i32, u32, i32, i32, P(abi.Photon), P(u32), P(u64)]
+        L.lrt_photon_trace_particles.argtypes = [vp, i32, u32, u32, i32, i32, u32, P(abi.Photon), P(u32)]
+        L.lrt_photon_map_build.argtypes = [vp, i32, P(abi.Photon), u32, f32]
+        L.lrt_photon_knn.argtypes = [vp, i32, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
+        L.lrt_photon_irradiance.argtypes = [vp, i32, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
+        _lib = L
+    return _lib
+
+
+def rough_transmittance_slice(ggx_path: str, eta: float, alpha: float):
+    table = np.zeros(abi.TRANS_SAMPLES, dtype=np.float32)
+    diffuse = C.c_float(0.0)
+    st = lib().lrt_rough_transmittance_slice(ggx_path.encode(), eta, alpha, ptr(table, C.c_float), C.byref(diffuse))
+    if st != 0:
+        raise LrtError(st, "rough transmittance slice failed")
+    return table, np.float32(diffuse.value)
+
+
+def fresnel_diffuse_reflectance(eta: float) -> np.float32:
+    return np.float32(lib().lrt_fresnel_diffuse_reflectance(eta))
+
+
+def kdtree_build(bmin: np.ndarray, bmax: np.ndarray):
+    """Host SAH kd-tree: (nodes (n,2) uint32, refs uint32, depth)."""
+    bmin = np.ascontiguousarray(bmin, dtype=np.float32)
+    bmax = np.ascontiguousarray(bmax, dtype=np.float32)
+    n = len(bmin)
+    nn, nr, depth = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+    cap_nodes, cap_refs = max(16, 8 * n), max(16, 8 * n)
+    for _ in range(4):
+        nodes = np.zeros((cap_nodes, 2), dtype=np.uint32)
+        refs = np.zeros(cap_refs, dtype=np.uint32)
+        st = lib().lrt_kdtree_build(ptr(bmin, C.c_float), ptr(bmax, C.c_float), n, ptr(nodes, C.c_uint32), cap_nodes,
+                                    ptr(refs, C.c_uint32), cap_refs, C.byref(nn), C.byref(nr), C.byref(depth))
+        if st == 0:
+            return nodes[: nn.value], refs[: nr.value], depth.value
+        if st != -5:
+            raise LrtError(st, "kd-tree build failed")
+        cap_nodes, cap_refs = nn.value, nr.value
+    raise LrtError(-5, "kd-tree build: output sizing failed")
+
+
+class Context:
+    """One liblrt context (one GPU, one CUDA stream)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.handle = C.c_void_p()
+        st = lib().lrt_create(device, C.c_void_p(stream) if stream else None, C.byref(self.handle))
+        if st != 0:
+            raise LrtError(st, "lrt_create(device=%d) failed" % device)
+        self.scene = None
+        self.holder = None
+
+    def _check(self, st):
+        if st != 0:
+            raise LrtError(st, lib().lrt_last_error(self.handle).decode())
+
+    def close(self):
+        if self.handle:
+            lib().lrt_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- scene ----
+    def upload(self, scene):
+        holder = abi.SceneHolder(scene)
+        self._check(lib().lrt_scene_upload(self.handle, C.byref(holder.desc)))
+        self.scene, self.holder = scene, holder
+        return self
+
+    def scene_bytes(self) -> int:
+        return int(lib().lrt_scene_device_bytes(self.handle))
+
+    def mesh_tree_info(self, obj: int):
+        n, r, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(lib().lrt_mesh_tree_info(self.handle, obj, C.byref(n), C.byref(r), C.byref(d)))
+        return n.value, r.value, d.value
+
+    # ---- parity queries ----
+    def trace(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
+        hits = np.zeros(len(rays), dtype=abi.HIT_DTYPE)
+        self._check(lib().lrt_trace(self.handle, ptr(rays, abi.Ray), len(rays), ptr(hits, abi.Hit)))
+        return hits
+
+    def trace_dev(self, rays_ptr: int, n: int, hits_ptr: int):
+        self._check(lib().lrt_trace_dev(self.handle, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr)))
+
+    def bsdf(self, material: int, queries: np.ndarray) -> np.ndarray:
+        queries = np.ascontiguousarray(queries, dtype=abi.BSDF_QUERY_DTYPE)
+        out = np.zeros(len(queries), dtype=abi.BSDF_RESULT_DTYPE)
+        self._check(lib().lrt_bsdf_evaluate(self.handle, material, ptr(queries, abi.BsdfQuery), len(queries),
+                                            ptr(out, abi.BsdfResult)))
+        return out
+
+    def sky(self, dirs: np.ndarray) -> np.ndarray:
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32)
+        out = np.zeros((len(dirs), 3), dtype=np.float32)
+        self._check(lib().lrt_sky_eval(self.handle, ptr(dirs, C.c_float), len(dirs), ptr(out, C.c_float)))
+        return out
+
+    def sampler_values(self, pixel_sample: np.ndarray, n_dims: int) -> np.ndarray:
+        ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
+        out = np.zeros((len(ps), n_dims), dtype=np.float32)
+        self._check(lib().lrt_sampler_values(self.handle, ptr(ps, C.c_uint32), len(ps), n_dims, ptr(out, C.c_float)))
+        return out
+
+    def camera_rays(self, width: int, height: int, pixel_sample: np.ndarray) -> np.ndarray:
+        ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
+        rays = np.zeros(len(ps), dtype=abi.RAY_DTYPE)
+        self._check(lib().lrt_camera_rays(self.handle, width, height, ptr(ps, C.c_uint32), len(ps), ptr(rays, abi.Ray)))
+        return rays
+
+    def emitter_query(self, points, u2, dirs):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        u2 = np.ascontiguousarray(u2, dtype=np.float32)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32)
+        out = np.zeros((len(points), 16), dtype=np.float32)
+        pdf = np.zeros(len(points), dtype=np.float32)
+        self._check(lib().lrt_emitter_query(self.handle, ptr(points, C.c_float), ptr(u2, C.c_float), ptr(dirs, C.c_float),
+                                            len(points), ptr(out, C.c_float), ptr(pdf, C.c_float)))
+        return out, pdf
+
+    # ---- rendering ----
+    def render(self, params: abi.RenderParams, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((params.height, params.width, 3), dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.size == params.width * params.height * 3
+        self._check(lib().lrt_render(self.handle, C.byref(params), ptr(out, C.c_float)))
+        return out
+
+    def render_dev(self, params: abi.RenderParams, rgb_ptr: int):
+        self._check(lib().lrt_render_dev(self.handle, C.byref(params), C.c_void_p(rgb_ptr)))
+
+    def set_option(self, name: str, value: int):
+        self._check(lib().lrt_set_option(self.handle, name.encode(), int(value)))
+
+    def stats(self) -> dict:
+        s = abi.RenderStats()
+        self._check(lib().lrt_render_stats_get(self.handle, C.byref(s)))
+        return {
+            "paths": s.paths, "extension_rays": s.extension_rays, "shadow_rays": s.shadow_rays,
+            "nodes_visited": s.nodes_visited, "triangles_tested": s.triangles_tested,
+            "shadow_nodes_visited": s.shadow_nodes_visited, "shadow_triangles_tested": s.shadow_triangles_tested,
+            "shading_events": s.shading_events, "kernel_launches": s.kernel_launches,
+            "stage_ms": {abi.STAGE_NAMES[i]: s.stage_ms[i] for i in range(6)},
+            "stage_launches": {abi.STAGE_NAMES[i]: s.stage_launches[i] for i in range(6)},
+        }
+
+    def reset_stats(self):
+        self._check(lib().lrt_render_stats_reset(self.handle))
+
+    # ---- photons ----
+    def photon_trace(self, kind: int, requested: int, max_depth: int, rr_depth: int):
+        photons = np.zeros(max(1, requested), dtype=abi.PHOTON_DTYPE)
+        n = C.c_uint32(0)
+        shot = C.c_uint64(0)
+        self._check(lib().lrt_photon_trace(self.handle, kind, requested, max_depth, rr_depth, ptr(photons, abi.Photon),
+                                           C.byref(n), C.byref(shot)))
+        return photons[: n.value], shot.value
+
+    def photon_trace_particles(self, kind, first, count, max_depth, rr_depth, max_per=64):
+        photons = np.zeros(count * max_per, dtype=abi.PHOTON_DTYPE)
+        counts = np.zeros(count, dtype=np.uint32)
+        self._check(lib().lrt_photon_trace_particles(self.handle, kind, first, count, max_depth, rr_depth, max_per,
+                                                     ptr(photons, abi.Photon), ptr(counts, C.c_uint32)))
+        return photons.reshape(count, max_per), counts
+
+    def photon_map_build(self, map_id: int, photons: np.ndarray, scale: float):
+        photons = np.ascontiguousarray(photons, dtype=abi.PHOTON_DTYPE)
+        self._check(lib().lrt_photon_map_build(self.handle, map_id, ptr(photons, abi.Photon), len(photons), scale))
+
+    def photon_knn(self, map_id: int, points, r2: float, k: int):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        n = len(points)
+        idx = np.full((n, k), 0xFFFFFFFF, dtype=np.uint32)
+        d2 = np.zeros((n, k), dtype=np.float32)
+        cnt = np.zeros(n, dtype=np.uint32)
+        self._check(lib().lrt_photon_knn(self.handle, map_id, ptr(points, C.c_float), n, r2, k, ptr(idx, C.c_uint32),
+                                         ptr(d2, C.c_float), ptr(cnt, C.c_uint32)))
+        return idx, d2, cnt
+
+    def photon_irradiance(self, map_id: int, points, normals, radius: float, max_depth: int, k: int):
+        points = np.ascontiguousarray(points, dtype=np.float32)
+        normals = np.ascontiguousarray(normals, dtype=np.float32)
+        out = np.zeros((len(points), 3), dtype=np.float32)
+        self._check(lib().lrt_photon_irradiance(self.handle, map_id, ptr(points, C.c_float), ptr(normals, C.c_float),
+                                                len(points), radius, max_depth, k, ptr(out, C.c_float)))
+        return out

@@ -1,0 +1,356 @@
+"""Seeded synthetic scenes of the LinRT rendering workloads.
+
+Every scene is built from plain numpy arrays (float32 positions, uint32 indices, float32 corner
+normals), so the GPU library and the reference harness receive identical inputs.
+
+* ``cornell_box``: a closed box of 10 axis-aligned quads (20 triangles, each quad its own
+  triangle_mesh), white walls 0.75, left wall (0.63, 0.06, 0.06), right wall (0.14, 0.45, 0.09), a
+  ceiling quad area light of radiance (17, 12, 4), and an icosphere subdivided 6 times (81,920
+  triangles) displaced radially by 5% with seeded 3-octave value noise, diffuse albedo 0.8.
+  ``open_box`` removes the roof and the light and lights the box with a Hosek sky (turbidity 3, sun
+  elevation 30 degrees, ground albedo 0.3); the sphere carries one of the seven materials.
+* Materials follow the reference constructors and src/main.cpp:38-47 where the workload leaves a
+  parameter open (plastic Kd, coating nests).
+
+Rough-transmittance tables and the cooked Hosek state are caller-side inputs of the library (the
+reference computes them on the host at material/emitter construction). They are read from
+``data/scene_data.json``; ``data/make_scene_data.py`` fills that file.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+import lrt_abi as abi
+
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+SCENE_DATA = os.path.join(DATA_DIR, "scene_data.json")
+
+COPPER_ETA = (0.200438, 0.924033, 1.102212)   # fresnel.h:15-20
+COPPER_K = (3.912948, 2.452847, 2.142188)
+
+SKY_TURBIDITY = 3.0
+SKY_ALBEDO = 0.3
+SKY_SCALE = 0.05            # src/main.cpp:53
+SUN_ELEVATION_DEG = 30.0
+SUN_AZIMUTH_DEG = 36.87     # horizontal direction (0.6, 0, 0.8)
+
+MATERIAL_NAMES = ["diffuse", "rough_dielectric", "rough_conductor", "plastic", "rough_plastic",
+                  "coating", "rough_coating"]
+
+
+@dataclass
+class Scene:
+    objects: list = field(default_factory=list)
+    materials: list = field(default_factory=list)
+    emitters: list = field(default_factory=list)
+    camera: dict = field(default_factory=dict)
+    name: str = ""
+
+    def triangle_count(self) -> int:
+        return sum(len(o["indices"]) // 3 for o in self.objects if o["kind"] == abi.OBJ_MESH)
+
+
+# ---------------------------------------------------------------------------------------------
+# caller-side tables (rough transmittance, cooked Hosek state)
+
+_scene_data_cache = None
+
+
+def _f32_key(*values) -> str:
+    return "_".join("%08x" % np.float32(v).view(np.uint32) for v in values)
+
+
+def load_scene_data() -> dict:
+    global _scene_data_cache
+    if _scene_data_cache is None:
+        if os.path.exists(SCENE_DATA):
+            with open(SCENE_DATA) as f:
+                _scene_data_cache = json.load(f)
+        else:
+            _scene_data_cache = {"transmittance": {}, "hosek": {}}
+    return _scene_data_cache
+
+
+def transmittance_table(eta: float, alpha: float):
+    """1-D rough-transmittance table and diffuse transmittance for (eta, alpha) as float32."""
+    key = _f32_key(eta, alpha)
+    data = load_scene_data()["transmittance"]
+    if key not in data:
+        raise KeyError("no rough-transmittance table for eta=%r alpha=%r in %s; run data/make_scene_data.py"
+                       % (float(eta), float(alpha), SCENE_DATA))
+    entry = data[key]
+    return np.array(entry["table"], dtype=np.float32), np.float32(entry["diffuse"])
+
+
+def hosek_state(sun_direction, turbidity: float, albedo: float):
+    key = _f32_key(*sun_direction, turbidity, albedo)
+    data = load_scene_data()["hosek"]
+    if key not in data:
+        raise KeyError("no cooked Hosek state for sun=%r in %s; run data/make_scene_data.py"
+                       % (tuple(map(float, sun_direction)), SCENE_DATA))
+    entry = data[key]
+    return np.array(entry["config"], dtype=np.float64).reshape(3, 9), np.array(entry["radiance"], dtype=np.float64)
+
+
+def required_tables(materials) -> list:
+    """(eta, alpha) pairs whose tables the materials need."""
+    out = []
+    for m in materials:
+        if m["type"] == abi.MAT_ROUGH_PLASTIC:
+            eta = np.float32(m["int_ior"]) / np.float32(m["ext_ior"])
+            out += [(eta, np.float32(m["alpha"])), (np.float32(1.0) / eta, np.float32(m["alpha"]))]
+        elif m["type"] == abi.MAT_ROUGH_COATING:
+            out.append((np.float32(m["int_ior"]) / np.float32(m["ext_ior"]), np.float32(m["alpha"])))
+    return out
+
+
+def attach_tables(materials) -> None:
+    """Fill trans_table / trans_internal_diffuse of rough plastic and rough coating materials."""
+    for m in materials:
+        if m["type"] == abi.MAT_ROUGH_PLASTIC:
+            eta = np.float32(m["int_ior"]) / np.float32(m["ext_ior"])
+            m["trans_table"], _ = transmittance_table(eta, m["alpha"])
+            _, m["trans_internal_diffuse"] = transmittance_table(np.float32(1.0) / eta, m["alpha"])
+        elif m["type"] == abi.MAT_ROUGH_COATING:
+            eta = np.float32(m["int_ior"]) / np.float32(m["ext_ior"])
+            m["trans_table"], _ = transmittance_table(eta, m["alpha"])
+
+
+def attach_hosek(emitters) -> None:
+    for e in emitters:
+        if e["kind"] == abi.EMITTER_ENV:
+            e["hosek_config"], e["hosek_radiance"] = hosek_state(e["sun_direction"], e["turbidity"], e["albedo"])
+
+
+def sun_direction(elevation_deg: float = SUN_ELEVATION_DEG, azimuth_deg: float = SUN_AZIMUTH_DEG):
+    el, az = math.radians(elevation_deg), math.radians(azimuth_deg)
+    return (math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az))
+
+
+# ---------------------------------------------------------------------------------------------
+# geometry
+
+def _hash3(ix, iy, iz, seed):
+    """32-bit integer lattice hash -> [-1, 1)."""
+    h = (ix.astype(np.uint32) * np.uint32(0x8DA6B343)) ^ (iy.astype(np.uint32) * np.uint32(0xD8163841)) \
+        ^ (iz.astype(np.uint32) * np.uint32(0xCB1AB31F)) ^ np.uint32(seed)
+    h ^= h >> np.uint32(16)
+    h *= np.uint32(0x7FEB352D)
+    h ^= h >> np.uint32(15)
+    h *= np.uint32(0x846CA68B)
+    h ^= h >> np.uint32(16)
+    return h.astype(np.float64) * (2.0 / 4294967296.0) - 1.0
+
+
+def value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinear lattice value noise with smoothstep weights, in [-1, 1]."""
+    fl = np.floor(p)
+    f = p - fl
+    i = fl.astype(np.int64)
+    w = f * f * (3.0 - 2.0 * f)
+    out = np.zeros(p.shape[0])
+    with np.errstate(over="ignore"):
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    v = _hash3(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed)
+                    wx = w[:, 0] if dx else 1.0 - w[:, 0]
+                    wy = w[:, 1] if dy else 1.0 - w[:, 1]
+                    wz = w[:, 2] if dz else 1.0 - w[:, 2]
+                    out += v * wx * wy * wz
+    return out
+
+
+def fbm(p: np.ndarray, seed: int, octaves: int = 3) -> np.ndarray:
+    """Octave sum with gains 1/2 and frequencies x2, normalised to [-1, 1]."""
+    total = np.zeros(p.shape[0])
+    norm = 0.0
+    amp, freq = 1.0, 1.0
+    for o in range(octaves):
+        total += amp * value_noise(p * freq, seed + 1013 * o)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+def icosphere(level: int):
+    """Unit icosphere: 20 * 4**level triangles (float64 vertices, int64 faces)."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        a, b, c = f[:, 0], f[:, 1], f[:, 2]
+        edges = np.stack([np.stack([a, b], 1), np.stack([b, c], 1), np.stack([c, a], 1)], 1).reshape(-1, 2)
+        key = np.sort(edges, axis=1)
+        uniq, inv = np.unique(key[:, 0] * (v.shape[0] + 1) + key[:, 1], return_inverse=True)
+        e0 = uniq // (v.shape[0] + 1)
+        e1 = uniq % (v.shape[0] + 1)
+        mid = v[e0] + v[e1]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        mid_idx = (inv + v.shape[0]).reshape(-1, 3)
+        v = np.concatenate([v, mid])
+        ab, bc, ca = mid_idx[:, 0], mid_idx[:, 1], mid_idx[:, 2]
+        f = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1),
+                            np.stack([ab, bc, ca], 1)])
+    return v, f
+
+
+def displaced_icosphere(level: int, center, radius: float, amplitude: float, seed: int, frequency: float = 2.0):
+    """Icosphere with radial displacement radius * (1 + amplitude * fbm(frequency * p)).
+
+    Returns float32 positions, uint32 indices and float32 corner normals (area-weighted vertex normals)."""
+    v, f = icosphere(level)
+    r = radius * (1.0 + amplitude * fbm(v * frequency, seed))
+    pos = v * r[:, None] + np.asarray(center, dtype=np.float64)[None, :]
+    p0, p1, p2 = pos[f[:, 0]], pos[f[:, 1]], pos[f[:, 2]]
+    fn = np.cross(p1 - p0, p2 - p0)
+    vn = np.zeros_like(pos)
+    for k in range(3):
+        np.add.at(vn, f[:, k], fn)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+    idx = f.reshape(-1).astype(np.uint32)
+    corner_normals = vn[f.reshape(-1)].astype(np.float32)
+    return pos.astype(np.float32), idx, corner_normals
+
+
+def quad_mesh(p0, p1, p2, p3, material: int):
+    """Two-triangle mesh (p0,p1,p2), (p0,p2,p3) with flat corner normals."""
+    pos = np.array([p0, p1, p2, p3], dtype=np.float32)
+    idx = np.array([0, 1, 2, 0, 2, 3], dtype=np.uint32)
+    n = np.cross(np.float64(pos[1]) - pos[0], np.float64(pos[2]) - pos[0])
+    n /= np.linalg.norm(n)
+    return {"kind": abi.OBJ_MESH, "material": material, "positions": pos, "indices": idx,
+            "corner_normals": np.tile(n.astype(np.float32), (6, 1))}
+
+
+# box extents: x in [-1, 1], y in [0, 2], z in [-1, 1.5]; light opening in the roof
+BOX_X, BOX_Y, BOX_Z0, BOX_Z1 = 1.0, 2.0, -1.0, 1.5
+HOLE = 0.3
+
+
+def _box_quads(white: int, red: int, green: int, roof: bool):
+    X, Y, Z0, Z1 = BOX_X, BOX_Y, BOX_Z0, BOX_Z1
+    zm = 0.25
+    quads = [
+        quad_mesh((-X, 0, Z0), (-X, 0, zm), (X, 0, zm), (X, 0, Z0), white),     # floor, back half (normal +y)
+        quad_mesh((-X, 0, zm), (-X, 0, Z1), (X, 0, Z1), (X, 0, zm), white),     # floor, front half
+        quad_mesh((-X, 0, Z0), (X, 0, Z0), (X, Y, Z0), (-X, Y, Z0), white),     # back wall (normal +z)
+        quad_mesh((-X, 0, Z1), (-X, Y, Z1), (X, Y, Z1), (X, 0, Z1), white),     # front wall (normal -z)
+        quad_mesh((-X, 0, Z0), (-X, Y, Z0), (-X, Y, Z1), (-X, 0, Z1), red),     # left wall (normal +x)
+        quad_mesh((X, 0, Z0), (X, 0, Z1), (X, Y, Z1), (X, Y, Z0), green),       # right wall (normal -x)
+    ]
+    if roof:
+        h = HOLE
+        quads += [  # roof strips around the light opening (normal -y)
+            quad_mesh((-X, Y, Z0), (X, Y, Z0), (X, Y, -h), (-X, Y, -h), white),
+            quad_mesh((-X, Y, h), (X, Y, h), (X, Y, Z1), (-X, Y, Z1), white),
+            quad_mesh((-X, Y, -h), (-h, Y, -h), (-h, Y, h), (-X, Y, h), white),
+            quad_mesh((h, Y, -h), (X, Y, -h), (X, Y, h), (h, Y, h), white),
+        ]
+    return quads
+
+
+def material_library(name: str):
+    """(materials list, index of the sphere material) for one of the seven materials; the three wall
+    materials always come first (0 white, 1 red, 2 green)."""
+    mats = [
+        {"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.75, 0.75, 0.75)},
+        {"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.63, 0.06, 0.06)},
+        {"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.14, 0.45, 0.09)},
+    ]
+    plastic = {"type": abi.MAT_PLASTIC, "int_ior": 1.49, "ext_ior": 1.000277, "specular_reflectance": (1, 1, 1),
+               "diffuse_reflectance": (0.8, 0.8, 0.5)}
+    if name == "diffuse":
+        mats.append({"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.8, 0.8, 0.8)})
+    elif name == "rough_dielectric":
+        mats.append({"type": abi.MAT_ROUGH_DIELECTRIC, "int_ior": 1.5, "ext_ior": 1.0, "alpha": 0.2})
+    elif name == "rough_conductor":
+        mats.append({"type": abi.MAT_ROUGH_CONDUCTOR, "eta": COPPER_ETA, "k": COPPER_K, "alpha": 0.1})
+    elif name == "plastic":
+        mats.append(plastic)
+    elif name == "rough_plastic":
+        mats.append({"type": abi.MAT_ROUGH_PLASTIC, "int_ior": 1.49, "ext_ior": 1.000277, "alpha": 0.15,
+                     "specular_reflectance": (1, 1, 1), "diffuse_reflectance": (0.8, 0.1, 0.05)})
+    elif name == "coating":
+        mats.append(plastic)
+        mats.append({"type": abi.MAT_COATING, "int_ior": 1.7, "ext_ior": 1.000277, "nested": len(mats) - 1,
+                     "specular_reflectance": (0.3, 0.6, 0.6)})
+    elif name == "rough_coating":
+        mats.append({"type": abi.MAT_ROUGH_DIELECTRIC, "int_ior": 1.5, "ext_ior": 1.0, "alpha": 0.05})
+        mats.append({"type": abi.MAT_ROUGH_COATING, "int_ior": 1.7, "ext_ior": 1.000277, "alpha": 0.2,
+                     "nested": len(mats) - 1})
+    elif name == "dielectric":
+        mats.append({"type": abi.MAT_DIELECTRIC, "int_ior": 1.5, "ext_ior": 1.0})
+    else:
+        raise ValueError("unknown material %r" % name)
+    return mats, len(mats) - 1
+
+
+def default_camera(aspect: float = 1.0):
+    return {"origin": (0.0, 1.0, 1.3), "look_at": (0.0, 0.55, 0.0), "up": (0.0, 1.0, 0.0), "fov": 60.0,
+            "aspect": aspect}
+
+
+SPHERE_CENTER = (0.0, 0.45, 0.0)
+SPHERE_RADIUS = 0.42
+
+
+def cornell_box(level: int = 6, seed: int = 20261203, material: str = "diffuse", aspect: float = 1.0,
+                attach: bool = True) -> Scene:
+    """Closed box + ceiling area light + displaced icosphere (diffuse 0.8 by default)."""
+    mats, sphere_mat = material_library(material)
+    objects = _box_quads(0, 1, 2, roof=True)
+    pos, idx, nrm = displaced_icosphere(level, SPHERE_CENTER, SPHERE_RADIUS, 0.05, seed)
+    objects.append({"kind": abi.OBJ_MESH, "material": sphere_mat, "positions": pos, "indices": idx,
+                    "corner_normals": nrm})
+    h = HOLE
+    light = {"kind": abi.OBJ_RECTANGLE, "material": -1, "corner": (-h, BOX_Y - 1e-3, -h),
+             "edge_u": (2 * h, 0.0, 0.0), "edge_v": (0.0, 0.0, 2 * h)}
+    objects.append(light)
+    emitters = [{"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (17.0, 12.0, 4.0)}]
+    scene = Scene(objects, mats, emitters, default_camera(aspect), name="cornell_box_%s" % material)
+    if attach:
+        attach_tables(scene.materials)
+    return scene
+
+
+def sky_emitter():
+    return {"kind": abi.EMITTER_ENV, "sun_direction": sun_direction(), "turbidity": SKY_TURBIDITY,
+            "albedo": SKY_ALBEDO, "scale": SKY_SCALE}
+
+
+def open_box(material: str = "diffuse", level: int = 6, seed: int = 20261203, aspect: float = 1.0,
+             attach: bool = True) -> Scene:
+    """The box without roof and light, open to the Hosek sky; the sphere carries `material`."""
+    mats, sphere_mat = material_library(material)
+    objects = _box_quads(0, 1, 2, roof=False)
+    pos, idx, nrm = displaced_icosphere(level, SPHERE_CENTER, SPHERE_RADIUS, 0.05, seed)
+    objects.append({"kind": abi.OBJ_MESH, "material": sphere_mat, "positions": pos, "indices": idx,
+                    "corner_normals": nrm})
+    emitters = [sky_emitter()]
+    scene = Scene(objects, mats, emitters, default_camera(aspect), name="open_box_%s" % material)
+    if attach:
+        attach_tables(scene.materials)
+        attach_hosek(scene.emitters)
+    return scene
+
+
+# workloads -----------------------------------------------------------------------------------
+
+CONFIG0 = {"width": 256, "height": 256, "spp": 16, "max_depth": 6, "rr_depth": 3}
+CONFIG1 = {"width": 512, "height": 512, "spp": 64, "max_depth": 8, "rr_depth": 3,
+           "photons": 1_000_000, "k": 64}
+
+
+def render_params(width, height, spp, max_depth, rr_depth, sample_offset=0, row_begin=0, row_end=0):
+    return abi.RenderParams(width, height, spp, max_depth, rr_depth, sample_offset, row_begin, row_end)

@@ -1,0 +1,55 @@
+"""Writes ray-tracing_b200/data/scene_data.json: the caller-side inputs the workload scenes need.
+
+* rough-transmittance 1-D tables for every (eta, alpha) the seven materials use, sliced from the
+  reference's ggx.dat by liblrt's own host routine (lrt_rough_transmittance_slice, which the CPU tests
+  check bit for bit against the reference's rough_transmittance);
+* the cooked RGB Hosek-Wilkie state of the workload sky, from the reference's vendored Hosek model
+  (arhosek_rgb_skymodelstate_alloc_init through the oracle build), which a reference-side caller would
+  read from its env_emitter.
+
+Run from the repository root after `make -C oracle ref` and `make -C ray-tracing_b200/csrc`:
+    python tests/golden/make_scene_data.py
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "ray-tracing_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import lrt  # noqa: E402
+import oracle  # noqa: E402
+import scenes  # noqa: E402
+
+
+def main():
+    data = {"transmittance": {}, "hosek": {},
+            "note": "caller-side inputs of the workload scenes; made by tests/golden/make_scene_data.py"}
+    pairs = []
+    for name in scenes.MATERIAL_NAMES:
+        mats, _ = scenes.material_library(name)
+        pairs += scenes.required_tables(mats)
+    for eta, alpha in pairs:
+        key = scenes._f32_key(eta, alpha)
+        if key in data["transmittance"]:
+            continue
+        table, diffuse = lrt.rough_transmittance_slice(oracle.GGX_PATH, float(eta), float(alpha))
+        data["transmittance"][key] = {"eta": float(eta), "alpha": float(alpha),
+                                      "table": [float(x) for x in table], "diffuse": float(diffuse)}
+    sky = scenes.sky_emitter()
+    key = scenes._f32_key(*sky["sun_direction"], sky["turbidity"], sky["albedo"])
+    cfg, rad = oracle.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
+    data["hosek"][key] = {"sun_direction": [float(np.float32(v)) for v in sky["sun_direction"]],
+                          "turbidity": sky["turbidity"], "albedo": sky["albedo"],
+                          "config": [float(x) for x in cfg.reshape(-1)], "radiance": [float(x) for x in rad]}
+    os.makedirs(scenes.DATA_DIR, exist_ok=True)
+    with open(scenes.SCENE_DATA, "w") as f:
+        json.dump(data, f, indent=1)
+    print("wrote", scenes.SCENE_DATA, len(data["transmittance"]), "tables,", len(data["hosek"]), "sky states")
+
+
+if __name__ == "__main__":
+    main()

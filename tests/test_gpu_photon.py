@@ -1,0 +1,138 @@
+"""Photon mapper parity: per-particle photon traces, the photon-gather cut and count semantics, the
+k-nearest-photon sets (bit-exact, photon identity) and the irradiance estimate."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_close
+
+import lrt_abi as abi
+import oracle
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("material", ["diffuse", "coating", "rough_dielectric"])
+@pytest.mark.parametrize("kind", [abi.GATHER_SURFACE, abi.GATHER_CAUSTIC])
+def test_trace_particles_golden(ctx, material, kind):
+    g = golden("photon_kat.npz")
+    ctx.upload(scenes.cornell_box(material=material))
+    ph, cnt = ctx.photon_trace_particles(kind, 0, 2048, 8, 5, max_per=16)
+    ref_ph = g["%s_%d_photons" % (material, kind)]
+    ref_cnt = g["%s_%d_counts" % (material, kind)]
+    same = cnt == ref_cnt
+    assert same.mean() >= 0.99, "photon counts differ for %.3f of particles" % (1 - same.mean())
+    # particles whose paths agree step for step: every stored photon matches within FP32 rounding
+    # accumulated over the bounces
+    for i in np.nonzero(same)[0]:
+        n = min(int(cnt[i]), 16)
+        a, b = ph[i, :n], ref_ph[i, :n]
+        if n == 0:
+            continue
+        assert np.array_equal(a["depth"], b["depth"])
+        ok = rel_close(a["position"], b["position"], 1e-3, 1e-4).all() and rel_close(a["power"], b["power"], 1e-3, 1e-6).all()
+        if not ok:  # a path that diverged late: allowed only for a handful
+            same[i] = False
+    assert same.mean() >= 0.98
+
+
+def test_photon_gather_semantics(ctx):
+    """photons in particle-index order, cut at `requested`; shot counts particles as photon_gather does
+    with one worker"""
+    ctx.upload(scenes.cornell_box(material="diffuse", level=3))
+    requested = 1600
+    ph, shot = ctx.photon_trace(abi.GATHER_SURFACE, requested, 8, 5)
+    assert len(ph) == requested
+    all_ph, cnt = ctx.photon_trace_particles(abi.GATHER_SURFACE, 0, 8192, 8, 5, max_per=16)
+    flat = np.concatenate([all_ph[i, : cnt[i]] for i in range(len(cnt))])
+    assert np.array_equal(ph.view(np.uint8), flat[:requested].view(np.uint8))
+    # expected shot (photon_gather.h:65-97 with one worker): work items of requested/16 particles
+    g = requested // 16
+    stored, shot_ref, returned = 0, 0, 0
+    b = 0
+    while returned < requested:
+        counted, full = 0, False
+        for i in range(b * g, (b + 1) * g):
+            returned += int(cnt[i])
+            if full:
+                continue
+            counted += 1
+            if cnt[i] > 0 and stored >= requested:
+                full = True  # its first photon finds the vector full
+                continue
+            if stored + int(cnt[i]) > requested:
+                stored, full = requested, True  # cut inside this particle
+            else:
+                stored += int(cnt[i])
+        shot_ref += counted
+        b += 1
+    assert shot == shot_ref
+
+
+def test_photon_trace_no_emitters(ctx):
+    """the sky cannot emit photons (env_emitter.h:96-98): nothing is stored and the gather gives up"""
+    ctx.upload(scenes.open_box(level=1))
+    ph, shot = ctx.photon_trace(abi.GATHER_SURFACE, 1000, 8, 5)
+    assert len(ph) == 0
+
+
+@pytest.mark.parametrize("k", [16, 64, 100])
+def test_knn_sets_bit_exact(ctx, k):
+    g = golden("knn_kat.npz")
+    ctx.upload(scenes.cornell_box(level=1))
+    ctx.photon_map_build(0, g["photons"], 1.0 / 7777.0)
+    r2 = {16: 0.0025, 64: 0.01, 100: 0.04}[k]
+    idx, d2, cnt = ctx.photon_knn(0, g["points"], r2, k)
+    ref_idx, ref_d2, ref_cnt = g["idx_%d" % k], g["d2_%d" % k], g["cnt_%d" % k]
+    assert np.array_equal(cnt, ref_cnt)
+    ties = 0
+    for q in range(len(cnt)):
+        a = dict(zip(idx[q, : cnt[q]].tolist(), d2[q, : cnt[q]].tolist()))
+        b = dict(zip(ref_idx[q, : cnt[q]].tolist(), ref_d2[q, : cnt[q]].tolist()))
+        if set(a) != set(b):
+            # only allowed when the boundary distance is tied
+            ties += 1
+            assert np.float32(max(a.values())) == np.float32(max(b.values()))
+            continue
+        for i, v in a.items():
+            assert np.float32(v).view(np.uint32) == np.float32(b[i]).view(np.uint32)
+    assert ties <= 2
+
+
+def test_knn_random_vs_reference(ctx):
+    if not oracle.reference_available():
+        pytest.skip("reference oracle not built")
+    rng = np.random.default_rng(5)
+    n = 200000
+    photons = np.zeros(n, dtype=abi.PHOTON_DTYPE)
+    photons["position"] = rng.random((n, 3)).astype(np.float32)
+    photons["direction"] = [0, -1, 0]
+    photons["normal"] = [0, 1, 0]
+    photons["power"] = 1.0
+    photons["depth"] = 2
+    q = rng.random((2000, 3)).astype(np.float32)
+    ctx.upload(scenes.cornell_box(level=1))
+    ctx.photon_map_build(1, photons, 1.0)
+    idx, d2, cnt = ctx.photon_knn(1, q, 0.0004, 64)
+    ridx, rd2, rcnt = oracle.RefPhotonMap(photons).knn(q, 0.0004, 64)
+    assert np.array_equal(cnt, rcnt)
+    for i in range(len(q)):
+        assert set(idx[i, : cnt[i]].tolist()) == set(ridx[i, : cnt[i]].tolist())
+
+
+@pytest.mark.parametrize("k,radius,depth", [(64, 0.05, 6), (100, 0.1, 4)])
+def test_irradiance_golden(ctx, k, radius, depth):
+    g = golden("knn_kat.npz")
+    ctx.upload(scenes.cornell_box(level=1))
+    ctx.photon_map_build(0, g["photons"], 1.0 / 7777.0)
+    out = ctx.photon_irradiance(0, g["points"], g["normals"], radius, depth, k)
+    assert rel_close(out, g["irr_%d" % k], 1e-5, 1e-9).all()
+
+
+def test_empty_map(ctx):
+    ctx.upload(scenes.cornell_box(level=1))
+    ctx.photon_map_build(2, np.zeros(0, dtype=abi.PHOTON_DTYPE), 1.0)
+    idx, d2, cnt = ctx.photon_knn(2, np.zeros((3, 3), np.float32), 1.0, 8)
+    assert np.all(cnt == 0)
+    out = ctx.photon_irradiance(2, np.zeros((3, 3), np.float32), np.ones((3, 3), np.float32), 0.1, 5, 8)
+    assert np.all(out == 0)

@@ -1,0 +1,152 @@
+"""CPU tests of liblrt's host side: the library loads and exports every C-ABI entry point, and the host
+restatements (SAH kd-tree build, ggx.dat slicing, Fdr quadrature, Sobol table) match the reference.
+No GPU work is launched here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+import lrt
+import lrt_abi as abi
+import oracle
+import scenes
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "lrt.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|float|uint64_t|const char\*)\s+(lrt_\w+)\s*\(", text, re.M)))
+
+
+def test_header_matches_binding_list():
+    assert header_symbols() == sorted(lrt.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = lrt.lib()
+    for name in header_symbols():
+        assert hasattr(L, name), name
+
+
+def test_status_strings():
+    L = lrt.lib()
+    L.lrt_status_string.restype = C.c_char_p
+    for code, name in abi.STATUS_NAMES.items():
+        assert L.lrt_status_string(code).decode() == name
+
+
+def test_create_without_gpu_reports_no_device():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    h = C.c_void_p()
+    assert lrt.lib().lrt_create(0, None, C.byref(h)) == -9  # LRT_ERR_NO_DEVICE
+
+
+def _tri_bounds(level):
+    pos, idx, _ = scenes.displaced_icosphere(level, scenes.SPHERE_CENTER, scenes.SPHERE_RADIUS, 0.05, 20261203)
+    tri = pos[idx.reshape(-1, 3)]
+    return tri.min(axis=1).astype(np.float32), tri.max(axis=1).astype(np.float32)
+
+
+def _ref_tree(bmin, bmax):
+    lib = oracle.ref_lib()
+    lib.ref_kdtree_packed.restype = C.c_int32
+    cap = 8 * len(bmin) + 16
+    rn = np.zeros((cap, 2), np.uint32)
+    rr = np.zeros(cap, np.uint32)
+    nn, nr = C.c_uint32(), C.c_uint32()
+    assert lib.ref_kdtree_packed(abi.ptr(bmin, C.c_float), abi.ptr(bmax, C.c_float), len(bmin), abi.ptr(rn, C.c_uint32),
+                                 cap, abi.ptr(rr, C.c_uint32), cap, C.byref(nn), C.byref(nr)) == 0
+    return rn[: nn.value], rr[: nr.value]
+
+
+needs_ref = pytest.mark.skipif(not oracle.reference_available(), reason="reference oracle not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("level", [2, 4, 5])
+def test_kdtree_identical_to_reference(level):
+    bmin, bmax = _tri_bounds(level)
+    nodes, refs, depth = lrt.kdtree_build(bmin, bmax)
+    rn, rr = _ref_tree(bmin, bmax)
+    assert np.array_equal(nodes, rn)
+    assert np.array_equal(refs, rr)
+    assert depth <= 48
+
+
+@needs_ref
+def test_kdtree_degenerate_and_planar_boxes():
+    rng = np.random.default_rng(7)
+    n = 3000
+    lo = rng.random((n, 3)).astype(np.float32)
+    hi = lo + rng.random((n, 3)).astype(np.float32) * 0.05
+    hi[::5, 1] = lo[::5, 1]            # planar in y
+    hi[::7] = lo[::7]                  # points
+    lo[::11, 0] = np.float32(0.5)      # many events on one plane
+    hi[::11, 0] = np.float32(0.5)
+    nodes, refs, _ = lrt.kdtree_build(lo, hi)
+    rn, rr = _ref_tree(lo, hi)
+    assert np.array_equal(nodes, rn) and np.array_equal(refs, rr)
+
+
+def test_kdtree_small_inputs():
+    nodes, refs, depth = lrt.kdtree_build(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32))
+    assert len(nodes) == 1 and len(refs) == 0
+    nodes, refs, depth = lrt.kdtree_build(np.zeros((3, 3), np.float32), np.ones((3, 3), np.float32))
+    assert len(nodes) == 1 and list(refs) == [0, 1, 2] and (nodes[0, 1] & 3) == 3
+
+
+@needs_ref
+@pytest.mark.parametrize("eta,alpha", [(1.49 / 1.000277, 0.15), (1.000277 / 1.49, 0.15), (1.7 / 1.000277, 0.2),
+                                       (1.5, 0.05), (1.2, 0.9), (0.8, 2.0), (3.9, 0.001)])
+def test_rough_transmittance_slice_bit_exact(eta, alpha):
+    eta, alpha = np.float32(eta), np.float32(alpha)
+    a, da = lrt.rough_transmittance_slice(oracle.GGX_PATH, eta, alpha)
+    b, db = oracle.rough_transmittance(eta, alpha)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.float32(da).view(np.uint32) == np.float32(db).view(np.uint32)
+
+
+@needs_ref
+def test_rough_transmittance_errors():
+    with pytest.raises(lrt.LrtError) as e:
+        lrt.rough_transmittance_slice(oracle.GGX_PATH, 1.5, 5.0)
+    assert e.value.status == -5
+    with pytest.raises(lrt.LrtError) as e:
+        lrt.rough_transmittance_slice("/nonexistent/ggx.dat", 1.5, 0.1)
+    assert e.value.status == -4
+
+
+@needs_ref
+@pytest.mark.parametrize("eta", [1 / 1.49, 1.000277 / 1.49, 1.5, 1 / 1.7, 2.4, 1.01])
+def test_fdr_matches_reference(eta):
+    assert lrt.fresnel_diffuse_reflectance(eta) == oracle.fresnel_diffuse_reflectance(eta)
+
+
+def test_scene_data_covers_workload_materials():
+    for name in scenes.MATERIAL_NAMES:
+        scenes.open_box(name, level=1)
+        scenes.cornell_box(level=1, material=name)
+
+
+@needs_ref
+def test_scene_data_tables_match_slicing():
+    data = scenes.load_scene_data()["transmittance"]
+    for entry in data.values():
+        a, d = lrt.rough_transmittance_slice(oracle.GGX_PATH, np.float32(entry["eta"]), np.float32(entry["alpha"]))
+        assert np.array_equal(a, np.array(entry["table"], np.float32)) and d == np.float32(entry["diffuse"])
+
+
+@needs_ref
+def test_scene_data_hosek_matches_reference():
+    sky = scenes.sky_emitter()
+    cfg, rad = scenes.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
+    rcfg, rrad = oracle.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
+    assert np.array_equal(cfg, rcfg) and np.array_equal(rad, rrad)
