@@ -300,6 +300,10 @@ int lrt_mesh_tree_info(const lrt_context* ctx, uint32_t object, uint32_t* nodes,
 int lrt_trace(lrt_context* ctx, const lrt_ray* rays, uint32_t n, lrt_hit* hits);
 int lrt_trace_dev(lrt_context* ctx, const lrt_ray* rays_dev, uint32_t n, lrt_hit* hits_dev);
 
+/* shadow-ray test of path_integrator.h:113-115 towards emitter `light`: blocked[i] = 1 when the
+ * closest hit in [t_min, t_max] exists and is not that emitter's shape */
+int lrt_occluded(lrt_context* ctx, const lrt_ray* rays, uint32_t n, int32_t light, uint8_t* blocked);
+
 /* BSDF sample + eval + pdf of material `material` for each query (parity) */
 int lrt_bsdf_evaluate(lrt_context* ctx, int32_t material, const lrt_bsdf_query* q, uint32_t n,
                       lrt_bsdf_result* out);

@@ -63,6 +63,15 @@ __global__ void k_trace(DeviceScene s, const lrt_ray* rays, uint32_t n, lrt_hit*
     hits[i] = out;
 }
 
+// shadow-ray occlusion as the path tracer evaluates it (early-exit any-hit unless the light is reachable)
+__global__ void k_occluded(DeviceScene s, const lrt_ray* rays, uint32_t n, int32_t light, uint8_t* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const lrt_ray in = rays[i];
+    TraceCount cnt{0, 0};
+    out[i] = scene_occluded<false>(s, Ray{load3(in.origin), load3(in.direction)}, in.t_min, in.t_max, light, cnt) ? 1 : 0;
+}
+
 __global__ void k_bsdf(DeviceScene s, int32_t mid, const lrt_bsdf_query* q, uint32_t n, lrt_bsdf_result* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
@@ -387,9 +396,8 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs a, int depth) {
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 o = a.sh_o[i], d = a.sh_d[i], c = a.sh_c[i];
         const int32_t light = __float_as_int(d.w);
-        const int32_t e = scene_hit_emitter<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, o.w, cnt);
+        const bool blocked = scene_occluded<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, o.w, light, cnt);
         ++rays;
-        const bool blocked = e != -2 && e != light;
         if(!blocked) {
             const uint32_t pid = __float_as_uint(c.w);
             float4 L = a.L[pid];
@@ -766,6 +774,24 @@ int lrt_trace(lrt_context* ctx, const lrt_ray* rays, uint32_t n, lrt_hit* hits) 
     const int st = lrt_trace_dev(ctx, dr, n, dh);
     if(st != LRT_OK) return st;
     LRT_CUDA(ctx, cudaMemcpyAsync(hits, dh, sizeof(lrt_hit) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+int lrt_occluded(lrt_context* ctx, const lrt_ray* rays, uint32_t n, int32_t light, uint8_t* blocked) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(light < 0 || light >= ctx->ds.n_emitters) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "emitter out of range");
+    if(n == 0) return LRT_OK;
+    if(!rays || !blocked) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t rb = sizeof(lrt_ray) * static_cast<size_t>(n);
+    LRT_CUDA(ctx, ctx->scratch_a.ensure(rb + n));
+    char* base = ctx->scratch_a.as<char>();
+    LRT_CUDA(ctx, cudaMemcpyAsync(base, rays, rb, cudaMemcpyHostToDevice, ctx->stream));
+    k_occluded<<<blocks_for(n), kBlock, 0, ctx->stream>>>(ctx->ds, reinterpret_cast<lrt_ray*>(base), n, light,
+                                                          reinterpret_cast<uint8_t*>(base + rb));
+    LRT_CUDA(ctx, cudaGetLastError());
+    LRT_CUDA(ctx, cudaMemcpyAsync(blocked, base + rb, n, cudaMemcpyDeviceToHost, ctx->stream));
     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return LRT_OK;
 }

@@ -76,15 +76,45 @@ struct MeshHit {
     uint32_t ref;  // leaf reference of the last accepted triangle
 };
 
-// sah_kdtree::intersect over one mesh's tree with the triangle_mesh::hit leaf callback.
-template <bool kCount>
+// Conservative object cull: false only when the ray's [t_min, t_max] interval cannot reach the mesh's
+// bounding box grown by 1e-3 (+ 1e-4 relative), so no triangle of the mesh can be accepted and its
+// traversal would test nothing that hits. Directions with a zero component are handled per slab.
+__device__ __forceinline__ bool ray_may_hit_box(const ObjRec& o, const Ray& r, float t_min, float t_max) {
+    float tn = t_min, tf = t_max;
+#pragma unroll
+    for(int a = 0; a < 3; ++a) {
+        const float lo = o.bmin[a], hi = o.bmax[a];
+        const float pad = 1e-3f + 1e-4f * (fabsf(lo) + fabsf(hi));
+        const float oa = comp(r.o, a), da = comp(r.d, a);
+        if(da == 0.0f) {
+            if(oa < lo - pad || oa > hi + pad) return false;
+            continue;
+        }
+        const float inv = 1.0f / da;
+        float t0 = (lo - pad - oa) * inv;
+        float t1 = (hi + pad - oa) * inv;
+        if(t0 > t1) {
+            const float t = t0;
+            t0 = t1;
+            t1 = t;
+        }
+        tn = fmaxf(tn, t0 - 1e-4f * fabsf(t0));
+        tf = fminf(tf, t1 + 1e-4f * fabsf(t1));
+    }
+    return !(tn > tf);
+}
+
+// sah_kdtree::intersect over one mesh's tree with the triangle_mesh::hit leaf callback, written as
+// a descend loop and a leaf loop (same node and triangle order as the reference's single loop, fewer
+// divergent branches per warp). kAny: stop at the first accepted triangle (occlusion queries).
+template <bool kCount, bool kAny>
 __device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o, const Ray& r, float t_min, float t_max,
                                            MeshHit& h, TraceCount& cnt) {
     const uint2* nodes = s.nodes + o.node_base;
     const float4* tris = s.tris + 3ull * o.ref_base;
     float closest = t_max;
     bool hit_any = false;
-    const float inv_d[3] = {1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
+    const float inv_x = 1.0f / r.d.x, inv_y = 1.0f / r.d.y, inv_z = 1.0f / r.d.z;
     struct Item {
         uint32_t node;
         float mint, maxt;
@@ -95,55 +125,59 @@ __device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o
     float maxt = closest;
     uint32_t node = 0;
     while(true) {
-        if(closest < mint) break;
-        const uint2 n = ld_node(nodes + node);
-        if(kCount) ++cnt.nodes;
-        if((n.y & 3u) == kLeafTag) {
-            const uint32_t count = n.y >> 2;
-            const uint32_t first = n.x;
-            float limit = smin(maxt, closest);
-            for(uint32_t i = 0; i < count; ++i) {
-                if(kCount) ++cnt.tris;
-                float u, v;
-                if(hit_tri_record(tris + 3ull * (first + i), r, mint, limit, closest, u, v)) {
-                    hit_any = true;
-                    h.t = closest;
-                    h.u = u;
-                    h.v = v;
-                    h.ref = first + i;
+        uint2 n;
+        // descend through interior nodes until a leaf (sah_kdtree.h:105-120)
+        while(true) {
+            if(closest < mint) return hit_any;
+            n = ld_node(nodes + node);
+            if(kCount) ++cnt.nodes;
+            if((n.y & 3u) == kLeafTag) break;
+            const uint32_t axis = n.y & 3u;
+            const float split = __uint_as_float(n.x);
+            const float o_a = comp(r.o, axis);
+            const float d_a = comp(r.d, axis);
+            const float t_plane = (split - o_a) * (axis == 0 ? inv_x : (axis == 1 ? inv_y : inv_z));
+            const bool left_of_split = o_a < split || (o_a == split && d_a <= 0.0f);
+            const uint32_t right = n.y >> 2;
+            const uint32_t first_child = left_of_split ? node + 1 : right;
+            const uint32_t second_child = left_of_split ? right : node + 1;
+            if(t_plane > maxt || t_plane <= 0.0f) {
+                node = first_child;
+            } else if(t_plane < mint) {
+                node = second_child;
+            } else {
+                if(top < kStackSize) {
+                    stack[top].node = second_child;
+                    stack[top].mint = t_plane;
+                    stack[top].maxt = maxt;
+                    ++top;
                 }
-                limit = smin(maxt, closest);
+                node = first_child;
+                maxt = t_plane;
             }
-            if(top == 0) break;
-            --top;
-            node = stack[top].node;
-            mint = stack[top].mint;
-            maxt = stack[top].maxt;
-            continue;
         }
-        const uint32_t axis = n.y & 3u;
-        const float split = __uint_as_float(n.x);
-        const float o_a = comp(r.o, axis);
-        const float d_a = comp(r.d, axis);
-        const float t_plane = (split - o_a) * (axis == 0 ? inv_d[0] : (axis == 1 ? inv_d[1] : inv_d[2]));
-        const bool left_of_split = o_a < split || (o_a == split && d_a <= 0.0f);
-        const uint32_t right = n.y >> 2;
-        const uint32_t first_child = left_of_split ? node + 1 : right;
-        const uint32_t second_child = left_of_split ? right : node + 1;
-        if(t_plane > maxt || t_plane <= 0.0f) {
-            node = first_child;
-        } else if(t_plane < mint) {
-            node = second_child;
-        } else {
-            if(top < kStackSize) {
-                stack[top].node = second_child;
-                stack[top].mint = t_plane;
-                stack[top].maxt = maxt;
-                ++top;
+        // leaf: the callback for each triangle with (mint, min(maxt, closest)) (sah_kdtree.h:86-93)
+        const uint32_t count = n.y >> 2;
+        const uint32_t first = n.x;
+        float limit = smin(maxt, closest);
+        for(uint32_t i = 0; i < count; ++i) {
+            if(kCount) ++cnt.tris;
+            float u, v;
+            if(hit_tri_record(tris + 3ull * (first + i), r, mint, limit, closest, u, v)) {
+                hit_any = true;
+                h.t = closest;
+                h.u = u;
+                h.v = v;
+                h.ref = first + i;
+                if(kAny) return true;
             }
-            node = first_child;
-            maxt = t_plane;
+            limit = smin(maxt, closest);
         }
+        if(top == 0) break;
+        --top;
+        node = stack[top].node;
+        mint = stack[top].mint;
+        maxt = stack[top].maxt;
     }
     return hit_any;
 }
@@ -207,7 +241,8 @@ __device__ __forceinline__ bool scene_hit(const DeviceScene& s, const Ray& r, fl
         const ObjRec& o = s.objects[i];
         if(o.kind == LRT_OBJECT_MESH) {
             MeshHit mh;
-            if(trace_mesh<kCount>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+            if(ray_may_hit_box(o, r, t_min, closest_so_far) &&
+               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt)) {
                 closest_so_far = mh.t;
                 best = i;
                 best_mesh = mh;
@@ -281,7 +316,8 @@ __device__ __forceinline__ int32_t scene_hit_emitter(const DeviceScene& s, const
         const ObjRec& o = s.objects[i];
         if(o.kind == LRT_OBJECT_MESH) {
             MeshHit mh;
-            if(trace_mesh<kCount>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+            if(ray_may_hit_box(o, r, t_min, closest_so_far) &&
+               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt)) {
                 closest_so_far = mh.t;
                 best = i;
             }
@@ -302,6 +338,43 @@ __device__ __forceinline__ int32_t scene_hit_emitter(const DeviceScene& s, const
     }
     if(best < 0) return -2;
     return s.objects[best].emitter;
+}
+
+// Shadow test of path_integrator.h:113-115: blocked = (closest hit exists) && (its emitter != light).
+// When the light's own shape cannot be hit within [t_min, t_max] (always the case for the sky), the
+// closest hit is never the light, so blocked == "any object has an accepted hit": objects are tested
+// in list order and each traversal stops at its first accepted triangle. Otherwise the closest-hit
+// query decides.
+template <bool kCount>
+__device__ __forceinline__ bool scene_occluded(const DeviceScene& s, const Ray& r, float t_min, float t_max,
+                                               int32_t light, TraceCount& cnt) {
+    const EmitRec& e = s.emitters[light];
+    if(e.kind == LRT_EMITTER_AREA) {
+        const ObjRec& lo = s.objects[e.object];
+        float t;
+        f3 p;
+        const bool light_reachable = lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, r, t_min, t_max, t, p)
+                                                                      : hit_sphere(lo, r, t_min, t_max, t);
+        if(light_reachable) {
+            const int32_t hit = scene_hit_emitter<kCount>(s, r, t_min, t_max, cnt);
+            return hit != -2 && hit != light;
+        }
+    }
+    for(int32_t i = 0; i < s.n_objects; ++i) {
+        const ObjRec& o = s.objects[i];
+        if(o.kind == LRT_OBJECT_MESH) {
+            MeshHit mh;
+            if(ray_may_hit_box(o, r, t_min, t_max) && trace_mesh<kCount, true>(s, o, r, t_min, t_max, mh, cnt)) return true;
+        } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+            float t;
+            f3 p;
+            if(hit_rectangle(o, r, t_min, t_max, t, p)) return true;
+        } else {
+            float t;
+            if(hit_sphere(o, r, t_min, t_max, t)) return true;
+        }
+    }
+    return false;
 }
 
 // ---- sky: env_emitter::eval (env_emitter.h:71-88) + ArHosekSkyModel_GetRadianceInternal (double) ----

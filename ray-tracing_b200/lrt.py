@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(HERE, "liblrt.so")
 EXPORTS = [
     "lrt_create", "lrt_destroy", "lrt_last_error", "lrt_status_string", "lrt_rough_transmittance_slice",
     "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_scene_upload", "lrt_scene_device_bytes",
-    "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_bsdf_evaluate", "lrt_sky_eval",
+    "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
@@ -65,6 +65,7 @@ def lib():
         L.lrt_mesh_tree_info.argtypes = [vp, u32, P(u32), P(u32), P(u32)]
         L.lrt_trace.argtypes = [vp, P(abi.Ray), u32, P(abi.Hit)]
         L.lrt_trace_dev.argtypes = [vp, vp, u32, vp]
+        L.lrt_occluded.argtypes = [vp, P(abi.Ray), u32, i32, P(C.c_uint8)]
         L.lrt_bsdf_evaluate.argtypes = [vp, i32, P(abi.BsdfQuery), u32, P(abi.BsdfResult)]
         L.lrt_sky_eval.argtypes = [vp, P(f32), u32, P(f32)]
         L.lrt_sampler_values.argtypes = [vp, P(u32), u32, u32, P(f32)]
@@ -170,6 +171,12 @@ class Context:
         hits = np.zeros(len(rays), dtype=abi.HIT_DTYPE)
         self._check(lib().lrt_trace(self.handle, ptr(rays, abi.Ray), len(rays), ptr(hits, abi.Hit)))
         return hits
+
+    def occluded(self, rays: np.ndarray, light: int) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
+        out = np.zeros(len(rays), dtype=np.uint8)
+        self._check(lib().lrt_occluded(self.handle, ptr(rays, abi.Ray), len(rays), light, ptr(out, C.c_uint8)))
+        return out
 
     def trace_dev(self, rays_ptr: int, n: int, hits_ptr: int):
         self._check(lib().lrt_trace_dev(self.handle, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr)))

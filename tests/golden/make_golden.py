@@ -121,7 +121,9 @@ def material_zoo():
     ]
     scenes.attach_tables(mats)
     quad = scenes.quad_mesh((-1, 0, -1), (-1, 0, 1), (1, 0, 1), (1, 0, -1), 0)
-    return scenes.Scene([quad], mats, [scenes.sky_emitter()], scenes.default_camera(), name="material_zoo")
+    emitters = [scenes.sky_emitter()]
+    scenes.attach_hosek(emitters)
+    return scenes.Scene([quad], mats, emitters, scenes.default_camera(), name="material_zoo")
 
 
 def bsdf_queries(rng, n):
