@@ -324,6 +324,16 @@ int lrt_emitter_query(lrt_context* ctx, const float* points, const float* u2, co
 /* path-traced image: rgb is width*height*3 floats, row-major from row 0 (as src/main.cpp) */
 int lrt_render(lrt_context* ctx, const lrt_render_params* params, float* rgb);
 int lrt_render_dev(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev);
+/* Allocation-free lrt_render_dev (no counterpart in the reference). For callers that must not have a
+ * library call cudaMalloc: a cudaMalloc can synchronise the whole device, which a frame loop sharing the
+ * GPU with other streams cannot afford, and it fails where the device memory is already committed to a
+ * caching allocator or a fixed budget. This entry point allocates nothing: its path state lives in one
+ * 32 MiB file-scope device array that every GPU loading the library holds until exit; the caller
+ * passes the output buffer and has uploaded the scene. Limits: max_depth <= 64 (LRT_ERR_RANGE beyond).
+ * Its first call on a device looks the array up (cudaGetSymbolAddress) and should come before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race. */
+int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev);
+
 /* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
 int lrt_render_stats_reset(lrt_context* ctx);

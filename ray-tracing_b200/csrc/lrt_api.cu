@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -939,3 +940,147 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
 }
 
 }  // extern "C"
+
+// ================================ allocation-free render ================================
+//
+// lrt_render_dev_noalloc renders with the same kernels as lrt_render_dev, but its wavefront state lives
+// in one fixed device array of this file instead of memory the library allocates. It serves callers
+// that cannot let a library call cudaMalloc: a cudaMalloc may synchronise the whole device (a stall a
+// frame loop sharing the GPU with other streams cannot take), and it fails in processes whose device
+// memory is already committed -- to a framework's caching allocator, or to a fixed budget reserved at
+// start-up. Those callers pass their own output buffer and keep the scene uploaded beforehand.
+//
+// The array is a file-scope __device__ variable: every GPU that loads this library holds its
+// kNoAllocScratchBytes until the process exits. Its name is a host-side stand-in in host code, so the
+// device address is looked up once per device with cudaGetSymbolAddress (on the entry point's first
+// call on that device, with that device current); make that first call before any stream capture.
+// All calls on a device share the array and it keeps the last call's contents: the counters are
+// cleared at every wave, and calls that overlap on the GPU (two streams, two threads) race on it.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 32ull << 20;  // 32 MiB
+constexpr int kNoAllocMaxDepth = 64;                  // counters for at most this many bounces
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {nullptr};
+
+// bytes of wavefront state per path slot: o, d, tp, L, hit_p, hit_n, sh_o, sh_d, sh_c (float4 each),
+// misc (float2), id (uint2), two queues, kKeys shading segments and the per-pixel sum (3 floats)
+constexpr size_t kNoAllocSlotBytes = 9 * 16 + 8 + 8 + 2 * 4 + kKeys * 4 + 12;
+constexpr size_t kNoAllocHeaderBytes = (sizeof(BounceCounters) * (kNoAllocMaxDepth + 1) + 255) / 256 * 256;
+constexpr uint32_t kNoAllocCapacity =
+    static_cast<uint32_t>((kNoAllocScratchBytes - kNoAllocHeaderBytes - 16 * 256) / kNoAllocSlotBytes);
+
+int noalloc_scratch(lrt_context* ctx, unsigned char** base) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if(ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) {
+        return fail(ctx, LRT_ERR_RANGE, "allocation-free render supports device ordinals below %d", kNoAllocMaxDevices);
+    }
+    if(!g_noalloc_base[ctx->device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if(e != cudaSuccess || !p) {
+            return fail(ctx, LRT_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", ctx->device,
+                        cudaGetErrorString(e));
+        }
+        g_noalloc_base[ctx->device] = static_cast<unsigned char*>(p);
+    }
+    *base = g_noalloc_base[ctx->device];
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!rgb_dev || !p) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(p->width < 2 || p->height < 2 || p->spp == 0 || p->max_depth < 1) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "render parameters out of range (width, height >= 2; spp, max_depth >= 1)");
+    }
+    if(p->max_depth > kNoAllocMaxDepth) {
+        return fail(ctx, LRT_ERR_RANGE, "allocation-free render: max_depth %d exceeds its maximum of %d", p->max_depth,
+                    kNoAllocMaxDepth);
+    }
+    if(static_cast<uint64_t>(p->width) * p->height > 0x3fffffffull) return fail(ctx, LRT_ERR_RANGE, "image too large");
+    const uint32_t row_begin = p->row_end > p->row_begin ? p->row_begin : 0u;
+    const uint32_t row_end = p->row_end > p->row_begin ? std::min(p->row_end, p->height) : p->height;
+    if(row_begin >= row_end) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "empty row range");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned char* base = nullptr;
+    const int st = noalloc_scratch(ctx, &base);
+    if(st != LRT_OK) return st;
+
+    // carve the fixed array: counters, then each slot array on a 256-byte boundary
+    const uint32_t cap = kNoAllocCapacity;
+    size_t off = kNoAllocHeaderBytes;
+    auto take = [&](size_t bytes) {
+        unsigned char* q = base + off;
+        off += (bytes + 255) / 256 * 256;
+        return q;
+    };
+    WaveArgs a{};
+    a.s = ctx->ds;
+    a.counters = reinterpret_cast<BounceCounters*>(base);
+    a.o = reinterpret_cast<float4*>(take(16ull * cap));
+    a.d = reinterpret_cast<float4*>(take(16ull * cap));
+    a.tp = reinterpret_cast<float4*>(take(16ull * cap));
+    a.L = reinterpret_cast<float4*>(take(16ull * cap));
+    a.hit_p = reinterpret_cast<float4*>(take(16ull * cap));
+    a.hit_n = reinterpret_cast<float4*>(take(16ull * cap));
+    a.sh_o = reinterpret_cast<float4*>(take(16ull * cap));
+    a.sh_d = reinterpret_cast<float4*>(take(16ull * cap));
+    a.sh_c = reinterpret_cast<float4*>(take(16ull * cap));
+    a.misc = reinterpret_cast<float2*>(take(8ull * cap));
+    a.id = reinterpret_cast<uint2*>(take(8ull * cap));
+    a.q0 = reinterpret_cast<uint32_t*>(take(4ull * cap));
+    a.q1 = reinterpret_cast<uint32_t*>(take(4ull * cap));
+    a.keyed = reinterpret_cast<uint32_t*>(take(4ull * cap * kKeys));
+    a.sum = reinterpret_cast<float*>(take(12ull * cap));
+    if(off > kNoAllocScratchBytes) return fail(ctx, LRT_ERR_RANGE, "allocation-free render: scratch layout overflow");
+    a.work = nullptr;
+    a.capacity = cap;
+    a.width = p->width;
+    a.height = p->height;
+    a.max_depth = p->max_depth;
+    a.rr_depth = p->rr_depth;
+    const size_t counters_bytes = sizeof(BounceCounters) * (p->max_depth + 1);
+
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
+    const int g_extend = grid_for(ctx, (const void*)k_extend<false>, kBlock);
+    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const int g_shadow = grid_for(ctx, (const void*)k_shadow<false>, kBlock);
+    const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
+    const uint32_t spp = p->spp;
+    const uint32_t samples_per_wave = std::min(spp, cap);
+    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
+    const uint32_t pix0 = row_begin * p->width;
+    const uint32_t pix1 = row_end * p->width;
+    uint64_t launches = 0;
+    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
+        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
+        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
+            const uint32_t ns = std::min(samples_per_wave, spp - sb);
+            a.pixel_begin = pb;
+            a.n_pixels = np;
+            a.sample_begin = p->sample_offset + sb;
+            a.n_samples = ns;
+            LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
+            k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
+            for(int depth = 0; depth < p->max_depth; ++depth) {
+                k_extend<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+                k_shadow<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+            }
+            k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
+            launches += 2 + 3ull * p->max_depth;
+            LRT_CUDA(ctx, cudaGetLastError());
+        }
+    }
+    ctx->stats.paths += static_cast<uint64_t>(pix1 - pix0) * spp;
+    ctx->stats.kernel_launches += launches;
+    return LRT_OK;
+}

@@ -27,6 +27,7 @@ EXPORTS = [
     "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_scene_upload", "lrt_scene_device_bytes",
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
+    "lrt_render_dev_noalloc",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
 ]
@@ -73,6 +74,7 @@ def lib():
         L.lrt_emitter_query.argtypes = [vp, P(f32), P(f32), P(f32), u32, P(f32), P(f32)]
         L.lrt_render.argtypes = [vp, P(abi.RenderParams), P(f32)]
         L.lrt_render_dev.argtypes = [vp, P(abi.RenderParams), vp]
+        L.lrt_render_dev_noalloc.argtypes = [vp, P(abi.RenderParams), vp]
         L.lrt_render_stats_get.argtypes = [vp, P(abi.RenderStats)]
         L.lrt_render_stats_reset.argtypes = [vp]
         L.lrt_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
