@@ -251,6 +251,7 @@ typedef struct lrt_render_params {
 #define LRT_STAGE_SHADOW  4
 #define LRT_STAGE_ACCUM   5
 #define LRT_STAGE_COUNT   6
+#define LRT_MAX_STAT_DEPTH 16
 
 typedef struct lrt_render_stats {
     uint64_t paths;              /* camera paths traced */
@@ -264,6 +265,7 @@ typedef struct lrt_render_stats {
     uint64_t kernel_launches;
     float stage_ms[LRT_STAGE_COUNT];
     uint32_t stage_launches[LRT_STAGE_COUNT];
+    uint64_t rays_at_depth[LRT_MAX_STAT_DEPTH];  /* extension rays per bounce (option count_work) */
 } lrt_render_stats;
 
 /* ---- context ---- */

@@ -185,7 +185,6 @@ struct WaveArgs {
 
 __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
     const uint32_t n = a.n_pixels * a.n_samples;
-    if(blockIdx.x == 0 && threadIdx.x == 0) a.counters[0].active = n;
     for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
         const uint32_t pix = a.pixel_begin + slot / a.n_samples;
         const uint32_t sample = a.sample_begin + slot % a.n_samples;
@@ -200,7 +199,8 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
         a.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         a.misc[slot] = make_float2(0.0f, 0.0f);
         a.id[slot] = make_uint2(pix, sample);
-        a.q0[slot] = slot;
+        const int seg = heavy_key(a.s, r, 0.001f, kInf);
+        a.q0[static_cast<size_t>(seg) * a.capacity + warp_append_keyed(a.counters[0].active, seg)] = slot;
     }
 }
 
@@ -208,11 +208,12 @@ template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
     const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
     BounceCounters& bc = a.counters[depth];
-    const uint32_t n = bc.active;
+    const uint32_t n0 = bc.active[0];
+    const uint32_t n = n0 + bc.active[1];
     TraceCount cnt{0, 0};
     uint32_t rays = 0;
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t pid = queue[i];
+        const uint32_t pid = i < n0 ? queue[i] : queue[a.capacity + (i - n0)];
         const float4 o = a.o[pid];
         const float4 d = a.d[pid];
         HitInfo h;
@@ -232,6 +233,154 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
         add_count(&a.work[0], cnt.nodes);
         add_count(&a.work[1], cnt.tris);
         add_count(&a.work[3], rays);
+        if(blockIdx.x == 0 && threadIdx.x == 0 && depth < LRT_MAX_STAT_DEPTH) {
+            atomicAdd(&a.work[8 + depth], static_cast<unsigned long long>(n));
+        }
+    }
+}
+
+// ---- persistent traversal: every lane keeps a ray, and takes the next one from the queue as soon as
+// its own finishes (ray replacement inside the traversal loop), so a warp's lanes stay busy while its
+// rays need very different numbers of nodes. The per-ray work is the state machine of trav_step.
+
+__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// fetch queue indices for the idle lanes of a warp: returns this lane's index (or >= n)
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter, bool idle, uint32_t n, bool& exhausted) {
+    const unsigned full = 0xffffffffu;
+    const unsigned want = __ballot_sync(full, idle);
+    uint32_t base = 0;
+    const int leader = __ffs(want) - 1;
+    if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(want)));
+    base = __shfl_sync(full, base, leader);
+    if(base + static_cast<uint32_t>(__popc(want)) >= n) exhausted = true;
+    return base + __popc(want & lanemask_lt());
+}
+
+// closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
+template <bool kCount>
+__global__ void __launch_bounds__(kBlock) k_extend_persistent(WaveArgs a, int depth) {
+    const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
+    BounceCounters& bc = a.counters[depth];
+    const uint32_t n0 = bc.active[0];
+    const uint32_t n = n0 + bc.active[1];
+    TravItem stack[kStackSize];
+    TravState st;
+    TraceCount cnt{0, 0};
+    uint32_t rays = 0;
+    bool active = false, exhausted = n == 0;
+    uint32_t pid = 0;
+    while(true) {
+        if(!exhausted && __any_sync(0xffffffffu, !active)) {
+            const uint32_t i = warp_fetch(&bc.pad[0], !active, n, exhausted);
+            if(!active && i < n) {
+                pid = i < n0 ? queue[i] : queue[a.capacity + (i - n0)];
+                const float4 o = a.o[pid];
+                const float4 d = a.d[pid];
+                trav_begin(st, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, kInf, false);
+                active = true;
+                ++rays;
+            }
+        }
+        if(!__any_sync(0xffffffffu, active)) break;
+        if(active && trav_step<kCount>(a.s, st, stack, cnt)) {
+            a.hit_p[pid] = make_float4(st.closest_so_far, st.best_mesh.u, st.best_mesh.v, __int_as_float(st.best));
+            a.hit_n[pid] = make_float4(__uint_as_float(st.best_mesh.ref), 0.0f, 0.0f, 0.0f);
+            active = false;
+        }
+    }
+    if(kCount) {
+        add_count(&a.work[0], cnt.nodes);
+        add_count(&a.work[1], cnt.tris);
+        add_count(&a.work[3], rays);
+        if(blockIdx.x == 0 && threadIdx.x == 0 && depth < LRT_MAX_STAT_DEPTH) {
+            atomicAdd(&a.work[8 + depth], static_cast<unsigned long long>(n));
+        }
+    }
+}
+
+// hit records of the raw results, in queue order (coherent), and the material-type shading queues
+__global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
+    const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
+    BounceCounters& bc = a.counters[depth];
+    const uint32_t n0 = bc.active[0];
+    const uint32_t n = n0 + bc.active[1];
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t pid = i < n0 ? queue[i] : queue[a.capacity + (i - n0)];
+        const float4 raw = a.hit_p[pid];
+        const int32_t best = __float_as_int(raw.w);
+        int key = 0;
+        if(best >= 0) {
+            const float4 o = a.o[pid];
+            const float4 d = a.d[pid];
+            const MeshHit mh{raw.x, raw.y, raw.z, __float_as_uint(a.hit_n[pid].x)};
+            HitInfo h;
+            hit_record_of(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, best, raw.x, mh, h);
+            const int32_t mat = a.s.objects[best].material;
+            key = mat < 0 ? 1 : 2 + a.s.materials[mat].type;
+            a.hit_p[pid] = make_float4(h.p.x, h.p.y, h.p.z, __int_as_float(h.object));
+            a.hit_n[pid] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.front_face ? 1.0f : 0.0f);
+        }
+        const uint32_t slot = warp_append_keyed(bc.key_count, key);
+        a.keyed[static_cast<size_t>(key) * a.capacity + slot] = pid;
+    }
+}
+
+// shadow rays with ray replacement: any-hit unless the light's own shape is reachable (then the
+// closest hit decides, scene_occluded)
+template <bool kCount>
+__global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int depth) {
+    BounceCounters& bc = a.counters[depth];
+    const uint32_t n0 = bc.shadow[0];
+    const uint32_t n = n0 + bc.shadow[1];
+    TravItem stack[kStackSize];
+    TravState st;
+    TraceCount cnt{0, 0};
+    uint32_t rays = 0;
+    bool active = false, exhausted = n == 0;
+    size_t k = 0;
+    int32_t light = 0;
+    while(true) {
+        if(!exhausted && __any_sync(0xffffffffu, !active)) {
+            const uint32_t i = warp_fetch(&bc.pad[1], !active, n, exhausted);
+            if(!active && i < n) {
+                k = i < n0 ? i : a.capacity + (i - n0);
+                const float4 o = a.sh_o[k], d = a.sh_d[k];
+                light = __float_as_int(d.w);
+                const Ray r{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}};
+                bool any_mode = true;
+                const EmitRec& e = a.s.emitters[light];
+                if(e.kind == LRT_EMITTER_AREA) {
+                    const ObjRec& lo = a.s.objects[e.object];
+                    float t;
+                    f3 p;
+                    any_mode = !(lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, r, 0.001f, o.w, t, p)
+                                                                : hit_sphere(lo, r, 0.001f, o.w, t));
+                }
+                trav_begin(st, r, 0.001f, o.w, any_mode);
+                active = true;
+                ++rays;
+            }
+        }
+        if(!__any_sync(0xffffffffu, active)) break;
+        if(active && trav_step<kCount>(a.s, st, stack, cnt)) {
+            const bool blocked = st.any_mode ? st.best >= 0 : (st.best >= 0 && a.s.objects[st.best].emitter != light);
+            if(!blocked) {
+                const float4 c = a.sh_c[k];
+                const uint32_t p = __float_as_uint(c.w);
+                float4 L = a.L[p];
+                L.x += c.x;
+                L.y += c.y;
+                L.z += c.z;
+                a.L[p] = L;
+            }
+            active = false;
+        }
+    }
+    if(kCount) {
+        add_count(&a.work[5], cnt.nodes);
+        add_count(&a.work[6], cnt.tris);
+        add_count(&a.work[4], rays);
     }
 }
 
@@ -346,7 +495,8 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
                         if(light_pdf > 0.0f) {
                             const float w = power_heuristic(light_pdf, bsdf_pdf_v);
                             const f3 contrib = throughput * f_cos * light.radiance * (w / light_pdf);
-                            const uint32_t si = warp_append(&bc.shadow);
+                            const int seg = heavy_key(s, Ray{shadow_origin, shadow_dir}, 0.001f, tmax);
+                            const size_t si = static_cast<size_t>(seg) * a.capacity + warp_append_keyed(bc.shadow, seg);
                             a.sh_o[si] = make_float4(shadow_origin.x, shadow_origin.y, shadow_origin.z, tmax);
                             a.sh_d[si] = make_float4(shadow_dir.x, shadow_dir.y, shadow_dir.z, __int_as_float(light.emitter));
                             a.sh_c[si] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(pid));
@@ -382,8 +532,8 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
             a.d[pid] = make_float4(new_dir.x, new_dir.y, new_dir.z, 0.0f);
             a.tp[pid] = make_float4(throughput.x, throughput.y, throughput.z, eta);
             a.misc[pid] = make_float2(rec.pdf, have ? 1.0f : 0.0f);
-            const uint32_t ni = warp_append(&nc.active);
-            next[ni] = pid;
+            const int seg = heavy_key(s, Ray{p, new_dir}, 0.001f, kInf);
+            next[static_cast<size_t>(seg) * a.capacity + warp_append_keyed(nc.active, seg)] = pid;
         }
     }
     if(a.work) add_count(&a.work[2], shading);
@@ -391,11 +541,13 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
 
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs a, int depth) {
-    const uint32_t n = a.counters[depth].shadow;
+    const uint32_t n0 = a.counters[depth].shadow[0];
+    const uint32_t n = n0 + a.counters[depth].shadow[1];
     TraceCount cnt{0, 0};
     uint32_t rays = 0;
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = a.sh_o[i], d = a.sh_d[i], c = a.sh_c[i];
+        const size_t k = i < n0 ? i : a.capacity + (i - n0);
+        const float4 o = a.sh_o[k], d = a.sh_d[k], c = a.sh_c[k];
         const int32_t light = __float_as_int(d.w);
         const bool blocked = scene_occluded<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, o.w, light, cnt);
         ++rays;
@@ -444,12 +596,12 @@ int ensure_wave(lrt_context* ctx, uint32_t cap) {
     LRT_CUDA(ctx, w.id.ensure(c * 8));
     LRT_CUDA(ctx, w.hit_p.ensure(c * 16));
     LRT_CUDA(ctx, w.hit_n.ensure(c * 16));
-    LRT_CUDA(ctx, w.q0.ensure(c * 4));
-    LRT_CUDA(ctx, w.q1.ensure(c * 4));
+    LRT_CUDA(ctx, w.q0.ensure(c * 8));
+    LRT_CUDA(ctx, w.q1.ensure(c * 8));
     LRT_CUDA(ctx, w.keyed.ensure(c * 4 * kKeys));
-    LRT_CUDA(ctx, w.sh_o.ensure(c * 16));
-    LRT_CUDA(ctx, w.sh_d.ensure(c * 16));
-    LRT_CUDA(ctx, w.sh_c.ensure(c * 16));
+    LRT_CUDA(ctx, w.sh_o.ensure(c * 32));
+    LRT_CUDA(ctx, w.sh_d.ensure(c * 32));
+    LRT_CUDA(ctx, w.sh_c.ensure(c * 32));
     LRT_CUDA(ctx, w.sum.ensure(c * 12));
     w.capacity = cap;
     return LRT_OK;
@@ -520,18 +672,22 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     a.max_depth = p->max_depth;
     a.rr_depth = p->rr_depth;
     unsigned long long* work = nullptr;
+    constexpr size_t kWorkBytes = 8 * (8 + LRT_MAX_STAT_DEPTH);
     if(ctx->count_work) {
-        LRT_CUDA(ctx, ctx->scratch_b.ensure(64));
+        LRT_CUDA(ctx, ctx->scratch_b.ensure(kWorkBytes));
         work = ctx->scratch_b.as<unsigned long long>();
-        LRT_CUDA(ctx, cudaMemsetAsync(work, 0, 64, ctx->stream));
+        LRT_CUDA(ctx, cudaMemsetAsync(work, 0, kWorkBytes, ctx->stream));
     }
     a.work = work;
 
     const bool cnt = ctx->count_work;
     const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
-    const int g_extend = grid_for(ctx, cnt ? (const void*)k_extend<true> : (const void*)k_extend<false>, kBlock);
+    const int g_extend =
+        grid_for(ctx, cnt ? (const void*)k_extend_persistent<true> : (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
     const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
-    const int g_shadow = grid_for(ctx, cnt ? (const void*)k_shadow<true> : (const void*)k_shadow<false>, kBlock);
+    const int g_shadow =
+        grid_for(ctx, cnt ? (const void*)k_shadow_persistent<true> : (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
 
     // wave plan: a pixel range x a sample range, at most `cap` slots
@@ -557,22 +713,25 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
             for(int depth = 0; depth < p->max_depth; ++depth) {
                 record_stage(ctx, LRT_STAGE_EXTEND, true);
                 if(cnt) {
-                    k_extend<true><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                    k_extend_persistent<true><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
                 } else {
-                    k_extend<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                    k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
                 }
                 record_stage(ctx, LRT_STAGE_EXTEND, false);
+                record_stage(ctx, LRT_STAGE_SORT, true);
+                k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
+                record_stage(ctx, LRT_STAGE_SORT, false);
                 record_stage(ctx, LRT_STAGE_SHADE, true);
                 k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
                 record_stage(ctx, LRT_STAGE_SHADE, false);
                 record_stage(ctx, LRT_STAGE_SHADOW, true);
                 if(cnt) {
-                    k_shadow<true><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                    k_shadow_persistent<true><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
                 } else {
-                    k_shadow<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                    k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
                 }
                 record_stage(ctx, LRT_STAGE_SHADOW, false);
-                launches += 3;
+                launches += 4;
             }
             record_stage(ctx, LRT_STAGE_ACCUM, true);
             k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
@@ -587,8 +746,9 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
         LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         collect_stage_times(ctx);
         if(cnt) {
-            unsigned long long h[7];
+            unsigned long long h[8 + LRT_MAX_STAT_DEPTH];
             LRT_CUDA(ctx, cudaMemcpy(h, work, sizeof(h), cudaMemcpyDeviceToHost));
+            for(int d = 0; d < LRT_MAX_STAT_DEPTH; ++d) ctx->stats.rays_at_depth[d] += h[8 + d];
             ctx->stats.nodes_visited += h[0];
             ctx->stats.triangles_tested += h[1];
             ctx->stats.shading_events += h[2];
@@ -737,6 +897,8 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     ds.n_infinite = h.n_infinite;
     ds.n_emission = static_cast<int32_t>(h.emission_cdf.size());
     ds.emission_power = h.emission_power;
+    ds.n_heavy = h.n_heavy;
+    for(int i = 0; i < 4; ++i) ds.heavy[i] = h.heavy[i];
     ds.cam = h.cam;
     ctx->scene_bytes = bytes;
     ctx->has_scene = true;
@@ -969,7 +1131,7 @@ unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {nullptr};
 
 // bytes of wavefront state per path slot: o, d, tp, L, hit_p, hit_n, sh_o, sh_d, sh_c (float4 each),
 // misc (float2), id (uint2), two queues, kKeys shading segments and the per-pixel sum (3 floats)
-constexpr size_t kNoAllocSlotBytes = 9 * 16 + 8 + 8 + 2 * 4 + kKeys * 4 + 12;
+constexpr size_t kNoAllocSlotBytes = 6 * 16 + 3 * 32 + 8 + 8 + 2 * 8 + kKeys * 4 + 12;
 constexpr size_t kNoAllocHeaderBytes = (sizeof(BounceCounters) * (kNoAllocMaxDepth + 1) + 255) / 256 * 256;
 constexpr uint32_t kNoAllocCapacity =
     static_cast<uint32_t>((kNoAllocScratchBytes - kNoAllocHeaderBytes - 16 * 256) / kNoAllocSlotBytes);
@@ -1031,13 +1193,13 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
     a.L = reinterpret_cast<float4*>(take(16ull * cap));
     a.hit_p = reinterpret_cast<float4*>(take(16ull * cap));
     a.hit_n = reinterpret_cast<float4*>(take(16ull * cap));
-    a.sh_o = reinterpret_cast<float4*>(take(16ull * cap));
-    a.sh_d = reinterpret_cast<float4*>(take(16ull * cap));
-    a.sh_c = reinterpret_cast<float4*>(take(16ull * cap));
+    a.sh_o = reinterpret_cast<float4*>(take(32ull * cap));
+    a.sh_d = reinterpret_cast<float4*>(take(32ull * cap));
+    a.sh_c = reinterpret_cast<float4*>(take(32ull * cap));
     a.misc = reinterpret_cast<float2*>(take(8ull * cap));
     a.id = reinterpret_cast<uint2*>(take(8ull * cap));
-    a.q0 = reinterpret_cast<uint32_t*>(take(4ull * cap));
-    a.q1 = reinterpret_cast<uint32_t*>(take(4ull * cap));
+    a.q0 = reinterpret_cast<uint32_t*>(take(8ull * cap));
+    a.q1 = reinterpret_cast<uint32_t*>(take(8ull * cap));
     a.keyed = reinterpret_cast<uint32_t*>(take(4ull * cap * kKeys));
     a.sum = reinterpret_cast<float*>(take(12ull * cap));
     if(off > kNoAllocScratchBytes) return fail(ctx, LRT_ERR_RANGE, "allocation-free render: scratch layout overflow");
@@ -1050,9 +1212,10 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
     const size_t counters_bytes = sizeof(BounceCounters) * (p->max_depth + 1);
 
     const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
-    const int g_extend = grid_for(ctx, (const void*)k_extend<false>, kBlock);
+    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
     const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
-    const int g_shadow = grid_for(ctx, (const void*)k_shadow<false>, kBlock);
+    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
     const uint32_t spp = p->spp;
     const uint32_t samples_per_wave = std::min(spp, cap);
@@ -1071,12 +1234,13 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
             LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
             k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
             for(int depth = 0; depth < p->max_depth; ++depth) {
-                k_extend<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
                 k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
-                k_shadow<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
             }
             k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
-            launches += 2 + 3ull * p->max_depth;
+            launches += 2 + 4ull * p->max_depth;
             LRT_CUDA(ctx, cudaGetLastError());
         }
     }

@@ -44,13 +44,16 @@ constexpr int kBlock = 128;
 constexpr int kMaxPhotonMaps = 4;
 constexpr uint32_t kMaxKnn = 128;
 
-// per-bounce device counters of one wave
+// per-bounce device counters of one wave. The active and shadow queues have two segments of
+// `capacity` entries: rays that may reach the box of a heavy mesh (segment 1) and the others, so that a
+// warp's rays share the cost of the large traversals.
 struct BounceCounters {
-    uint32_t active;  // paths entering this bounce
-    uint32_t shadow;  // shadow rays emitted by this bounce
+    uint32_t active[2];  // paths entering this bounce, per segment
+    uint32_t shadow[2];  // shadow rays emitted by this bounce, per segment
     uint32_t key_count[kKeys];
-    uint32_t pad[4];
+    uint32_t pad[2];
 };
+static_assert(sizeof(BounceCounters) == 64, "counter layout");
 
 struct WaveState {
     uint32_t capacity = 0;

@@ -857,6 +857,19 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
         const f3 half = (scene_box.hi - scene_box.lo) * 0.5f;
         s.bounding_radius = length(half);
     }
+    {
+        std::vector<std::pair<uint32_t, int32_t>> heavy;
+        for(size_t i = 0; i < s.objects.size(); ++i) {
+            if(s.objects[i].kind == LRT_OBJECT_MESH && s.objects[i].n_tris > 64) {
+                heavy.push_back({s.objects[i].n_tris, static_cast<int32_t>(i)});
+            }
+        }
+        if(!heavy.empty() && heavy.size() <= 4) {
+            std::sort(heavy.begin(), heavy.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            s.n_heavy = static_cast<int32_t>(heavy.size());
+            for(size_t i = 0; i < heavy.size(); ++i) s.heavy[i] = heavy[i].second;
+        }
+    }
 
     // ---- emitters ----
     float sum = 0.0f;

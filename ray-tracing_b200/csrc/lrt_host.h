@@ -36,6 +36,9 @@ struct HostScene {
     float emission_power = 0.0f;
     float bounding_radius = 0.0f;  // scene::bounding_sphere_radius (scene.h:41-45)
     bool has_delta_bsdf = false;   // scene::has_delta_bsdf (scene.h:48-57)
+    // meshes of more than 64 triangles, largest first; queue segmentation is off when there are > 4
+    int32_t n_heavy = 0;
+    int32_t heavy[4] = {-1, -1, -1, -1};
 };
 
 // Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message.

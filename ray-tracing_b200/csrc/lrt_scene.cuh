@@ -104,6 +104,15 @@ __device__ __forceinline__ bool ray_may_hit_box(const ObjRec& o, const Ray& r, f
     return !(tn > tf);
 }
 
+// Queue segment of a ray: 1 when it may reach the box of one of the scene's heavy meshes (the ones whose
+// traversal dominates), 0 otherwise. Only a scheduling hint: every ray is traced the same way.
+__device__ __forceinline__ int heavy_key(const DeviceScene& s, const Ray& r, float t_min, float t_max) {
+    for(int32_t h = 0; h < s.n_heavy; ++h) {
+        if(ray_may_hit_box(s.objects[s.heavy[h]], r, t_min, t_max)) return 1;
+    }
+    return 0;
+}
+
 // sah_kdtree::intersect over one mesh's tree with the triangle_mesh::hit leaf callback, written as
 // a descend loop and a leaf loop (same node and triangle order as the reference's single loop, fewer
 // divergent branches per warp). kAny: stop at the first accepted triangle (occlusion queries).
@@ -375,6 +384,208 @@ __device__ __forceinline__ bool scene_occluded(const DeviceScene& s, const Ray& 
         }
     }
     return false;
+}
+
+// ---- resumable traversal (persistent kernels) ----
+//
+// The object-list walk of scene_hit (and of the occlusion test) as a state machine that advances one
+// unit of work per call: either scans objects up to the next mesh whose box the ray may reach (testing
+// analytic shapes on the way), or runs one descend-to-leaf + leaf of the current mesh's traversal. The
+// nodes, triangles and their order per ray are exactly those of trace_mesh / scene_hit; persistent
+// kernels interleave rays so that a lane whose ray finishes takes a new one at once.
+struct TravItem {
+    uint32_t node;
+    float mint, maxt;
+};
+
+struct TravState {
+    Ray r;
+    float t_min;
+    float t_max;          // occlusion: the shadow ray's tmax; closest hit: +inf
+    int32_t obj;          // next (or current) object of the list
+    bool in_mesh;
+    bool any_mode;        // occlusion without a reachable light: stop at the first accepted hit
+    uint32_t node;
+    float mint, maxt;
+    int32_t top;
+    float closest;        // closest inside the current mesh
+    float closest_so_far; // across the list
+    int32_t best;
+    MeshHit best_mesh;
+    MeshHit cur;
+    bool cur_hit;
+    float inv_x, inv_y, inv_z;
+};
+
+__device__ __forceinline__ void trav_begin(TravState& st, const Ray& r, float t_min, float t_max, bool any_mode) {
+    st.r = r;
+    st.t_min = t_min;
+    st.t_max = t_max;
+    st.obj = 0;
+    st.in_mesh = false;
+    st.any_mode = any_mode;
+    st.closest_so_far = t_max;
+    st.best = -1;
+    st.cur_hit = false;
+    st.inv_x = 1.0f / r.d.x;
+    st.inv_y = 1.0f / r.d.y;
+    st.inv_z = 1.0f / r.d.z;
+}
+
+// One unit of work; returns true when the ray is finished (result in best / best_mesh / closest_so_far;
+// in any_mode best >= 0 means "hit").
+template <bool kCount>
+__device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, TravItem* stack, TraceCount& cnt) {
+    if(!st.in_mesh) {
+        while(st.obj < s.n_objects) {
+            const ObjRec& o = s.objects[st.obj];
+            if(o.kind == LRT_OBJECT_MESH) {
+                if(ray_may_hit_box(o, st.r, st.t_min, st.closest_so_far)) {
+                    st.in_mesh = true;
+                    st.node = 0;
+                    st.mint = st.t_min;
+                    st.maxt = st.closest_so_far;
+                    st.closest = st.closest_so_far;
+                    st.top = 0;
+                    st.cur_hit = false;
+                    return false;
+                }
+            } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+                float t;
+                f3 p;
+                if(hit_rectangle(o, st.r, st.t_min, st.closest_so_far, t, p)) {
+                    st.closest_so_far = t;
+                    st.best = st.obj;
+                    if(st.any_mode) return true;
+                }
+            } else {
+                float t;
+                if(hit_sphere(o, st.r, st.t_min, st.closest_so_far, t)) {
+                    st.closest_so_far = t;
+                    st.best = st.obj;
+                    if(st.any_mode) return true;
+                }
+            }
+            ++st.obj;
+        }
+        return true;
+    }
+    const ObjRec& o = s.objects[st.obj];
+    const uint2* nodes = s.nodes + o.node_base;
+    bool mesh_done = false;
+    uint2 n;
+    while(true) {  // descend (sah_kdtree.h:105-120)
+        if(st.closest < st.mint) {
+            mesh_done = true;
+            break;
+        }
+        n = ld_node(nodes + st.node);
+        if(kCount) ++cnt.nodes;
+        if((n.y & 3u) == kLeafTag) break;
+        const uint32_t axis = n.y & 3u;
+        const float split = __uint_as_float(n.x);
+        const float o_a = comp(st.r.o, axis);
+        const float d_a = comp(st.r.d, axis);
+        const float t_plane = (split - o_a) * (axis == 0 ? st.inv_x : (axis == 1 ? st.inv_y : st.inv_z));
+        const bool left_of_split = o_a < split || (o_a == split && d_a <= 0.0f);
+        const uint32_t right = n.y >> 2;
+        const uint32_t first_child = left_of_split ? st.node + 1 : right;
+        const uint32_t second_child = left_of_split ? right : st.node + 1;
+        if(t_plane > st.maxt || t_plane <= 0.0f) {
+            st.node = first_child;
+        } else if(t_plane < st.mint) {
+            st.node = second_child;
+        } else {
+            if(st.top < kStackSize) {
+                stack[st.top].node = second_child;
+                stack[st.top].mint = t_plane;
+                stack[st.top].maxt = st.maxt;
+                ++st.top;
+            }
+            st.node = first_child;
+            st.maxt = t_plane;
+        }
+    }
+    if(!mesh_done) {  // leaf (sah_kdtree.h:86-93)
+        const float4* tris = s.tris + 3ull * o.ref_base;
+        const uint32_t count = n.y >> 2;
+        const uint32_t first = n.x;
+        float limit = smin(st.maxt, st.closest);
+        for(uint32_t i = 0; i < count; ++i) {
+            if(kCount) ++cnt.tris;
+            float u, v;
+            if(hit_tri_record(tris + 3ull * (first + i), st.r, st.mint, limit, st.closest, u, v)) {
+                st.cur_hit = true;
+                st.cur.t = st.closest;
+                st.cur.u = u;
+                st.cur.v = v;
+                st.cur.ref = first + i;
+                if(st.any_mode) {
+                    st.best = st.obj;
+                    return true;
+                }
+            }
+            limit = smin(st.maxt, st.closest);
+        }
+        if(st.top == 0) {
+            mesh_done = true;
+        } else {
+            --st.top;
+            st.node = stack[st.top].node;
+            st.mint = stack[st.top].mint;
+            st.maxt = stack[st.top].maxt;
+        }
+    }
+    if(mesh_done) {
+        if(st.cur_hit) {
+            st.closest_so_far = st.cur.t;
+            st.best = st.obj;
+            st.best_mesh = st.cur;
+        }
+        st.in_mesh = false;
+        ++st.obj;
+    }
+    return false;
+}
+
+// The hit record of a finished closest-hit traversal (the second half of scene_hit).
+__device__ __forceinline__ void hit_record_of(const DeviceScene& s, const Ray& r, int32_t best, float t,
+                                              const MeshHit& best_mesh, HitInfo& out) {
+    out.object = best;
+    out.prim = -1;
+    const ObjRec& o = s.objects[best];
+    out.t = t;
+    out.p = r.o + t * r.d;
+    if(o.kind == LRT_OBJECT_MESH) {
+        const uint32_t ref = o.ref_base + best_mesh.ref;
+        const uint32_t tri = __ldg(s.ref_prim + ref);
+        out.prim = static_cast<int32_t>(tri);
+        const float4 b = ld_tri(s.tris + 3ull * ref + 1);
+        const float4 c = ld_tri(s.tris + 3ull * ref + 2);
+        const f3 geometric = cross(f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z});
+        const f3 outward = geometric / length(geometric);
+        out.front_face = dot(r.d, outward) < 0.0f;
+        out.normal = out.front_face ? outward : -outward;
+        const float u = best_mesh.u;
+        const float v = best_mesh.v;
+        const float b0 = 1.0f - u - v;
+        const float4* cn = s.normals + 3ull * (o.tri_base + tri);
+        const float4 n0 = __ldg(cn), n1 = __ldg(cn + 1), n2 = __ldg(cn + 2);
+        f3 shading = b0 * f3{n0.x, n0.y, n0.z} + u * f3{n1.x, n1.y, n1.z} + v * f3{n2.x, n2.y, n2.z};
+        if(length_squared(shading) > 0.0f) {
+            shading = shading / length(shading);
+            if(dot(r.d, shading) > 0.0f) shading = -shading;
+            out.normal = shading;
+        }
+    } else if(o.kind == LRT_OBJECT_RECTANGLE) {
+        const f3 normal = load3(o.normal);
+        out.front_face = dot(r.d, normal) < 0.0f;
+        out.normal = out.front_face ? normal : -normal;
+    } else {
+        const f3 outward = (out.p - load3(o.center)) / o.radius;
+        out.front_face = dot(r.d, outward) < 0.0f;
+        out.normal = out.front_face ? outward : -outward;
+    }
 }
 
 // ---- sky: env_emitter::eval (env_emitter.h:71-88) + ArHosekSkyModel_GetRadianceInternal (double) ----

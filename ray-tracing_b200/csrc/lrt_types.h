@@ -109,6 +109,8 @@ struct DeviceScene {
     int32_t n_infinite;      // emitters with is_infinite()
     int32_t n_emission;      // CDF bins
     float emission_power;    // total luminance of emitted power
+    int32_t n_heavy;         // meshes large enough that rays reaching their box are queued apart
+    int32_t heavy[4];
     CamRec cam;
 };
 

@@ -242,6 +242,7 @@ class Context:
             "shading_events": s.shading_events, "kernel_launches": s.kernel_launches,
             "stage_ms": {abi.STAGE_NAMES[i]: s.stage_ms[i] for i in range(6)},
             "stage_launches": {abi.STAGE_NAMES[i]: s.stage_launches[i] for i in range(6)},
+            "rays_at_depth": [int(s.rays_at_depth[i]) for i in range(16)],
         }
 
     def reset_stats(self):
