@@ -358,6 +358,34 @@ int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t 
 int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, const float* normals,
                           uint32_t n, float radius, int32_t max_depth, uint32_t k, float* rgb_out);
 
+/* photon-mapper eye pass settings (photon_integrator.h:15-17,57-65) */
+typedef struct lrt_photon_render_params {
+    int32_t global_map;          /* photon map id, -1 = empty */
+    int32_t caustic_map;
+    float global_radius;
+    float caustic_radius;
+    int32_t max_depth;           /* 128 in the reference */
+    int32_t max_specular_depth;  /* 4 */
+    int32_t direct_samples;      /* 16 */
+    int32_t glossy_samples;      /* 32 */
+    uint32_t lookup_size;        /* k, 120 in the reference; at most 128 */
+} lrt_photon_render_params;
+
+/* photon_integrator::preprocess (photon_integrator.h:15-37): radii 0.05 R and 0.0125 R of the scene's
+ * bounding sphere (each capped at radius_cap; pass INFINITY for none), a global gather and -- when the
+ * scene has a specular BSDF -- a caustic gather with photon depth max_depth - 1, and maps 0 / 1 for the
+ * gathers that stored their request. Fills the map ids and radii of *out; shots[2] gets the particle
+ * counts (may be null). */
+int lrt_photon_preprocess(lrt_context* ctx, uint32_t global_photons, uint32_t caustic_photons,
+                          int32_t max_depth, int32_t rr_depth, float radius_cap,
+                          lrt_photon_render_params* out, uint64_t* shots);
+/* photon-mapper image: photon_integrator::radiance for every (pixel, sample) of the tile loop of
+ * src/main.cpp:103-147 */
+int lrt_render_photon(lrt_context* ctx, const lrt_render_params* params, const lrt_photon_render_params* pp,
+                      float* rgb);
+int lrt_render_photon_dev(lrt_context* ctx, const lrt_render_params* params,
+                          const lrt_photon_render_params* pp, float* rgb_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,9 @@ def ref_lib():
         lib.ref_camera_rays.argtypes = [vp, u32, u32, P(u32), u32, P(abi.Ray)]
         lib.ref_render.restype = C.c_double
         lib.ref_render.argtypes = [vp, P(abi.RenderParams), u32, P(f32), P(f32)]
+        lib.ref_photon_render.restype = C.c_double
+        lib.ref_photon_render.argtypes = [vp, P(abi.RenderParams), u32, P(abi.Photon), u32, f32, P(abi.Photon), u32, f32,
+                                          P(abi.PhotonRenderParams), P(f32), P(f32)]
         lib.ref_trace_particles.argtypes = [vp, i32, u32, u32, i32, i32, u32, P(abi.Photon), P(u32)]
         lib.ref_photon_gather.restype = u32
         lib.ref_photon_gather.argtypes = [vp, i32, u32, i32, i32, P(abi.Photon), P(C.c_uint64), P(C.c_double)]
@@ -146,6 +149,18 @@ class RefWorld:
         sq = np.zeros_like(img) if want_sq else None
         secs = ref_lib().ref_render(self.handle, C.byref(params), threads, _p(img),
                                     _p(sq) if sq is not None else None)
+        return img, sq, secs
+
+    def render_photon(self, params, pp, global_photons, global_scale, caustic_photons, caustic_scale, threads=0,
+                      want_sq=True):
+        """photon_integrator::radiance over the image with maps built from the given photon arrays"""
+        g = np.ascontiguousarray(global_photons, dtype=abi.PHOTON_DTYPE)
+        c = np.ascontiguousarray(caustic_photons, dtype=abi.PHOTON_DTYPE)
+        img = np.zeros((params.height, params.width, 3), dtype=np.float32)
+        sq = np.zeros_like(img) if want_sq else None
+        secs = ref_lib().ref_photon_render(self.handle, C.byref(params), threads, _p(g, abi.Photon) if len(g) else None,
+                                           len(g), global_scale, _p(c, abi.Photon) if len(c) else None, len(c),
+                                           caustic_scale, C.byref(pp), _p(img), _p(sq) if sq is not None else None)
         return img, sq, secs
 
     def trace_particles(self, kind, first, count, max_depth, rr_depth, max_per=64):

@@ -43,6 +43,15 @@
 
 int lrt_ref_max_depth = 50;  // path_integrator.h:173, made settable in the generated copy
 int lrt_ref_rr_depth = 5;    // path_integrator.h:19
+// photon_integrator.h:57-64, made settable in the generated copy
+int lrt_ref_pm_max_depth = 128;
+int lrt_ref_pm_max_specular_depth = 4;
+int lrt_ref_pm_rr_depth = 5;
+int lrt_ref_pm_direct_samples = 16;
+int lrt_ref_pm_glossy_samples = 32;
+std::size_t lrt_ref_pm_global_photons = 250000;
+std::size_t lrt_ref_pm_caustic_photons = 250000;
+std::size_t lrt_ref_pm_lookup_size = 120;
 
 #define private public
 #include "core/scene.h"
@@ -67,6 +76,7 @@ int lrt_ref_rr_depth = 5;    // path_integrator.h:19
 #include "integrator/photonmapper/photon_map.h"
 #include "integrator/photonmapper/photon_tracer.h"
 #include "integrator/photonmapper/photon_gather.h"
+#include "integrator/photonmapper/photon_integrator.h"
 #undef private
 
 #include "lrt.h"
@@ -202,6 +212,55 @@ struct ref_photon_map {
     photon_map map;
     std::vector<uint32_t> original;  // post-build position -> index in the caller's array
 };
+
+// The tile loop of src/main.cpp:103-147 (32x32 tiles on a thread_pool of `threads` workers) around
+// `radiance(ray, sampler)`. rgb = per-pixel mean; rgb_sq (optional) = per-pixel mean of squares. Returns
+// the wall-clock seconds of the tile loop (steady_clock, as main.cpp:103,148).
+template <typename Radiance>
+double render_tiles(const ref_world& w, const lrt_render_params* p, uint32_t threads, float* rgb, float* rgb_sq,
+                    Radiance&& radiance) {
+    const int width = static_cast<int>(p->width);
+    const int height = static_cast<int>(p->height);
+    const int row_begin = p->row_end > p->row_begin ? static_cast<int>(p->row_begin) : 0;
+    const int row_end = p->row_end > p->row_begin ? static_cast<int>(p->row_end) : height;
+    const int spp = static_cast<int>(p->spp);
+    constexpr int tile = 32;
+    const auto start = std::chrono::steady_clock::now();
+    {
+        thread_pool pool(threads == 0 ? std::thread::hardware_concurrency() : threads);
+        for(int y0 = row_begin; y0 < row_end; y0 += tile) {
+            for(int x0 = 0; x0 < width; x0 += tile) {
+                const int x1 = std::min(x0 + tile, width);
+                const int y1 = std::min(y0 + tile, row_end);
+                pool.submit([&, x0, y0, x1, y1] {
+                    for(int y = y0; y < y1; ++y) {
+                        for(int x = x0; x < x1; ++x) {
+                            color sum(0.0f);
+                            color sum_sq(0.0f);
+                            for(int s = 0; s < spp; ++s) {
+                                const auto pixel_index = static_cast<uint32_t>(y * width + x);
+                                sampler smp;
+                                smp.start(pixel_index, static_cast<uint32_t>(s) + p->sample_offset);
+                                const auto offset = smp.next_2d();
+                                const auto u = (static_cast<float>(x) + offset.x) / static_cast<float>(width - 1);
+                                const auto v = (static_cast<float>(y) + offset.y) / static_cast<float>(height - 1);
+                                auto r = w.world->sensor().get_ray(u, v);
+                                const auto L = radiance(r, smp);
+                                sum += L;
+                                sum_sq += L * L;
+                            }
+                            const size_t o = 3 * (static_cast<size_t>(y) * width + x);
+                            put3(rgb + o, sum / static_cast<float>(spp));
+                            if(rgb_sq) { put3(rgb_sq + o, sum_sq / static_cast<float>(spp)); }
+                        }
+                    }
+                });
+            }
+        }
+        pool.wait();
+    }
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+}
 
 }  // namespace
 
@@ -409,55 +468,37 @@ void ref_camera_rays(void* handle, uint32_t width, uint32_t height, const uint32
     }
 }
 
-// Path-traced image with the tile loop of src/main.cpp:103-147 (32x32 tiles on a thread_pool of
-// `threads` workers). rgb = per-pixel mean; rgb_sq (optional) = per-pixel mean of squares. Returns
-// the wall-clock seconds of the tile loop (steady_clock, as main.cpp:103,148).
+// Path-traced image (path_integrator::radiance with run-time max_depth / rr_depth).
 double ref_render(void* handle, const lrt_render_params* p, uint32_t threads, float* rgb, float* rgb_sq) {
     const auto& w = *static_cast<ref_world*>(handle);
     lrt_ref_max_depth = p->max_depth;
     lrt_ref_rr_depth = p->rr_depth;
-    const int width = static_cast<int>(p->width);
-    const int height = static_cast<int>(p->height);
-    const int row_begin = p->row_end > p->row_begin ? static_cast<int>(p->row_begin) : 0;
-    const int row_end = p->row_end > p->row_begin ? static_cast<int>(p->row_end) : height;
-    const int spp = static_cast<int>(p->spp);
-    constexpr int tile = 32;
     const path_integrator integrator;
-    const auto start = std::chrono::steady_clock::now();
-    {
-        thread_pool pool(threads == 0 ? std::thread::hardware_concurrency() : threads);
-        for(int y0 = row_begin; y0 < row_end; y0 += tile) {
-            for(int x0 = 0; x0 < width; x0 += tile) {
-                const int x1 = std::min(x0 + tile, width);
-                const int y1 = std::min(y0 + tile, row_end);
-                pool.submit([&, x0, y0, x1, y1] {
-                    for(int y = y0; y < y1; ++y) {
-                        for(int x = x0; x < x1; ++x) {
-                            color sum(0.0f);
-                            color sum_sq(0.0f);
-                            for(int s = 0; s < spp; ++s) {
-                                const auto pixel_index = static_cast<uint32_t>(y * width + x);
-                                sampler smp;
-                                smp.start(pixel_index, static_cast<uint32_t>(s) + p->sample_offset);
-                                const auto offset = smp.next_2d();
-                                const auto u = (static_cast<float>(x) + offset.x) / static_cast<float>(width - 1);
-                                const auto v = (static_cast<float>(y) + offset.y) / static_cast<float>(height - 1);
-                                auto r = w.world->sensor().get_ray(u, v);
-                                const auto L = integrator.radiance(r, *w.world, smp);
-                                sum += L;
-                                sum_sq += L * L;
-                            }
-                            const size_t o = 3 * (static_cast<size_t>(y) * width + x);
-                            put3(rgb + o, sum / static_cast<float>(spp));
-                            if(rgb_sq) { put3(rgb_sq + o, sum_sq / static_cast<float>(spp)); }
-                        }
-                    }
-                });
-            }
-        }
-        pool.wait();
-    }
-    return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    return render_tiles(w, p, threads, rgb, rgb_sq,
+                        [&](ray& r, sampler& smp) { return integrator.radiance(r, *w.world, smp); });
+}
+
+// Photon-mapper image: photon_integrator::radiance with the given photon maps (built by
+// photon_map::build from the arrays) and radii in place of preprocess(), and run-time constants.
+double ref_photon_render(void* handle, const lrt_render_params* p, uint32_t threads, const lrt_photon* global,
+                         uint32_t n_global, float global_scale, const lrt_photon* caustic, uint32_t n_caustic,
+                         float caustic_scale, const lrt_photon_render_params* pp, float* rgb, float* rgb_sq) {
+    const auto& w = *static_cast<ref_world*>(handle);
+    lrt_ref_pm_max_depth = pp->max_depth;
+    lrt_ref_pm_max_specular_depth = pp->max_specular_depth;
+    lrt_ref_pm_direct_samples = pp->direct_samples;
+    lrt_ref_pm_glossy_samples = pp->glossy_samples;
+    lrt_ref_pm_lookup_size = pp->lookup_size;
+    photon_integrator integrator;
+    std::vector<photon> g(n_global), c(n_caustic);
+    for(uint32_t i = 0; i < n_global; ++i) { g[i] = to_photon(global[i]); }
+    for(uint32_t i = 0; i < n_caustic; ++i) { c[i] = to_photon(caustic[i]); }
+    if(n_global) { integrator.global_map.build(g, global_scale); }
+    if(n_caustic) { integrator.caustic_map.build(c, caustic_scale); }
+    integrator.global_radius = pp->global_radius;
+    integrator.caustic_radius = pp->caustic_radius;
+    return render_tiles(w, p, threads, rgb, rgb_sq,
+                        [&](ray& r, sampler& smp) { return integrator.radiance(r, *w.world, smp); });
 }
 
 // photon_tracer::trace_particle for particles [first, first+count), sampler.start(0, index) as

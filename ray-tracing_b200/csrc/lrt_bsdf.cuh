@@ -918,6 +918,34 @@ LRT_HD f3 rcoat_sample(const MatRec& m, const MatRec& n, const float* tables, co
     return rcoat_eval(m, n, tables, c, r, meas) / density;
 }
 
+// bsdf::component_flags (bsdf.h:62 default; dielectric_bsdf.h:25-27; plastic_bsdf.h:37-39;
+// rough_plastic_bsdf.h:41-43; coating_bsdf.h:39-41; rough_coating_bsdf.h:45-47)
+LRT_HD uint32_t base_component_flags(const MatRec& m, int component) {
+    switch(m.type) {
+    case LRT_DIELECTRIC: return component == 0 ? kDielRefl : kDielTrans;
+    case LRT_PLASTIC: return component == 0 ? kPlasticSpec : kPlasticDiff;
+    case LRT_ROUGH_PLASTIC: return component == 0 ? kRPlasticGlossy : kPlasticDiff;
+    default: return m.flags;
+    }
+}
+LRT_HD uint32_t bsdf_component_flags(const MatRec* mats, int32_t mid, int component) {
+    const MatRec& m = mats[mid];
+    if(m.type == LRT_COATING) return component == m.specular_component ? kCoatSpec : base_component_flags(mats[m.nested], component);
+    if(m.type == LRT_ROUGH_COATING) {
+        return component == m.specular_component ? kRCoatSpec : base_component_flags(mats[m.nested], component);
+    }
+    return base_component_flags(m, component);
+}
+// bsdf::diffuse_reflectance: the albedo of a diffuse BSDF, passed through by the coatings
+LRT_HD f3 bsdf_diffuse_reflectance(const MatRec* mats, int32_t mid) {
+    const MatRec& m = mats[mid];
+    if(m.type == LRT_COATING || m.type == LRT_ROUGH_COATING) {
+        const MatRec& n = mats[m.nested];
+        return n.type == LRT_DIFFUSE ? load3(n.diffuse) : mk(0.0f);
+    }
+    return m.type == LRT_DIFFUSE ? load3(m.diffuse) : mk(0.0f);
+}
+
 // ================= top-level dispatch =================
 LRT_HD f3 bsdf_sample(const MatRec* mats, const float* tables, int32_t mid, const BsdfCtx& c, BRec& r, float ux,
                       float uy) {

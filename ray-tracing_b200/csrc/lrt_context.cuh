@@ -106,7 +106,7 @@ struct lrt_context {
     // photons
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
-    lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg;
+    lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye;
 };
 
 namespace lrt {

@@ -412,38 +412,308 @@ __global__ void __launch_bounds__(kBlock) k_knn(MapView m, const float* points, 
     }
 }
 
+// photon_map::estimate_irradiance (photon_map.h:38-70), neighbours in heap pop order
+__device__ __forceinline__ f3 estimate_irradiance(const MapView& m, f3 point, f3 normal, float radius, int32_t max_depth,
+                                                 uint32_t k, KnnHeap& heap) {
+    f3 sum = mk(0.0f);
+    if(m.n == 0 || radius <= 0.0f || k == 0) return sum;
+    const float squared_radius = radius * radius;
+    knn_search(m, point, squared_radius, k, heap);
+    const float inverse_squared_radius = 1.0f / squared_radius;
+    while(heap.size > 0) {
+        const uint32_t pi = heap.i[0];
+        const float d2 = heap.d[0];
+        heap.pop();
+        const float4 dir = m.dir[pi];
+        if(__float_as_int(dir.w) > max_depth) continue;
+        const float4 pn = m.nrm[pi];
+        const f3 photon_normal{pn.x, pn.y, pn.z};
+        const f3 incoming = -f3{dir.x, dir.y, dir.z};
+        const float incoming_dot_photon = dot(photon_normal, incoming);
+        const float incoming_dot_shading = dot(normal, incoming);
+        if(incoming_dot_shading <= 0.0f || dot(photon_normal, normal) <= 1e-1f || incoming_dot_photon <= 1e-2f) {
+            continue;
+        }
+        const float square = 1.0f - d2 * inverse_squared_radius;
+        const float weight = (incoming_dot_shading / incoming_dot_photon) * (square * square);
+        const float4 pw = m.pw[pi];
+        sum += f3{pw.x, pw.y, pw.z} * fabsf(weight);
+    }
+    return sum * (m.scale * 3.0f * (1.0f / kPi) * inverse_squared_radius);
+}
+
 __global__ void __launch_bounds__(kBlock) k_irradiance(MapView m, const float* points, const float* normals, uint32_t n,
                                                        float radius, int32_t max_depth, uint32_t k, float* rgb) {
     for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        f3 sum = mk(0.0f);
-        if(m.n > 0 && radius > 0.0f && k > 0) {
-            const float squared_radius = radius * radius;
-            KnnHeap heap;
-            knn_search(m, load3(points + 3ull * q), squared_radius, k, heap);
-            const float inverse_squared_radius = 1.0f / squared_radius;
-            const f3 normal = load3(normals + 3ull * q);
-            while(heap.size > 0) {
-                const uint32_t pi = heap.i[0];
-                const float d2 = heap.d[0];
-                heap.pop();
-                const float4 dir = m.dir[pi];
-                if(__float_as_int(dir.w) > max_depth) continue;
-                const float4 pn = m.nrm[pi];
-                const f3 photon_normal{pn.x, pn.y, pn.z};
-                const f3 incoming = -f3{dir.x, dir.y, dir.z};
-                const float incoming_dot_photon = dot(photon_normal, incoming);
-                const float incoming_dot_shading = dot(normal, incoming);
-                if(incoming_dot_shading <= 0.0f || dot(photon_normal, normal) <= 1e-1f || incoming_dot_photon <= 1e-2f) {
-                    continue;
+        KnnHeap heap;
+        store3(rgb + 3ull * q, estimate_irradiance(m, load3(points + 3ull * q), load3(normals + 3ull * q), radius,
+                                                   max_depth, k, heap));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// photon-map eye pass: photon_integrator::li and its helpers (photon_integrator.h:39-296) with the
+// recursion as an explicit per-thread stack of frames. Frames run in the reference's depth-first
+// order, so every camera sample draws its sampler dimensions in the reference's order. A frame's
+// contributions are added to the sample's radiance times the product of the weights on the way down
+// (the reference multiplies the child's returned radiance instead: same terms, other rounding).
+
+constexpr int kEyeFrames = 128;  // one frame per recursion level: max_depth <= 128
+enum EyeStage : uint8_t { kEyeStart = 0, kEyeSpecular = 1, kEyeEmitters = 2, kEyeBsdf = 3 };
+
+struct EyeFrame {
+    f3 ro, rd;       // the ray li was called with
+    f3 p, n;         // its hit
+    f3 tp;           // weight of this frame's radiance in the camera sample
+    int32_t obj;     // hit object, -1 on a miss
+    int16_t depth;
+    int16_t iter;
+    uint8_t stage;
+    uint8_t evaluated;
+    uint8_t emission;
+    uint8_t front_face;
+};
+
+struct EyeParams {
+    MapView global, caustic;
+    float global_radius, caustic_radius;
+    int32_t max_depth, max_specular_depth, direct_samples, glossy_samples;
+    uint32_t lookup_size;
+};
+
+struct EyeCounts {
+    int emitter, bsdf;
+    float emitter_weight, bsdf_weight;
+};
+
+__device__ __forceinline__ EyeCounts eye_counts(const EyeParams& ep, int depth, bool diffuse) {
+    EyeCounts c{1, 1, 1.0f, 1.0f};  // photon_integrator.h:287-296
+    if(depth == 1) {
+        c.emitter = ep.direct_samples;
+        c.bsdf = diffuse ? ep.direct_samples : ep.glossy_samples;
+        c.emitter_weight = 1.0f / static_cast<float>(c.emitter);
+        c.bsdf_weight = 1.0f / static_cast<float>(c.bsdf);
+    }
+    return c;
+}
+
+__device__ f3 eye_sample(const DeviceScene& s, const EyeParams& ep, Sampler& smp, Ray camera, EyeFrame* st, KnnHeap& heap,
+                         int* overflow) {
+    const uint32_t(*table)[32] = sobol_table(s);
+    constexpr uint32_t kSmooth = kDiffuse | kGlossy;
+    TraceCount cnt{0, 0};
+    f3 L = mk(0.0f);
+    int top = 0;
+    st[0] = EyeFrame{camera.o, camera.d, mk(0.0f), mk(0.0f), mk(1.0f), -1, 1, 0, kEyeStart, 0, 1, 0};
+    while(top >= 0) {
+        EyeFrame& F = st[top];
+        const int32_t mid = F.obj >= 0 ? s.objects[F.obj].material : -1;
+        if(F.stage == kEyeStart) {
+            if(!F.evaluated) {
+                HitInfo h;
+                if(scene_hit<false>(s, Ray{F.ro, F.rd}, 0.001f, kInf, h, cnt)) {
+                    F.obj = h.object;
+                    F.p = h.p;
+                    F.n = h.normal;
+                    F.front_face = h.front_face ? 1 : 0;
+                } else {
+                    F.obj = -1;
                 }
-                const float square = 1.0f - d2 * inverse_squared_radius;
-                const float weight = (incoming_dot_shading / incoming_dot_photon) * (square * square);
-                const float4 pw = m.pw[pi];
-                sum += f3{pw.x, pw.y, pw.z} * fabsf(weight);
+                F.evaluated = 1;
             }
-            sum = sum * (m.scale * 3.0f * (1.0f / kPi) * inverse_squared_radius);
+            if(F.obj < 0) {
+                if(F.emission) L += F.tp * eval_environment(s, F.rd);
+                --top;
+                continue;
+            }
+            const ObjRec& o = s.objects[F.obj];
+            if(F.emission && o.emitter >= 0 && F.front_face) {
+                L += F.tp * area_emitted(s.emitters[o.emitter], F.n, -normalize(F.rd));
+            }
+            const int32_t m = o.material;
+            if(F.depth >= ep.max_depth || m < 0) {
+                --top;
+                continue;
+            }
+            const uint32_t flags = s.materials[m].flags;
+            const bool diffuse = (flags & (kDiffuse | kGlossy | kSpecular)) == kDiffuse;
+            if(diffuse && dot(F.n, F.rd) < 0.0f) {  // photon lookups (photon_integrator.h:95-106)
+                const int photon_depth = ep.max_depth - F.depth;
+                const f3 reflectance = bsdf_diffuse_reflectance(s.materials, m) * (1.0f / kPi);
+                if(ep.global.n > 0) {
+                    L += F.tp * (estimate_irradiance(ep.global, F.p, F.n, ep.global_radius, photon_depth, ep.lookup_size,
+                                                     heap) * reflectance);
+                }
+                if(ep.caustic.n > 0) {
+                    L += F.tp * (estimate_irradiance(ep.caustic, F.p, F.n, ep.caustic_radius, photon_depth,
+                                                     ep.lookup_size, heap) * reflectance);
+                }
+            }
+            F.stage = kEyeSpecular;
+            F.iter = 0;
+            continue;
         }
-        store3(rgb + 3ull * q, sum);
+        const uint32_t flags = s.materials[mid].flags;
+        const bool diffuse = (flags & (kDiffuse | kGlossy | kSpecular)) == kDiffuse;
+        const bool specular = (flags & kSpecular) != 0;
+        const bool smooth = (flags & kSmooth) != 0;
+        const bool exhaustive = specular && F.depth < ep.max_specular_depth;
+        const Onb basis = onb_from_normal(F.n);
+        BRec rec{};
+        rec.wi = to_local(basis, -normalize(F.rd));
+        rec.wo = mk(0.0f);
+        rec.front_face = F.front_face != 0;
+        rec.eta = 1.0f;
+        if(F.stage == kEyeSpecular) {  // specular_lobes (photon_integrator.h:126-155)
+            bool pushed = false;
+            if(exhaustive) {
+                const int count = s.materials[mid].component_count;
+                while(F.iter < count) {
+                    const int c = F.iter++;
+                    if((bsdf_component_flags(s.materials, mid, c) & kSpecular) == 0) continue;
+                    BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                    ctx.component = c;
+                    BRec r = rec;
+                    const f3 w = bsdf_sample(s.materials, s.tables, mid, ctx, r, 0.5f, 0.5f);
+                    if(is_zero(w)) continue;
+                    if(top + 1 >= kEyeFrames) {
+                        *overflow = 1;
+                        continue;
+                    }
+                    st[top + 1] = EyeFrame{F.p, to_world(basis, r.wo), mk(0.0f), mk(0.0f), F.tp * w, -1,
+                                           static_cast<int16_t>(F.depth + 1), 0, kEyeStart, 0, 1, 0};
+                    ++top;
+                    pushed = true;
+                    break;
+                }
+            }
+            if(pushed) continue;
+            F.stage = kEyeEmitters;
+        }
+        if(F.stage == kEyeEmitters) {  // emitter_samples (photon_integrator.h:157-217)
+            if(smooth) {
+                const EyeCounts counts = eye_counts(ep, F.depth, diffuse);
+                for(int i = 0; i < counts.emitter; ++i) {
+                    const F2 u = sampler_next_2d(table, smp);
+                    DirectSample light{};
+                    light.distance = kInf;
+                    if(!sample_emitter_direction(s, F.p, u.x, u.y, light)) continue;
+                    const f3 shadow_origin = F.p + F.n * 1e-4f;
+                    f3 shadow_dir = light.direction;
+                    float tmax = kInf;
+                    if(!isinf(light.distance)) {
+                        const f3 to_light = light.point - shadow_origin;
+                        const float distance = length(to_light);
+                        if(distance < 1e-6f) continue;
+                        shadow_dir = to_light / distance;
+                        tmax = distance * (1.0f - 1e-4f);
+                    }
+                    BRec r = rec;
+                    r.wo = to_local(basis, shadow_dir);
+                    BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                    if(!specular || exhaustive) ctx.type_mask = kSmooth;
+                    const f3 value = bsdf_eval(s.materials, s.tables, mid, ctx, r, kSolidAngle);
+                    if(is_zero(value)) continue;
+                    if(scene_occluded<false>(s, Ray{shadow_origin, shadow_dir}, 0.001f, tmax, light.emitter, cnt)) continue;
+                    const float light_pdf = pdf_emitter_direction(s, F.p, shadow_dir);
+                    const float bsdf_pdf_v = bsdf_pdf(s.materials, s.tables, mid, ctx, r, kSolidAngle);
+                    if(light_pdf <= 0.0f) continue;
+                    const float weight = power_heuristic(light_pdf * static_cast<float>(counts.emitter),
+                                                         bsdf_pdf_v * static_cast<float>(counts.bsdf)) * counts.emitter_weight;
+                    L += F.tp * (value * light.radiance * (weight / light_pdf));
+                }
+            }
+            F.stage = kEyeBsdf;
+            F.iter = 0;
+        }
+        // bsdf_samples (photon_integrator.h:219-277)
+        const bool sample_direct = smooth || (specular && !exhaustive);
+        const bool sample_indirect = !diffuse && (smooth || (specular && !exhaustive));
+        bool pushed = false;
+        if(sample_direct || sample_indirect) {
+            const EyeCounts counts = eye_counts(ep, F.depth, diffuse);
+            while(F.iter < counts.bsdf) {
+                ++F.iter;
+                BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                ctx.lobe_sample = sampler_next_1d(table, smp);
+                if(!specular || exhaustive) ctx.type_mask = kSmooth;
+                BRec r = rec;
+                const F2 u = sampler_next_2d(table, smp);
+                const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, r, u.x, u.y);
+                if(is_zero(weight) || r.pdf <= 0.0f) continue;
+                const Ray scattered{F.p, to_world(basis, r.wo)};
+                HitInfo occluder;
+                const bool hit = scene_hit<false>(s, scattered, 0.001f, kInf, occluder, cnt);
+                if(sample_direct) {
+                    f3 emission = mk(0.0f);
+                    float light_pdf = 0.0f;
+                    if(hit) {
+                        const ObjRec& oo = s.objects[occluder.object];
+                        if(oo.emitter >= 0 && occluder.front_face) {
+                            emission = area_emitted(s.emitters[oo.emitter], occluder.normal, -normalize(scattered.d));
+                            light_pdf = pdf_emitter_direction(s, F.p, scattered.d);
+                        }
+                    } else {
+                        emission = eval_environment(s, scattered.d);
+                        light_pdf = pdf_emitter_direction(s, F.p, scattered.d);
+                    }
+                    if(!is_zero(emission)) {
+                        const float mis = power_heuristic(r.pdf * static_cast<float>(counts.bsdf),
+                                                          light_pdf * static_cast<float>(counts.emitter)) * counts.bsdf_weight;
+                        L += F.tp * (emission * weight * mis);
+                    }
+                }
+                if(sample_indirect) {
+                    if(top + 1 >= kEyeFrames) {
+                        *overflow = 1;
+                        continue;
+                    }
+                    EyeFrame child{scattered.o, scattered.d, occluder.p, occluder.normal, F.tp * weight * counts.bsdf_weight,
+                                   hit ? occluder.object : -1, static_cast<int16_t>(F.depth + 1), 0, kEyeStart, 1, 0,
+                                   static_cast<uint8_t>(hit && occluder.front_face ? 1 : 0)};
+                    st[top + 1] = child;
+                    ++top;
+                    pushed = true;
+                    break;
+                }
+            }
+        }
+        if(!pushed) --top;
+    }
+    return L;
+}
+
+__global__ void __launch_bounds__(kBlock) k_photon_eye(DeviceScene s, EyeParams ep, uint32_t width, uint32_t height,
+                                                       uint32_t pixel_begin, uint32_t n_pixels, uint32_t sample_begin,
+                                                       uint32_t n_samples, float4* L_out, int* overflow) {
+    EyeFrame frames[kEyeFrames];
+    KnnHeap heap;
+    const uint32_t n = n_pixels * n_samples;
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const uint32_t pix = pixel_begin + slot / n_samples;
+        const uint32_t sample = sample_begin + slot % n_samples;
+        Sampler smp = sampler_start(pix, sample);
+        const F2 off = sampler_next_2d(sobol_table(s), smp);
+        const float u = (static_cast<float>(pix % width) + off.x) / static_cast<float>(width - 1);
+        const float v = (static_cast<float>(pix / width) + off.y) / static_cast<float>(height - 1);
+        const f3 L = eye_sample(s, ep, smp, camera_ray(s.cam, u, v), frames, heap, overflow);
+        L_out[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+    }
+}
+
+__global__ void k_photon_eye_accumulate(const float4* L, uint32_t pixel_begin, uint32_t n_pixels, uint32_t n_samples,
+                                        uint32_t spp, float* sum, int first, int last, float* rgb) {
+    const uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x;
+    if(pl >= n_pixels) return;
+    f3 acc = first ? mk(0.0f) : load3(sum + 3ull * pl);
+    for(uint32_t s = 0; s < n_samples; ++s) {
+        const float4 v = L[static_cast<size_t>(pl) * n_samples + s];
+        acc += f3{v.x, v.y, v.z};
+    }
+    if(last) {
+        store3(rgb + 3ull * (pixel_begin + pl), acc / static_cast<float>(spp));
+    } else {
+        store3(sum + 3ull * pl, acc);
     }
 }
 
@@ -737,6 +1007,132 @@ int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, co
     LRT_CUDA(ctx, cudaGetLastError());
     LRT_CUDA(ctx, cudaMemcpyAsync(rgb_out, base + 6ull * n, pb, cudaMemcpyDeviceToHost, ctx->stream));
     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// eye pass + preprocess entry points
+
+namespace {
+
+MapView view_or_empty(lrt_context* ctx, int32_t map) {
+    if(map < 0 || map >= kMaxPhotonMaps) return MapView{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 1.0f};
+    return view_of(ctx->maps[map]);
+}
+
+int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_photon_render_params* pp, float* rgb_dev) {
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(!p || !pp || p->width < 2 || p->height < 2 || p->spp == 0) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "render parameters out of range");
+    }
+    if(pp->lookup_size > kMaxKnn) return fail(ctx, LRT_ERR_RANGE, "lookup_size must be at most %u", kMaxKnn);
+    if(pp->max_depth < 1 || pp->max_depth > kEyeFrames || pp->direct_samples < 1 || pp->glossy_samples < 1) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon render parameters out of range");
+    }
+    const uint32_t row_begin = p->row_end > p->row_begin ? p->row_begin : 0u;
+    const uint32_t row_end = p->row_end > p->row_begin ? std::min(p->row_end, p->height) : p->height;
+    if(row_begin >= row_end) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "empty row range");
+    EyeParams ep;
+    ep.global = view_or_empty(ctx, pp->global_map);
+    ep.caustic = view_or_empty(ctx, pp->caustic_map);
+    ep.global_radius = pp->global_radius;
+    ep.caustic_radius = pp->caustic_radius;
+    ep.max_depth = pp->max_depth;
+    ep.max_specular_depth = pp->max_specular_depth;
+    ep.direct_samples = pp->direct_samples;
+    ep.glossy_samples = pp->glossy_samples;
+    ep.lookup_size = pp->lookup_size;
+    const uint32_t cap = 1u << 20;
+    LRT_CUDA(ctx, ctx->ph_eye.ensure(16ull * cap + 12ull * cap + 64));
+    float4* L = ctx->ph_eye.as<float4>();
+    float* sum = reinterpret_cast<float*>(L + cap);
+    int* overflow = reinterpret_cast<int*>(sum + 3ull * cap);
+    LRT_CUDA(ctx, cudaMemsetAsync(overflow, 0, 4, ctx->stream));
+    const int grid = grid_for(ctx, (const void*)k_photon_eye, kBlock);
+    const uint32_t spp = p->spp;
+    const uint32_t samples_per_wave = std::min(spp, cap);
+    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
+    const uint32_t pix0 = row_begin * p->width, pix1 = row_end * p->width;
+    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
+        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
+        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
+            const uint32_t ns = std::min(samples_per_wave, spp - sb);
+            k_photon_eye<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, ep, p->width, p->height, pb, np, p->sample_offset + sb,
+                                                           ns, L, overflow);
+            k_photon_eye_accumulate<<<blocks_for(np), kBlock, 0, ctx->stream>>>(L, pb, np, ns, spp, sum, sb == 0 ? 1 : 0,
+                                                                                sb + ns >= spp ? 1 : 0, rgb_dev);
+            LRT_CUDA(ctx, cudaGetLastError());
+            ctx->stats.kernel_launches += 2;
+        }
+    }
+    int h_overflow = 0;
+    LRT_CUDA(ctx, cudaMemcpyAsync(&h_overflow, overflow, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stats.paths += static_cast<uint64_t>(pix1 - pix0) * spp;
+    if(h_overflow) return fail(ctx, LRT_ERR_RANGE, "photon eye pass: recursion deeper than %d levels", kEyeFrames);
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_render_photon_dev(lrt_context* ctx, const lrt_render_params* params, const lrt_photon_render_params* pp,
+                          float* rgb_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null output");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    return photon_render_impl(ctx, params, pp, rgb_dev);
+}
+
+int lrt_render_photon(lrt_context* ctx, const lrt_render_params* params, const lrt_photon_render_params* pp, float* rgb) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!rgb || !params) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(params->width) * params->height;
+    LRT_CUDA(ctx, ctx->out_rgb.ensure(bytes));
+    LRT_CUDA(ctx, cudaMemsetAsync(ctx->out_rgb.ptr, 0, bytes, ctx->stream));
+    const int st = photon_render_impl(ctx, params, pp, ctx->out_rgb.as<float>());
+    if(st != LRT_OK) return st;
+    LRT_CUDA(ctx, cudaMemcpyAsync(rgb, ctx->out_rgb.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
+// photon_integrator::preprocess (photon_integrator.h:15-37): radii from the scene's bounding sphere
+// (capped at radius_cap), the global gather, the caustic gather when the scene has a specular BSDF, and
+// a map for each gather that reached its request (maps 0 and 1).
+int lrt_photon_preprocess(lrt_context* ctx, uint32_t global_photons, uint32_t caustic_photons, int32_t max_depth,
+                          int32_t rr_depth, float radius_cap, lrt_photon_render_params* out, uint64_t* shots) {
+    if(!ctx || !out) return LRT_ERR_INVALID_ARGUMENT;
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    const float radius = ctx->host.bounding_radius;
+    out->global_radius = smin(radius_cap, 0.05f * radius);
+    out->caustic_radius = smin(radius_cap, 0.0125f * radius);
+    out->global_map = -1;
+    out->caustic_map = -1;
+    const uint32_t requested[2] = {global_photons, ctx->host.has_delta_bsdf ? caustic_photons : 0u};
+    const int32_t kinds[2] = {LRT_GATHER_SURFACE, LRT_GATHER_CAUSTIC};
+    for(int m = 0; m < 2; ++m) {
+        if(shots) shots[m] = 0;
+        if(requested[m] == 0) continue;
+        std::vector<lrt_photon> photons(requested[m]);
+        uint32_t n = 0;
+        uint64_t shot = 0;
+        int st = lrt_photon_trace(ctx, kinds[m], requested[m], max_depth - 1, rr_depth, photons.data(), &n, &shot);
+        if(st != LRT_OK) return st;
+        if(shots) shots[m] = shot;
+        if(n != requested[m]) continue;  // not full: the reference leaves the map empty
+        st = lrt_photon_map_build(ctx, m, photons.data(), n, 1.0f / static_cast<float>(shot));
+        if(st != LRT_OK) return st;
+        if(m == 0) {
+            out->global_map = 0;
+        } else {
+            out->caustic_map = 1;
+        }
+    }
     return LRT_OK;
 }
 

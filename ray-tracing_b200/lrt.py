@@ -30,6 +30,7 @@ EXPORTS = [
     "lrt_render_dev_noalloc",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
+    "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
 ]
 
 
@@ -83,6 +84,9 @@ def lib():
         L.lrt_photon_map_build.argtypes = [vp, i32, P(abi.Photon), u32, f32]
         L.lrt_photon_knn.argtypes = [vp, i32, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
         L.lrt_photon_irradiance.argtypes = [vp, i32, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
+        L.lrt_photon_preprocess.argtypes = [vp, u32, u32, i32, i32, f32, P(abi.PhotonRenderParams), P(u64)]
+        L.lrt_render_photon.argtypes = [vp, P(abi.RenderParams), P(abi.PhotonRenderParams), P(f32)]
+        L.lrt_render_photon_dev.argtypes = [vp, P(abi.RenderParams), P(abi.PhotonRenderParams), vp]
         _lib = L
     return _lib
 
@@ -277,6 +281,24 @@ class Context:
         self._check(lib().lrt_photon_knn(self.handle, map_id, ptr(points, C.c_float), n, r2, k, ptr(idx, C.c_uint32),
                                          ptr(d2, C.c_float), ptr(cnt, C.c_uint32)))
         return idx, d2, cnt
+
+    def photon_preprocess(self, global_photons: int, caustic_photons: int, max_depth: int = 128, rr_depth: int = 5,
+                          radius_cap: float = float("inf"), lookup_size: int = 120):
+        pp = abi.PhotonRenderParams.reference_defaults(lookup_size)
+        pp.max_depth = max_depth
+        shots = (C.c_uint64 * 2)()
+        self._check(lib().lrt_photon_preprocess(self.handle, global_photons, caustic_photons, max_depth, rr_depth,
+                                                radius_cap, C.byref(pp), shots))
+        return pp, (shots[0], shots[1])
+
+    def render_photon(self, params: abi.RenderParams, pp: abi.PhotonRenderParams, out: np.ndarray | None = None):
+        if out is None:
+            out = np.zeros((params.height, params.width, 3), dtype=np.float32)
+        self._check(lib().lrt_render_photon(self.handle, C.byref(params), C.byref(pp), ptr(out, C.c_float)))
+        return out
+
+    def render_photon_dev(self, params: abi.RenderParams, pp: abi.PhotonRenderParams, rgb_ptr: int):
+        self._check(lib().lrt_render_photon_dev(self.handle, C.byref(params), C.byref(pp), C.c_void_p(rgb_ptr)))
 
     def photon_irradiance(self, map_id: int, points, normals, radius: float, max_depth: int, k: int):
         points = np.ascontiguousarray(points, dtype=np.float32)

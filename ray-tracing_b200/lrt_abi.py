@@ -110,6 +110,17 @@ class RenderParams(C.Structure):
                 ("row_end", C.c_uint32)]
 
 
+class PhotonRenderParams(C.Structure):
+    _fields_ = [("global_map", C.c_int32), ("caustic_map", C.c_int32), ("global_radius", C.c_float),
+                ("caustic_radius", C.c_float), ("max_depth", C.c_int32), ("max_specular_depth", C.c_int32),
+                ("direct_samples", C.c_int32), ("glossy_samples", C.c_int32), ("lookup_size", C.c_uint32)]
+
+    @classmethod
+    def reference_defaults(cls, lookup_size=120):
+        """photon_integrator.h:57-65"""
+        return cls(-1, -1, 0.0, 0.0, 128, 4, 16, 32, lookup_size)
+
+
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("nodes_visited", C.c_uint64), ("triangles_tested", C.c_uint64),

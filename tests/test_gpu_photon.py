@@ -129,6 +129,47 @@ def test_irradiance_golden(ctx, k, radius, depth):
     assert rel_close(out, g["irr_%d" % k], 1e-5, 1e-9).all()
 
 
+@pytest.mark.parametrize("material", ["diffuse", "coating", "rough_conductor", "rough_dielectric"])
+def test_photon_eye_pass_matches_reference(ctx, material):
+    """photon_integrator::radiance on the GPU against the reference with the same photon maps (built by both
+    from the same photon arrays) and the same samples: per pixel within 3 standard errors of the
+    reference's own per-pixel spread (the allowed 1% covers the 3-sigma tail and paths that diverge after a
+    last-bit difference of a transcendental function)"""
+    if not oracle.reference_available():
+        pytest.skip("reference oracle not built")
+    sc = scenes.cornell_box(material=material, level=4)
+    ctx.upload(sc)
+    g, shot_g = ctx.photon_trace(abi.GATHER_SURFACE, 20000, 127, 5)
+    c, shot_c = ctx.photon_trace(abi.GATHER_CAUSTIC, 20000, 127, 5)
+    if len(c) < 20000:
+        c = c[:0]
+    pp = abi.PhotonRenderParams.reference_defaults(lookup_size=64)
+    pp.global_radius, pp.caustic_radius = 0.1, 0.025
+    ctx.photon_map_build(0, g, 1.0 / shot_g)
+    pp.global_map = 0
+    if len(c):
+        ctx.photon_map_build(1, c, 1.0 / shot_c)
+        pp.caustic_map = 1
+    params = scenes.render_params(24, 24, 4, 8, 3)
+    img = ctx.render_photon(params, pp)
+    ref, sq, _ = oracle.RefWorld(sc).render_photon(params, pp, g, np.float32(1.0 / shot_g), c,
+                                                   np.float32(1.0 / shot_c) if len(c) else np.float32(1.0))
+    se = np.sqrt(np.maximum(sq - ref * ref, 0.0) / 4)
+    z = np.abs(img - ref) / (se + 1e-6 * np.maximum(ref, 1e-3))
+    assert (z > 3).mean() <= 0.01, "%s: fraction beyond 3 sigma %g" % (material, (z > 3).mean())
+    assert abs(img.mean() - ref.mean()) <= 0.02 * ref.mean()
+
+
+def test_photon_preprocess_radii_and_maps(ctx):
+    sc = scenes.cornell_box(material="coating", level=3)
+    ctx.upload(sc)
+    pp, shots = ctx.photon_preprocess(5000, 5000, 128, 5, radius_cap=0.05, lookup_size=64)
+    assert pp.global_map == 0 and pp.caustic_map == 1 and shots[0] > 0 and shots[1] > 0
+    assert pp.global_radius <= np.float32(0.05) and 0.0 < pp.caustic_radius <= pp.global_radius
+    img = ctx.render_photon(scenes.render_params(16, 16, 2, 8, 3), pp)
+    assert np.isfinite(img).all() and img.mean() > 0
+
+
 def test_empty_map(ctx):
     ctx.upload(scenes.cornell_box(level=1))
     ctx.photon_map_build(2, np.zeros(0, dtype=abi.PHOTON_DTYPE), 1.0)
