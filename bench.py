@@ -183,7 +183,8 @@ def run_lrt(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # the library's stream; flushes and timing events go on it too
+    torch.cuda.set_stream(stream)
 
     ctxs = []
     for m in MATERIALS:
@@ -315,6 +316,94 @@ def run_lrt(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+# batched workload: 64 seeded jobs (resolution, spp 4-256, camera, sphere material) on the open box
+
+BATCH_METRIC = "jobs/s (64 seeded jobs: 128^2..1024x768, 4-256 spp, 7 materials, depth 8)"
+
+
+def run_batch(args):
+    import torch
+    import lrt
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)  # the library's stream; flushes and timing events go on it too
+    torch.cuda.set_stream(stream)
+    scene, sphere, index = scenes.open_box_library()
+    jobs, specs = scenes.batch_jobs(index, sphere, n_jobs=args.jobs)
+    n_paths = sum(j["width"] * j["height"] * j["spp"] for j in specs)
+    floats = max(j["output_offset"] + 3 * j["width"] * j["height"] for j in specs)
+    ctx = lrt.Context(local, stream.cuda_stream)
+    ctx.upload(scene)
+    out = torch.zeros(floats, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def batched():
+        ctx.render_batch_dev(jobs, DEPTH, RR, out.data_ptr())
+
+    def per_job_plain():
+        for j in jobs:
+            ctx.render_plain_dev([j], DEPTH, RR, out.data_ptr())
+
+    def per_job_wavefront():
+        for j in jobs:
+            ctx.render_batch_dev([j], DEPTH, RR, out.data_ptr())
+
+    arms = {"batched": batched, "per_job_plain": per_job_plain, "per_job_wavefront": per_job_wavefront}
+    results, images = {}, {}
+    clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+    clocks.start()
+    for name, fn in arms.items():
+        if name == "per_job_wavefront":
+            ctx.set_option("batch_graph", 0)
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ctx.reset_stats()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        ctx.set_option("batch_graph", 1)
+        total = sum(ms) / 1000.0
+        results[name] = {"jobs_per_s": len(jobs) * args.steps / total, "ms_per_step": 1000 * total / args.steps,
+                         "mpaths_per_s": n_paths * args.steps / total / 1e6,
+                         "gpu_launches": int(ctx.stats()["kernel_launches"])}
+        images[name] = out.cpu().numpy()
+    clock_info = clocks.stop()
+    same = all(np.array_equal(images["batched"], images[k]) for k in images)
+
+    # end to end: lrt_render_batch with the host output buffer
+    host = np.zeros(floats, dtype=np.float32)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.render_batch(jobs, DEPTH, RR, host)
+    e2e = len(jobs) * args.steps / (time.perf_counter() - t0)
+    b = results["batched"]
+    line = {"metric": BATCH_METRIC, "value": b["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": b["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes.batch_jobs)",
+            "config": {"workload": "batch_%d_jobs_seed_%d" % (len(jobs), scenes.BATCH_SEED), "jobs": len(jobs),
+                       "paths_per_step": n_paths, "max_depth": DEPTH, "rr_depth": RR,
+                       "l2": "flushed (256 MB write) between timed steps", "arms": results,
+                       "images_identical_across_arms": same},
+            "e2e": {"value": e2e, "unit": "jobs/s", "h2d_bytes_per_step": 80 * len(jobs),
+                    "d2h_bytes_per_step": 4 * floats, "path": "lrt_render_batch (host output buffer)"},
+            "clocks": clock_info, "gpu_launches": b["gpu_launches"]}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def abi_stage_names():
     import lrt_abi
     return lrt_abi.STAGE_NAMES
@@ -327,9 +416,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lrt", choices=["lrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="paths", choices=["paths", "batch"],
+                    help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison")
+    ap.add_argument("--jobs", type=int, default=64)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_lrt(args)
 
 

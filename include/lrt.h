@@ -336,6 +336,38 @@ int lrt_render_dev(lrt_context* ctx, const lrt_render_params* params, float* rgb
  * stream capture. Calls share the array: calls that overlap on the GPU race. */
 int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev);
 
+/* One render job of a batch: its own pinhole camera, resolution, samples and (optionally) the material
+ * of one object replaced, rendered over the uploaded scene exactly as lrt_render would render it with
+ * that camera and material. Its image (width*height*3 floats, layout of lrt_render) starts at float
+ * `output_offset` of the batch's output buffer. */
+typedef struct lrt_job_desc {
+    lrt_camera_desc camera;
+    uint32_t width;
+    uint32_t height;
+    uint32_t spp;
+    uint32_t sample_offset;
+    int32_t override_object;    /* -1: none */
+    int32_t override_material;
+    uint64_t output_offset;
+} lrt_job_desc;
+
+/* Many jobs in shared waves: the paths of all jobs fill the same wavefront queues, and the launch
+ * sequence of one wave is captured once as a CUDA graph and replayed for every wave (the wave cursor
+ * lives in device memory). No counterpart in the reference, whose main renders one image; a
+ * reference-side caller would otherwise loop lrt_render over its jobs. */
+int lrt_render_batch(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                     int32_t rr_depth, float* rgb);
+int lrt_render_batch_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                         int32_t rr_depth, float* rgb_dev);
+
+/* The plain GPU path tracer, for comparison: one kernel launch per job, one thread per pixel running
+ * the reference's render loop (main.cpp:121-136 over path_integrator::li, path_integrator.h:23-166)
+ * with the whole path in registers. Same jobs, output layout and images as lrt_render_batch. */
+int lrt_render_plain(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                     int32_t rr_depth, float* rgb);
+int lrt_render_plain_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                         int32_t rr_depth, float* rgb_dev);
+
 /* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
 int lrt_render_stats_reset(lrt_context* ctx);

@@ -26,6 +26,39 @@
 
 using namespace lrt;
 
+namespace lrt {
+
+int job_records(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, std::vector<JobRec>& recs,
+                unsigned long long& total, unsigned long long& out_floats) {
+    recs.resize(n_jobs);
+    total = 0;
+    out_floats = 0;
+    for(uint32_t i = 0; i < n_jobs; ++i) {
+        const lrt_job_desc& j = jobs[i];
+        if(j.width < 2 || j.height < 2 || j.spp == 0) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "job %u: bad size", i);
+        if(static_cast<uint64_t>(j.width) * j.height > 0x3fffffffull) return fail(ctx, LRT_ERR_RANGE, "job %u: image too large", i);
+        if(j.override_object >= ctx->ds.n_objects || j.override_material >= ctx->ds.n_materials ||
+           (j.override_object >= 0 && j.override_material < 0)) {
+            return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "job %u: material override out of range", i);
+        }
+        JobRec& r = recs[i];
+        r.cam = camera_from_desc(j.camera);
+        r.width = j.width;
+        r.height = j.height;
+        r.spp = j.spp;
+        r.sample_offset = j.sample_offset;
+        r.override_obj = j.override_object;
+        r.override_mat = j.override_object >= 0 ? j.override_material : -1;
+        r.path_begin = total;
+        r.out_offset = j.output_offset;
+        total += static_cast<unsigned long long>(j.width) * j.height * j.spp;
+        out_floats = std::max<unsigned long long>(out_floats, j.output_offset + 3ull * j.width * j.height);
+    }
+    return LRT_OK;
+}
+
+}  // namespace lrt
+
 namespace {
 
 template <typename T>
@@ -181,7 +214,25 @@ struct WaveArgs {
     uint32_t sample_begin;   // first sample index of the wave
     uint32_t n_samples;      // samples per pixel in this wave
     int32_t max_depth, rr_depth;
+    // batched jobs (null for single-image renders)
+    const JobRec* jobs;
+    uint32_t n_jobs;
+    uint32_t* path_job;             // job of each slot
+    unsigned long long* wave_base;  // first batch path of the current wave (device, advanced per wave)
+    unsigned long long total_paths;
+    float* batch_out;
+    float* batch_sums;              // running per-pixel sums where a pixel spans waves
 };
+
+// the material of object `obj` for path `pid`: a batch job may replace one object's material
+__device__ __forceinline__ int32_t effective_material(const WaveArgs& a, uint32_t pid, int32_t obj) {
+    int32_t m = a.s.objects[obj].material;
+    if(a.jobs) {
+        const JobRec& j = a.jobs[a.path_job[pid]];
+        if(obj == j.override_obj) m = j.override_mat;
+    }
+    return m;
+}
 
 __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
     const uint32_t n = a.n_pixels * a.n_samples;
@@ -316,7 +367,7 @@ __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
             const MeshHit mh{raw.x, raw.y, raw.z, __float_as_uint(a.hit_n[pid].x)};
             HitInfo h;
             hit_record_of(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, best, raw.x, mh, h);
-            const int32_t mat = a.s.objects[best].material;
+            const int32_t mat = effective_material(a, pid, best);
             key = mat < 0 ? 1 : 2 + a.s.materials[mat].type;
             a.hit_p[pid] = make_float4(h.p.x, h.p.y, h.p.z, __int_as_float(h.object));
             a.hit_n[pid] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.front_face ? 1.0f : 0.0f);
@@ -450,7 +501,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
             continue;
         }
         ++shading;
-        const int32_t mid = obj.material;
+        const int32_t mid = effective_material(a, pid, __float_as_int(hp.w));
         const Onb basis = onb_from_normal(normal);
         BRec rec{};
         rec.wi = to_local(basis, -normalize(rd));
@@ -582,6 +633,82 @@ __global__ void __launch_bounds__(kBlock) k_accumulate(WaveArgs a, float* rgb, u
             store3(a.sum + 3ull * pl, acc);
         }
     }
+}
+
+// ---- batched jobs ----
+
+__device__ __forceinline__ uint32_t wave_slots(const WaveArgs& a) {
+    const unsigned long long base = *a.wave_base;
+    if(base >= a.total_paths) return 0u;
+    const unsigned long long left = a.total_paths - base;
+    return left < a.capacity ? static_cast<uint32_t>(left) : a.capacity;
+}
+
+// camera rays of the batch paths [wave_base, wave_base + capacity)
+__global__ void __launch_bounds__(kBlock) k_raygen_batch(WaveArgs a) {
+    const unsigned long long base = *a.wave_base;
+    const uint32_t n = wave_slots(a);
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const unsigned long long g = base + slot;
+        uint32_t lo = 0, hi = a.n_jobs;  // last job with path_begin <= g
+        while(hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if(a.jobs[mid].path_begin <= g) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
+        }
+        const JobRec& job = a.jobs[lo];
+        const unsigned long long local = g - job.path_begin;
+        const uint32_t pix = static_cast<uint32_t>(local / job.spp);
+        const uint32_t sample = job.sample_offset + static_cast<uint32_t>(local % job.spp);
+        Sampler smp = sampler_start(pix, sample);
+        const F2 off = sampler_next_2d(sobol_table(a.s), smp);
+        const float u = (static_cast<float>(pix % job.width) + off.x) / static_cast<float>(job.width - 1);
+        const float v = (static_cast<float>(pix / job.width) + off.y) / static_cast<float>(job.height - 1);
+        const Ray r = camera_ray(job.cam, u, v);
+        a.o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+        a.d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
+        a.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        a.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        a.misc[slot] = make_float2(0.0f, 0.0f);
+        a.id[slot] = make_uint2(pix, sample);
+        a.path_job[slot] = lo;
+        const int seg = heavy_key(a.s, r, 0.001f, kInf);
+        a.q0[static_cast<size_t>(seg) * a.capacity + warp_append_keyed(a.counters[0].active, seg)] = slot;
+    }
+}
+
+// per pixel run of the wave (consecutive slots of one job pixel), in sample order: the run's sum joins
+// the pixel's running sum; the run holding the pixel's last sample writes sum / spp
+__global__ void __launch_bounds__(kBlock) k_accumulate_batch(WaveArgs a) {
+    const uint32_t n = wave_slots(a);
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const uint32_t job_i = a.path_job[slot];
+        const uint2 ident = a.id[slot];
+        if(slot > 0 && a.path_job[slot - 1] == job_i && a.id[slot - 1].x == ident.x) continue;
+        const JobRec& job = a.jobs[job_i];
+        const unsigned long long px = job.out_offset + 3ull * ident.x;
+        f3 acc = ident.y == job.sample_offset ? mk(0.0f) : load3(a.batch_sums + px);
+        uint32_t k = slot;
+        uint32_t last_sample = ident.y;
+        while(k < n && a.path_job[k] == job_i && a.id[k].x == ident.x) {
+            const float4 L = a.L[k];
+            acc += f3{L.x, L.y, L.z};
+            last_sample = a.id[k].y;
+            ++k;
+        }
+        if(last_sample == job.sample_offset + job.spp - 1) {
+            store3(a.batch_out + px, acc / static_cast<float>(job.spp));
+        } else {
+            store3(a.batch_sums + px, acc);
+        }
+    }
+}
+
+__global__ void k_wave_advance(WaveArgs a) {
+    if(blockIdx.x == 0 && threadIdx.x == 0) *a.wave_base += a.capacity;
 }
 
 int ensure_wave(lrt_context* ctx, uint32_t cap) {
@@ -758,6 +885,110 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
             ctx->stats.shadow_triangles_tested += h[6];
         }
     }
+    return LRT_OK;
+}
+
+
+// The launch sequence of one wave of a batch (also what the CUDA graph holds).
+void launch_batch_wave(lrt_context* ctx, const WaveArgs& a, size_t counters_bytes, int g_raygen, int g_extend,
+                       int g_hitrec, int g_shade, int g_shadow, int g_accum) {
+    cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream);
+    k_raygen_batch<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
+    for(int depth = 0; depth < a.max_depth; ++depth) {
+        k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+        k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
+        k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+        k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+    }
+    k_accumulate_batch<<<g_accum, kBlock, 0, ctx->stream>>>(a);
+    k_wave_advance<<<1, 32, 0, ctx->stream>>>(a);
+}
+
+int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
+                      float* rgb_dev) {
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n_jobs == 0) return LRT_OK;
+    if(!jobs || !rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    if(max_depth < 1 || max_depth > 1024) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "max_depth out of range");
+    std::vector<JobRec> recs;
+    unsigned long long total = 0, out_floats = 0;
+    const int jst = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
+    if(jst != LRT_OK) return jst;
+    const uint32_t cap = ctx->wave_capacity;
+    int st = ensure_wave(ctx, cap);
+    if(st != LRT_OK) return st;
+    const size_t counters_bytes = sizeof(BounceCounters) * (max_depth + 1);
+    LRT_CUDA(ctx, ctx->counters.ensure(counters_bytes));
+    LRT_CUDA(ctx, ctx->batch_jobs.ensure(sizeof(JobRec) * n_jobs));
+    LRT_CUDA(ctx, ctx->batch_path_job.ensure(4ull * cap));
+    LRT_CUDA(ctx, ctx->batch_sums.ensure(4ull * out_floats));
+    LRT_CUDA(ctx, ctx->batch_cursor.ensure(8));
+    LRT_CUDA(ctx, cudaMemcpyAsync(ctx->batch_jobs.ptr, recs.data(), sizeof(JobRec) * n_jobs, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    LRT_CUDA(ctx, cudaMemsetAsync(ctx->batch_cursor.ptr, 0, 8, ctx->stream));
+    WaveState& w = ctx->wave;
+    WaveArgs a{};
+    a.s = ctx->ds;
+    a.o = w.o.as<float4>();
+    a.d = w.d.as<float4>();
+    a.tp = w.tp.as<float4>();
+    a.L = w.L.as<float4>();
+    a.misc = w.misc.as<float2>();
+    a.id = w.id.as<uint2>();
+    a.hit_p = w.hit_p.as<float4>();
+    a.hit_n = w.hit_n.as<float4>();
+    a.q0 = w.q0.as<uint32_t>();
+    a.q1 = w.q1.as<uint32_t>();
+    a.keyed = w.keyed.as<uint32_t>();
+    a.sh_o = w.sh_o.as<float4>();
+    a.sh_d = w.sh_d.as<float4>();
+    a.sh_c = w.sh_c.as<float4>();
+    a.counters = ctx->counters.as<BounceCounters>();
+    a.sum = w.sum.as<float>();
+    a.capacity = cap;
+    a.max_depth = max_depth;
+    a.rr_depth = rr_depth;
+    a.work = nullptr;
+    a.jobs = ctx->batch_jobs.as<JobRec>();
+    a.n_jobs = n_jobs;
+    a.path_job = ctx->batch_path_job.as<uint32_t>();
+    a.wave_base = ctx->batch_cursor.as<unsigned long long>();
+    a.total_paths = total;
+    a.batch_out = rgb_dev;
+    a.batch_sums = ctx->batch_sums.as<float>();
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
+    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
+    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
+    const int g_accum = grid_for(ctx, (const void*)k_accumulate_batch, kBlock);
+    const unsigned long long waves = (total + cap - 1) / cap;
+    const uint64_t per_wave = 3 + 4ull * max_depth;
+    if(ctx->batch_graph) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        LRT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if(ce != cudaSuccess) return fail(ctx, LRT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        if(ie != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return fail(ctx, LRT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+        }
+        cudaError_t le = cudaSuccess;
+        for(unsigned long long i = 0; i < waves && le == cudaSuccess; ++i) le = cudaGraphLaunch(exec, ctx->stream);
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if(le != cudaSuccess) return fail(ctx, LRT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(le));
+    } else {
+        for(unsigned long long i = 0; i < waves; ++i) {
+            launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
+        }
+        LRT_CUDA(ctx, cudaGetLastError());
+    }
+    ctx->stats.paths += total;
+    ctx->stats.kernel_launches += waves * per_wave;
     return LRT_OK;
 }
 
@@ -1072,6 +1303,32 @@ int lrt_render(lrt_context* ctx, const lrt_render_params* params, float* rgb) {
     return LRT_OK;
 }
 
+int lrt_render_batch_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
+                         float* rgb_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    return render_batch_impl(ctx, jobs, n_jobs, max_depth, rr_depth, rgb_dev);
+}
+
+int lrt_render_batch(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
+                     float* rgb) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(n_jobs == 0) return LRT_OK;
+    if(!jobs || !rgb) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned long long floats = 0;
+    for(uint32_t i = 0; i < n_jobs; ++i) {
+        floats = std::max<unsigned long long>(floats, jobs[i].output_offset + 3ull * jobs[i].width * jobs[i].height);
+    }
+    LRT_CUDA(ctx, ctx->batch_out.ensure(4ull * floats));
+    LRT_CUDA(ctx, cudaMemsetAsync(ctx->batch_out.ptr, 0, 4ull * floats, ctx->stream));
+    const int st = render_batch_impl(ctx, jobs, n_jobs, max_depth, rr_depth, ctx->batch_out.as<float>());
+    if(st != LRT_OK) return st;
+    LRT_CUDA(ctx, cudaMemcpyAsync(rgb, ctx->batch_out.ptr, 4ull * floats, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LRT_OK;
+}
+
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out) {
     if(!ctx || !out) return LRT_ERR_INVALID_ARGUMENT;
     *out = ctx->stats;
@@ -1090,6 +1347,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->stage_timing = value != 0;
     } else if(strcmp(name, "count_work") == 0) {
         ctx->count_work = value != 0;
+    } else if(strcmp(name, "batch_graph") == 0) {
+        ctx->batch_graph = value != 0;
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
     } else if(strcmp(name, "wave_capacity") == 0) {

@@ -97,6 +97,8 @@ struct lrt_context {
     // render
     lrt::WaveState wave;
     lrt::DevBuf out_rgb, scratch_a, scratch_b, counters;
+    lrt::DevBuf batch_jobs, batch_path_job, batch_sums, batch_cursor, batch_out;
+    bool batch_graph = true;
     lrt_render_stats stats{};
     bool stage_timing = false;
     bool count_work = false;
@@ -129,6 +131,11 @@ inline int fail(lrt_context* ctx, int code, const char* fmt, ...) {
                                "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);          \
         }                                                                                                     \
     } while(0)
+
+// Validates a batch's jobs and lays out their path ranges (pixel-major, samples inner) and outputs;
+// total = the batch's paths, out_floats = the output floats the jobs reach.
+int job_records(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, std::vector<JobRec>& recs,
+                unsigned long long& total, unsigned long long& out_floats);
 
 inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 

@@ -665,6 +665,28 @@ void sobol_direction_table(uint32_t table[16][32]) {
 
 // ------------------------------------------------------------------------------------------------
 
+CamRec camera_from_desc(const lrt_camera_desc& c) {
+    const f3 origin = load3(c.origin);
+    const f3 look_at = load3(c.look_at);
+    const float radians = c.fov_degrees * kPi / 180.0f;
+    const float h = tanf(radians / 2.0f);
+    const float viewport_height = 2.0f * h;
+    const float viewport_width = c.aspect_ratio * viewport_height;
+    const float focus_dist = 1.0f;
+    const f3 w = normalize(origin - look_at);
+    const f3 u = normalize(cross(load3(c.up), w));
+    const f3 v = cross(w, u);
+    const f3 horizontal = focus_dist * viewport_width * u;
+    const f3 vertical = focus_dist * viewport_height * v;
+    const f3 llc = origin - horizontal / 2.0f - vertical / 2.0f - focus_dist * w;
+    CamRec cam{};
+    store3(cam.origin, origin);
+    store3(cam.llc, llc);
+    store3(cam.horizontal, horizontal);
+    store3(cam.vertical, vertical);
+    return cam;
+}
+
 int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
     s = HostScene{};
     if(!d) {
@@ -936,27 +958,7 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
     }
     s.emission_power = sum;
 
-    // ---- camera: camera::update (camera.h:20-44), pinhole, focus distance 1 ----
-    {
-        const lrt_camera_desc& c = d->camera;
-        const f3 origin = load3(c.origin);
-        const f3 look_at = load3(c.look_at);
-        const float radians = c.fov_degrees * kPi / 180.0f;
-        const float h = tanf(radians / 2.0f);
-        const float viewport_height = 2.0f * h;
-        const float viewport_width = c.aspect_ratio * viewport_height;
-        const float focus_dist = 1.0f;
-        const f3 w = normalize(origin - look_at);
-        const f3 u = normalize(cross(load3(c.up), w));
-        const f3 v = cross(w, u);
-        const f3 horizontal = focus_dist * viewport_width * u;
-        const f3 vertical = focus_dist * viewport_height * v;
-        const f3 llc = origin - horizontal / 2.0f - vertical / 2.0f - focus_dist * w;
-        store3(s.cam.origin, origin);
-        store3(s.cam.llc, llc);
-        store3(s.cam.horizontal, horizontal);
-        store3(s.cam.vertical, vertical);
-    }
+    s.cam = camera_from_desc(d->camera);
     if(s.nodes.empty()) s.nodes.push_back(uint2{0u, kLeafTag});
     if(s.tris.empty()) s.tris.push_back(float4{0, 0, 0, 1.0f});
     if(s.ref_prim.empty()) s.ref_prim.push_back(0u);

@@ -53,6 +53,9 @@ struct PackedTree {
 };
 void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out);
 
+// camera::update for a pinhole with focus distance 1 (src/core/camera.h:20-44)
+CamRec camera_from_desc(const lrt_camera_desc& c);
+
 int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& error);
 float fresnel_diffuse_reflectance(float eta);
 void sobol_direction_table(uint32_t table[16][32]);

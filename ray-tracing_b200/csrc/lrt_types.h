@@ -91,6 +91,16 @@ struct CamRec {
     float vertical[3];
 };
 
+// one job of a batched render: its paths occupy [path_begin, path_begin + width*height*spp) of the
+// batch's path index space, ordered by (pixel, sample)
+struct JobRec {
+    CamRec cam;
+    uint32_t width, height, spp, sample_offset;
+    int32_t override_obj, override_mat;
+    unsigned long long path_begin;
+    unsigned long long out_offset;  // float offset of the job's image in the output
+};
+
 struct DeviceScene {
     const uint2* nodes;
     const float4* tris;

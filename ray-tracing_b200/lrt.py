@@ -27,7 +27,8 @@ EXPORTS = [
     "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_scene_upload", "lrt_scene_device_bytes",
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
-    "lrt_render_dev_noalloc",
+    "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
+    "lrt_render_plain", "lrt_render_plain_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
     "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
@@ -76,6 +77,10 @@ def lib():
         L.lrt_render.argtypes = [vp, P(abi.RenderParams), P(f32)]
         L.lrt_render_dev.argtypes = [vp, P(abi.RenderParams), vp]
         L.lrt_render_dev_noalloc.argtypes = [vp, P(abi.RenderParams), vp]
+        L.lrt_render_batch.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32)]
+        L.lrt_render_batch_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
+        L.lrt_render_plain.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32)]
+        L.lrt_render_plain_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
         L.lrt_render_stats_get.argtypes = [vp, P(abi.RenderStats)]
         L.lrt_render_stats_reset.argtypes = [vp]
         L.lrt_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
@@ -232,6 +237,34 @@ class Context:
 
     def render_dev(self, params: abi.RenderParams, rgb_ptr: int):
         self._check(lib().lrt_render_dev(self.handle, C.byref(params), C.c_void_p(rgb_ptr)))
+
+    def render_batch(self, jobs, max_depth: int, rr_depth: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Renders every job (abi.JobDesc) in shared waves; returns the flat output buffer."""
+        arr = (abi.JobDesc * len(jobs))(*jobs)
+        floats = max((j.output_offset + 3 * j.width * j.height for j in jobs), default=0)
+        if out is None:
+            out = np.zeros(max(1, floats), dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.size >= floats
+        self._check(lib().lrt_render_batch(self.handle, arr, len(jobs), max_depth, rr_depth, ptr(out, C.c_float)))
+        return out
+
+    def render_batch_dev(self, jobs, max_depth: int, rr_depth: int, rgb_ptr: int):
+        arr = (abi.JobDesc * len(jobs))(*jobs)
+        self._check(lib().lrt_render_batch_dev(self.handle, arr, len(jobs), max_depth, rr_depth, C.c_void_p(rgb_ptr)))
+
+    def render_plain(self, jobs, max_depth: int, rr_depth: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The plain one-launch-per-job path tracer over the same jobs and output layout."""
+        arr = (abi.JobDesc * len(jobs))(*jobs)
+        floats = max((j.output_offset + 3 * j.width * j.height for j in jobs), default=0)
+        if out is None:
+            out = np.zeros(max(1, floats), dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.size >= floats
+        self._check(lib().lrt_render_plain(self.handle, arr, len(jobs), max_depth, rr_depth, ptr(out, C.c_float)))
+        return out
+
+    def render_plain_dev(self, jobs, max_depth: int, rr_depth: int, rgb_ptr: int):
+        arr = (abi.JobDesc * len(jobs))(*jobs)
+        self._check(lib().lrt_render_plain_dev(self.handle, arr, len(jobs), max_depth, rr_depth, C.c_void_p(rgb_ptr)))
 
     def set_option(self, name: str, value: int):
         self._check(lib().lrt_set_option(self.handle, name.encode(), int(value)))

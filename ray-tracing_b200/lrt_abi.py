@@ -16,6 +16,8 @@ STATUS_NAMES = {
     -4: "LRT_ERR_IO", -5: "LRT_ERR_RANGE", -6: "LRT_ERR_NO_SCENE", -7: "LRT_ERR_QUEUE_OVERFLOW",
     -8: "LRT_ERR_TIMEOUT", -9: "LRT_ERR_NO_DEVICE", -10: "LRT_ERR_DEVICE_CHECK",
 }
+for _code, _name in STATUS_NAMES.items():
+    globals()[_name] = _code
 
 # BSDF flags (src/material/bsdf.h:18-28)
 DIFFUSE, SPECULAR, REFLECTIVE, TRANSPARENT = 1, 2, 4, 8
@@ -108,6 +110,22 @@ class RenderParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_depth", C.c_int32),
                 ("rr_depth", C.c_int32), ("sample_offset", C.c_uint32), ("row_begin", C.c_uint32),
                 ("row_end", C.c_uint32)]
+
+
+def camera_desc(camera: dict) -> CameraDesc:
+    cam = CameraDesc()
+    cam.origin = _f3(camera["origin"])
+    cam.look_at = _f3(camera["look_at"])
+    cam.up = _f3(camera["up"])
+    cam.fov_degrees = camera["fov"]
+    cam.aspect_ratio = camera["aspect"]
+    return cam
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("camera", CameraDesc), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("sample_offset", C.c_uint32), ("override_object", C.c_int32), ("override_material", C.c_int32),
+                ("output_offset", C.c_uint64)]
 
 
 class PhotonRenderParams(C.Structure):
@@ -228,12 +246,7 @@ class SceneHolder:
                             d.hosek_config[c][j] = float(cfg[c, j])
                     for c in range(3):
                         d.hosek_radiance[c] = float(e["hosek_radiance"][c])
-        cam = CameraDesc()
-        cam.origin = _f3(scene.camera["origin"])
-        cam.look_at = _f3(scene.camera["look_at"])
-        cam.up = _f3(scene.camera["up"])
-        cam.fov_degrees = scene.camera["fov"]
-        cam.aspect_ratio = scene.camera["aspect"]
+        cam = camera_desc(scene.camera)
         self.objects, self.materials, self.emitters = objs, mats, ems
         self.desc = SceneDesc(len(scene.objects), objs, len(scene.materials), mats, len(scene.emitters), ems, cam)
 

@@ -345,11 +345,74 @@ def open_box(material: str = "diffuse", level: int = 6, seed: int = 20261203, as
     return scene
 
 
+def open_box_library(level: int = 6, seed: int = 20261203, aspect: float = 1.0, attach: bool = True):
+    """The open box with every material of MATERIAL_NAMES in one material list, for batched jobs that
+    each put one of them on the sphere. Returns (scene, sphere object index, {name: material index});
+    the sphere carries the diffuse material by default."""
+    mats = []
+    index = {}
+    for name in MATERIAL_NAMES:
+        lib_mats, sphere = material_library(name)
+        if not mats:
+            mats.extend(dict(m) for m in lib_mats[:3])
+        offset = len(mats) - 3
+        for m in lib_mats[3:]:
+            m = dict(m)
+            if "nested" in m:
+                m["nested"] += offset
+            mats.append(m)
+        index[name] = sphere + offset
+    scene = open_box("diffuse", level, seed, aspect, attach=False)
+    sphere_obj = next(i for i, o in enumerate(scene.objects) if o["kind"] == abi.OBJ_MESH and len(o["indices"]) > 6 * 3)
+    scene.objects[sphere_obj]["material"] = index["diffuse"]
+    scene.materials = mats
+    scene.name = "open_box_library"
+    if attach:
+        attach_tables(scene.materials)
+        attach_hosek(scene.emitters)
+    return scene, sphere_obj, index
+
+
+def job_desc(camera: dict, width: int, height: int, spp: int, sample_offset: int = 0, override_object: int = -1,
+             override_material: int = -1, output_offset: int = 0):
+    return abi.JobDesc(abi.camera_desc(camera), width, height, spp, sample_offset, override_object,
+                       override_material, output_offset)
+
+
 # workloads -----------------------------------------------------------------------------------
 
 CONFIG0 = {"width": 256, "height": 256, "spp": 16, "max_depth": 6, "rr_depth": 3}
 CONFIG1 = {"width": 512, "height": 512, "spp": 64, "max_depth": 8, "rr_depth": 3,
            "photons": 1_000_000, "k": 64}
+
+
+BATCH_RESOLUTIONS = [(128, 128), (256, 256), (512, 512), (1024, 768)]
+BATCH_SEED = 20261204
+
+
+def batch_jobs(scene_index: dict, sphere: int, n_jobs: int = 64, seed: int = BATCH_SEED, spp_range=(4, 256)):
+    """The batched workload: n_jobs jobs drawn from `seed`, each with a resolution from BATCH_RESOLUTIONS,
+    spp uniform in spp_range (inclusive), a camera on a sphere of radius 3-5 around the origin looking at
+    it (upper hemisphere, 10-70 degrees elevation, so that it sees into the open box), and one of the
+    seven materials on the sphere. Jobs are packed back to back in the output buffer. Returns
+    (jobs, specs) with specs the per-job dicts."""
+    rng = np.random.default_rng(seed)
+    jobs, specs, offset = [], [], 0
+    for _ in range(n_jobs):
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(len(BATCH_RESOLUTIONS)))]
+        spp = int(rng.integers(spp_range[0], spp_range[1] + 1))
+        radius = float(rng.uniform(3.0, 5.0))
+        elev = np.radians(float(rng.uniform(10.0, 70.0)))
+        azim = np.radians(float(rng.uniform(0.0, 360.0)))
+        origin = (radius * np.cos(elev) * np.sin(azim), radius * np.sin(elev), radius * np.cos(elev) * np.cos(azim))
+        material = MATERIAL_NAMES[int(rng.integers(len(MATERIAL_NAMES)))]
+        cam = {"origin": tuple(float(x) for x in origin), "look_at": (0.0, 0.3, 0.0), "up": (0.0, 1.0, 0.0),
+               "fov": 30.0, "aspect": w / h}
+        spec = {"camera": cam, "width": w, "height": h, "spp": spp, "material": material, "output_offset": offset}
+        jobs.append(job_desc(cam, w, h, spp, 0, sphere, scene_index[material], offset))
+        specs.append(spec)
+        offset += 3 * w * h
+    return jobs, specs
 
 
 def render_params(width, height, spp, max_depth, rr_depth, sample_offset=0, row_begin=0, row_end=0):
