@@ -280,6 +280,15 @@ const char* lrt_status_string(int status);
 int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha,
                                   float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
 float lrt_fresnel_diffuse_reflectance(float eta);
+/* The same table in two steps, so that a caller without ggx.dat can re-slice for any alpha: the eta
+ * slice (set_eta, rough_transmittance.h:129-167) = n_alpha x LRT_TRANS_SAMPLES transmittance values
+ * (alpha-major) and n_alpha diffuse values, with the file's alpha range; then set_alpha on it
+ * (rough_transmittance.h:169-185). `capacity` is the n_alpha the two buffers hold. */
+int lrt_rough_transmittance_eta_slice(const char* ggx_path, float eta, float* sliced_table, float* sliced_diffuse,
+                                      uint32_t capacity, uint32_t* n_alpha_out, float* alpha_range_out /* 2 */);
+int lrt_rough_transmittance_at_alpha(const float* sliced_table, const float* sliced_diffuse, uint32_t n_alpha,
+                                     const float* alpha_range /* 2 */, float alpha,
+                                     float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
 
 /* Host-only SAH kd-tree build over n primitive bounds (3 floats each in bmin/bmax): the tree
  * sah_kdtree::build makes (src/accelerator/sah_kdtree.h:35-57,175-347), packed depth-first into
@@ -367,6 +376,31 @@ int lrt_render_plain(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs
                      int32_t rr_depth, float* rgb);
 int lrt_render_plain_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
                          int32_t rr_depth, float* rgb_dev);
+
+/* ---- differentiation: path-replay adjoint of the path tracer ----
+ *
+ * Parameters are scalars of the material list (an albedo channel, a roughness, a conductor eta/k
+ * channel ...). The caller describes parameter j by two full material lists, the scene's list with
+ * that scalar moved by +steps[j] and by -steps[j] (rough-transmittance tables re-sliced where alpha
+ * moved), which the library packs like lrt_scene_upload. The adjoint replays every path of the jobs
+ * from its sampler state and adds sum over paths of <adjoint[pixel] / spp, dL_path / dparam> into
+ * grad, with dL_path/dparam from the derivative of each BSDF value on the path (central difference of
+ * the packed +/- records) under detached sampling: sampled directions, lobe choices, Russian roulette
+ * and MIS weights do not move with the parameters. No counterpart in the reference. */
+#define LRT_MAX_DIFF_PARAMS 64
+#define LRT_MAX_ADJOINT_DEPTH 16
+#define LRT_MAX_PARAMS_PER_MATERIAL 8
+/* replace the material values of the uploaded scene (same count, types, nesting and BSDF flags);
+ * clears the differentiation setup */
+int lrt_scene_update_materials(lrt_context* ctx, const lrt_material_desc* materials, uint32_t n_materials);
+/* plus / minus: n_params consecutive material lists of the scene's material count each */
+int lrt_diff_setup(lrt_context* ctx, uint32_t n_params, const float* steps, const lrt_material_desc* plus,
+                   const lrt_material_desc* minus);
+/* adjoint: dLoss/dimage in the batch output layout of `jobs`; grad: n_params doubles, added to */
+int lrt_render_adjoint(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                       int32_t rr_depth, const float* adjoint, double* grad);
+int lrt_render_adjoint_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
+                           int32_t rr_depth, const float* adjoint_dev, double* grad_dev);
 
 /* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);

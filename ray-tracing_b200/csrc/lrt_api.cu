@@ -1065,6 +1065,32 @@ int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha, 
 
 float lrt_fresnel_diffuse_reflectance(float eta) { return fresnel_diffuse_reflectance(eta); }
 
+int lrt_rough_transmittance_eta_slice(const char* ggx_path, float eta, float* sliced_table, float* sliced_diffuse,
+                                      uint32_t capacity, uint32_t* n_alpha_out, float* alpha_range_out) {
+    if(!ggx_path || !n_alpha_out || !alpha_range_out) return LRT_ERR_INVALID_ARGUMENT;
+    std::string err;
+    std::vector<float> t, d;
+    float lo = 0.0f, hi = 0.0f;
+    const int st = rough_transmittance_eta(ggx_path, eta, t, d, lo, hi, err);
+    if(st != LRT_OK) return st;
+    *n_alpha_out = static_cast<uint32_t>(d.size());
+    alpha_range_out[0] = lo;
+    alpha_range_out[1] = hi;
+    if(d.size() > capacity) return LRT_ERR_RANGE;
+    if(!sliced_table || !sliced_diffuse) return LRT_ERR_INVALID_ARGUMENT;
+    memcpy(sliced_table, t.data(), t.size() * sizeof(float));
+    memcpy(sliced_diffuse, d.data(), d.size() * sizeof(float));
+    return LRT_OK;
+}
+
+int lrt_rough_transmittance_at_alpha(const float* sliced_table, const float* sliced_diffuse, uint32_t n_alpha,
+                                     const float* alpha_range, float alpha, float* table_out, float* diffuse_out) {
+    if(!sliced_table || !sliced_diffuse || !alpha_range || !table_out || !diffuse_out) return LRT_ERR_INVALID_ARGUMENT;
+    std::string err;
+    return rough_transmittance_alpha(sliced_table, sliced_diffuse, n_alpha, alpha_range[0], alpha_range[1], alpha,
+                                     table_out, diffuse_out, err);
+}
+
 int lrt_kdtree_build(const float* bmin, const float* bmax, uint32_t n, uint32_t* nodes_out, uint32_t max_nodes,
                      uint32_t* refs_out, uint32_t max_refs, uint32_t* n_nodes, uint32_t* n_refs, uint32_t* depth) {
     if((n && (!bmin || !bmax)) || !n_nodes || !n_refs) return LRT_ERR_INVALID_ARGUMENT;
@@ -1088,6 +1114,7 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     LRT_CUDA(ctx, cudaSetDevice(ctx->device));
     ctx->has_scene = false;
+    ctx->diff_params = 0;
     std::string err;
     const int st = build_host_scene(desc, ctx->host, err);
     if(st != LRT_OK) return fail(ctx, st, "%s", err.c_str());

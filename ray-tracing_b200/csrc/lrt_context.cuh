@@ -99,6 +99,9 @@ struct lrt_context {
     lrt::DevBuf out_rgb, scratch_a, scratch_b, counters;
     lrt::DevBuf batch_jobs, batch_path_job, batch_sums, batch_cursor, batch_out;
     bool batch_graph = true;
+    // differentiation: per parameter the material list moved by +step and by -step
+    uint32_t diff_params = 0;  // 0: no lrt_diff_setup for the current materials
+    lrt::DevBuf diff_mats, diff_tables, diff_inv2step, diff_aff_begin, diff_aff_list, diff_adjoint, diff_grad;
     lrt_render_stats stats{};
     bool stage_timing = false;
     bool count_work = false;

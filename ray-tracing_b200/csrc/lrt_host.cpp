@@ -540,7 +540,8 @@ void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTr
     pack_node(b, 0, out, 1);
 }
 
-int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& err) {
+int rough_transmittance_eta(const char* path, float eta, std::vector<float>& sliced_t, std::vector<float>& sliced_d,
+                            float& alpha_min_out, float& alpha_max_out, std::string& err) {
     std::ifstream in(path, std::ios::binary);
     if(!in) {
         err = std::string("rough transmittance: missing ") + path;
@@ -587,10 +588,6 @@ int rough_transmittance_slice(const char* path, float eta, float alpha, float* t
         err = "rough transmittance: eta outside table range";
         return LRT_ERR_RANGE;
     }
-    if(alpha < alpha_min || alpha > alpha_max) {
-        err = "rough transmittance: alpha outside table range";
-        return LRT_ERR_RANGE;
-    }
     // set_eta (rough_transmittance.h:129-167)
     const float* trans_src = trans.data();
     const float* diff_src = diff.data();
@@ -605,7 +602,8 @@ int rough_transmittance_slice(const char* path, float eta, float alpha, float* t
     const float d_theta = 1.0f / static_cast<float>(n_theta - 1);
     const size_t size3[3] = {n_theta, n_alpha, n_eta};
     const size_t size2e[2] = {n_alpha, n_eta};
-    std::vector<float> sliced_t(n_alpha * n_theta), sliced_d(n_alpha);
+    sliced_t.assign(n_alpha * n_theta, 0.0f);
+    sliced_d.assign(n_alpha, 0.0f);
     for(size_t i = 0; i < n_alpha; ++i) {
         for(size_t j = 0; j < n_theta; ++j) {
             const float p[3] = {static_cast<float>(j) * d_theta, static_cast<float>(i) * d_alpha, warped_eta};
@@ -614,16 +612,42 @@ int rough_transmittance_slice(const char* path, float eta, float alpha, float* t
         const float q[2] = {static_cast<float>(i) * d_alpha, warped_eta};
         sliced_d[i] = interp_2d(q, diff_src, size2e);
     }
+    alpha_min_out = alpha_min;
+    alpha_max_out = alpha_max;
+    return LRT_OK;
+}
+
+int rough_transmittance_alpha(const float* sliced_t, const float* sliced_d, uint32_t n_alpha, float alpha_min,
+                              float alpha_max, float alpha, float* table, float* diffuse, std::string& err) {
+    const size_t n_theta = LRT_TRANS_SAMPLES;
+    if(n_alpha < 2 || n_alpha > 4096) {
+        err = "rough transmittance: unexpected table dimensions";
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+    if(alpha < alpha_min || alpha > alpha_max) {
+        err = "rough transmittance: alpha outside table range";
+        return LRT_ERR_RANGE;
+    }
+    const float d_theta = 1.0f / static_cast<float>(n_theta - 1);
     // set_alpha (rough_transmittance.h:169-185)
     const float warped_alpha = powf((alpha - alpha_min) / (alpha_max - alpha_min), 0.25f);
     const size_t size2a[2] = {n_theta, n_alpha};
     for(size_t i = 0; i < n_theta; ++i) {
         const float p[2] = {static_cast<float>(i) * d_theta, warped_alpha};
-        table[i] = interp_2d(p, sliced_t.data(), size2a);
+        table[i] = interp_2d(p, sliced_t, size2a);
     }
-    const float d = interp_1d(warped_alpha, sliced_d.data(), n_alpha, 0.0f, 1.0f);
+    const float d = interp_1d(warped_alpha, sliced_d, n_alpha, 0.0f, 1.0f);
     *diffuse = sclamp(d, 0.0f, 1.0f);  // eval_diffuse()
     return LRT_OK;
+}
+
+int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& err) {
+    std::vector<float> sliced_t, sliced_d;
+    float alpha_min = 0.0f, alpha_max = 0.0f;
+    const int st = rough_transmittance_eta(path, eta, sliced_t, sliced_d, alpha_min, alpha_max, err);
+    if(st != LRT_OK) return st;
+    return rough_transmittance_alpha(sliced_t.data(), sliced_d.data(), static_cast<uint32_t>(sliced_d.size()), alpha_min,
+                                     alpha_max, alpha, table, diffuse, err);
 }
 
 float fresnel_diffuse_reflectance(float eta) {
@@ -687,20 +711,16 @@ CamRec camera_from_desc(const lrt_camera_desc& c) {
     return cam;
 }
 
-int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
-    s = HostScene{};
-    if(!d) {
-        err = "scene description is null";
+int pack_materials(const lrt_material_desc* mats, uint32_t n, std::vector<MatRec>& out, std::vector<float>& tables,
+                   std::string& err) {
+    out.clear();
+    tables.clear();
+    if(n && !mats) {
+        err = "material list is null";
         return LRT_ERR_INVALID_ARGUMENT;
     }
-    if((d->n_objects && !d->objects) || (d->n_materials && !d->materials) || (d->n_emitters && !d->emitters)) {
-        err = "scene arrays are null";
-        return LRT_ERR_INVALID_ARGUMENT;
-    }
-
-    // ---- materials ----
-    for(uint32_t i = 0; i < d->n_materials; ++i) {
-        const lrt_material_desc& m = d->materials[i];
+    for(uint32_t i = 0; i < n; ++i) {
+        const lrt_material_desc& m = mats[i];
         if(m.type < LRT_DIFFUSE || m.type > LRT_ROUGH_COATING) {
             err = "material " + std::to_string(i) + ": unknown type";
             return LRT_ERR_INVALID_ARGUMENT;
@@ -710,7 +730,7 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
                 err = "material " + std::to_string(i) + ": nested material must precede the coating";
                 return LRT_ERR_INVALID_ARGUMENT;
             }
-            const int nt = d->materials[m.nested].type;
+            const int nt = mats[m.nested].type;
             if(nt == LRT_COATING || nt == LRT_ROUGH_COATING) {
                 err = "material " + std::to_string(i) + ": nested coatings are not supported";
                 return LRT_ERR_INVALID_ARGUMENT;
@@ -719,8 +739,8 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
         MatRec r{};
         r.type = m.type;
         r.nested = (m.type == LRT_COATING || m.type == LRT_ROUGH_COATING) ? m.nested : -1;
-        r.flags = bsdf_flags(m, d->materials);
-        r.component_count = component_count(m, d->materials);
+        r.flags = bsdf_flags(m, mats);
+        r.component_count = component_count(m, mats);
         r.int_ior = m.int_ior;
         r.ext_ior = m.ext_ior;
         r.alpha = m.alpha;
@@ -753,7 +773,7 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
             const f3 optical = load3(m.sigma_a) * (-2.0f * m.thickness);
             const float avg = (expf(optical.x) + expf(optical.y) + expf(optical.z)) / 3.0f;
             r.specular_sampling_weight = 1.0f / (avg + 1.0f);
-            r.specular_component = component_count(d->materials[m.nested], d->materials);
+            r.specular_component = component_count(mats[m.nested], mats);
         }
         if(m.type == LRT_ROUGH_PLASTIC || m.type == LRT_ROUGH_COATING) {
             bool any = false;
@@ -762,10 +782,30 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
                 err = "material " + std::to_string(i) + ": rough-transmittance table is empty";
                 return LRT_ERR_INVALID_ARGUMENT;
             }
-            r.table = static_cast<int32_t>(s.tables.size() / LRT_TRANS_SAMPLES);
-            s.tables.insert(s.tables.end(), m.trans_table, m.trans_table + LRT_TRANS_SAMPLES);
+            r.table = static_cast<int32_t>(tables.size() / LRT_TRANS_SAMPLES);
+            tables.insert(tables.end(), m.trans_table, m.trans_table + LRT_TRANS_SAMPLES);
         }
-        s.materials.push_back(r);
+        out.push_back(r);
+    }
+
+    return LRT_OK;
+}
+
+int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
+    s = HostScene{};
+    if(!d) {
+        err = "scene description is null";
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+    if((d->n_objects && !d->objects) || (d->n_materials && !d->materials) || (d->n_emitters && !d->emitters)) {
+        err = "scene arrays are null";
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+
+    // ---- materials ----
+    {
+        const int st = pack_materials(d->materials, d->n_materials, s.materials, s.tables, err);
+        if(st != LRT_OK) return st;
     }
 
     // ---- objects ----

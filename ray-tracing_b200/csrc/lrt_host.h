@@ -56,6 +56,17 @@ void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTr
 // camera::update for a pinhole with focus distance 1 (src/core/camera.h:20-44)
 CamRec camera_from_desc(const lrt_camera_desc& c);
 
+// Packs a material list into device records; rough plastic / rough coating tables are appended to `tables`.
+int pack_materials(const lrt_material_desc* mats, uint32_t n, std::vector<MatRec>& out, std::vector<float>& tables,
+                   std::string& error);
+
+// rough_transmittance (src/material/func/rough_transmittance.h:67-185) in two steps: set_eta on the
+// file's data gives an eta slice (n_alpha x LRT_TRANS_SAMPLES values, n_alpha diffuse values), set_alpha
+// on that slice gives the 1-D table; rough_transmittance_slice runs both.
+int rough_transmittance_eta(const char* path, float eta, std::vector<float>& sliced_t, std::vector<float>& sliced_d,
+                            float& alpha_min, float& alpha_max, std::string& error);
+int rough_transmittance_alpha(const float* sliced_t, const float* sliced_d, uint32_t n_alpha, float alpha_min,
+                              float alpha_max, float alpha, float* table, float* diffuse, std::string& error);
 int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& error);
 float fresnel_diffuse_reflectance(float eta);
 void sobol_direction_table(uint32_t table[16][32]);

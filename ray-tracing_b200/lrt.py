@@ -28,7 +28,9 @@ EXPORTS = [
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
-    "lrt_render_plain", "lrt_render_plain_dev",
+    "lrt_render_plain", "lrt_render_plain_dev", "lrt_rough_transmittance_eta_slice",
+    "lrt_rough_transmittance_at_alpha", "lrt_scene_update_materials", "lrt_diff_setup", "lrt_render_adjoint",
+    "lrt_render_adjoint_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
     "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
@@ -81,6 +83,12 @@ def lib():
         L.lrt_render_batch_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
         L.lrt_render_plain.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32)]
         L.lrt_render_plain_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
+        L.lrt_rough_transmittance_eta_slice.argtypes = [C.c_char_p, f32, P(f32), P(f32), u32, P(u32), P(f32)]
+        L.lrt_rough_transmittance_at_alpha.argtypes = [P(f32), P(f32), u32, P(f32), f32, P(f32), P(f32)]
+        L.lrt_scene_update_materials.argtypes = [vp, P(abi.MaterialDesc), u32]
+        L.lrt_diff_setup.argtypes = [vp, u32, P(f32), P(abi.MaterialDesc), P(abi.MaterialDesc)]
+        L.lrt_render_adjoint.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32), P(C.c_double)]
+        L.lrt_render_adjoint_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp, vp]
         L.lrt_render_stats_get.argtypes = [vp, P(abi.RenderStats)]
         L.lrt_render_stats_reset.argtypes = [vp]
         L.lrt_set_option.argtypes = [vp, C.c_char_p, C.c_int64]
@@ -102,6 +110,34 @@ def rough_transmittance_slice(ggx_path: str, eta: float, alpha: float):
     st = lib().lrt_rough_transmittance_slice(ggx_path.encode(), eta, alpha, ptr(table, C.c_float), C.byref(diffuse))
     if st != 0:
         raise LrtError(st, "rough transmittance slice failed")
+    return table, np.float32(diffuse.value)
+
+
+def rough_transmittance_eta_slice(ggx_path: str, eta: float):
+    """(sliced_table [n_alpha, TRANS_SAMPLES], sliced_diffuse [n_alpha], alpha_range [2]) of ggx.dat at eta"""
+    cap = 4096
+    table = np.zeros(cap * abi.TRANS_SAMPLES, dtype=np.float32)
+    diffuse = np.zeros(cap, dtype=np.float32)
+    n = C.c_uint32(0)
+    rng = np.zeros(2, dtype=np.float32)
+    st = lib().lrt_rough_transmittance_eta_slice(ggx_path.encode(), eta, ptr(table, C.c_float), ptr(diffuse, C.c_float),
+                                                 cap, C.byref(n), ptr(rng, C.c_float))
+    if st != 0:
+        raise LrtError(st, "rough transmittance eta slice failed")
+    k = n.value
+    return table[:k * abi.TRANS_SAMPLES].reshape(k, abi.TRANS_SAMPLES).copy(), diffuse[:k].copy(), rng
+
+
+def rough_transmittance_at_alpha(sliced_table, sliced_diffuse, alpha_range, alpha: float):
+    t = np.ascontiguousarray(sliced_table, dtype=np.float32)
+    d = np.ascontiguousarray(sliced_diffuse, dtype=np.float32)
+    r = np.ascontiguousarray(alpha_range, dtype=np.float32)
+    table = np.zeros(abi.TRANS_SAMPLES, dtype=np.float32)
+    diffuse = C.c_float(0.0)
+    st = lib().lrt_rough_transmittance_at_alpha(ptr(t, C.c_float), ptr(d, C.c_float), len(d), ptr(r, C.c_float), alpha,
+                                                ptr(table, C.c_float), C.byref(diffuse))
+    if st != 0:
+        raise LrtError(st, "rough transmittance at alpha %r failed" % alpha)
     return table, np.float32(diffuse.value)
 
 

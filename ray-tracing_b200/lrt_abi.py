@@ -178,6 +178,34 @@ def _f3(values) -> "C.Array":
     return (C.c_float * 3)(*[float(x) for x in v])
 
 
+def material_descs(materials, out=None, start=0):
+    """lrt_material_desc records of a material list (into `out` from index `start` when given)."""
+    if out is None:
+        out = (MaterialDesc * max(1, len(materials)))()
+    for i, m in enumerate(materials):
+        d = out[start + i]
+        d.type = m["type"]
+        d.nested = m.get("nested", -1)
+        d.nonlinear = int(m.get("nonlinear", 0))
+        d.int_ior = m.get("int_ior", 1.5)
+        d.ext_ior = m.get("ext_ior", 1.0)
+        d.alpha = m.get("alpha", 0.0)
+        d.thickness = m.get("thickness", 1.0)
+        d.diffuse_reflectance = _f3(m.get("diffuse_reflectance", (0.5, 0.5, 0.5)))
+        d.specular_reflectance = _f3(m.get("specular_reflectance", (1, 1, 1)))
+        d.specular_transmittance = _f3(m.get("specular_transmittance", (1, 1, 1)))
+        d.eta = _f3(m.get("eta", (0, 0, 0)))
+        d.k = _f3(m.get("k", (0, 0, 0)))
+        d.sigma_a = _f3(m.get("sigma_a", (0, 0, 0)))
+        table = m.get("trans_table")
+        if table is not None:
+            t = np.asarray(table, dtype=np.float32)
+            assert t.size == TRANS_SAMPLES
+            d.trans_table = (C.c_float * TRANS_SAMPLES)(*[float(x) for x in t])
+        d.trans_internal_diffuse = float(m.get("trans_internal_diffuse", 0.0))
+    return out
+
+
 class SceneHolder:
     """Owns the ctypes descriptors and numpy buffers of one lrt_scene_desc."""
 
@@ -205,28 +233,7 @@ class SceneHolder:
             else:
                 d.center = _f3(o["center"])
                 d.radius = float(np.float32(o["radius"]))
-        mats = (MaterialDesc * max(1, len(scene.materials)))()
-        for i, m in enumerate(scene.materials):
-            d = mats[i]
-            d.type = m["type"]
-            d.nested = m.get("nested", -1)
-            d.nonlinear = int(m.get("nonlinear", 0))
-            d.int_ior = m.get("int_ior", 1.5)
-            d.ext_ior = m.get("ext_ior", 1.0)
-            d.alpha = m.get("alpha", 0.0)
-            d.thickness = m.get("thickness", 1.0)
-            d.diffuse_reflectance = _f3(m.get("diffuse_reflectance", (0.5, 0.5, 0.5)))
-            d.specular_reflectance = _f3(m.get("specular_reflectance", (1, 1, 1)))
-            d.specular_transmittance = _f3(m.get("specular_transmittance", (1, 1, 1)))
-            d.eta = _f3(m.get("eta", (0, 0, 0)))
-            d.k = _f3(m.get("k", (0, 0, 0)))
-            d.sigma_a = _f3(m.get("sigma_a", (0, 0, 0)))
-            table = m.get("trans_table")
-            if table is not None:
-                t = np.asarray(table, dtype=np.float32)
-                assert t.size == TRANS_SAMPLES
-                d.trans_table = (C.c_float * TRANS_SAMPLES)(*[float(x) for x in t])
-            d.trans_internal_diffuse = float(m.get("trans_internal_diffuse", 0.0))
+        mats = material_descs(scene.materials)
         ems = (EmitterDesc * max(1, len(scene.emitters)))()
         for i, e in enumerate(scene.emitters):
             d = ems[i]

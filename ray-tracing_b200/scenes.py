@@ -18,6 +18,7 @@ reference computes them on the host at material/emitter construction). They are 
 """
 from __future__ import annotations
 
+import base64
 import json
 import math
 import os
@@ -76,15 +77,32 @@ def load_scene_data() -> dict:
     return _scene_data_cache
 
 
+_eta_slice_cache = {}
+
+
+def eta_slice(eta: float):
+    """(sliced_table, sliced_diffuse, alpha_range) of the rough-transmittance data at eta (float32 key)."""
+    key = _f32_key(eta)
+    if key not in _eta_slice_cache:
+        data = load_scene_data().get("eta_slices", {})
+        if key not in data:
+            raise KeyError("no rough-transmittance eta slice for eta=%r in %s; run tests/golden/make_scene_data.py"
+                           % (float(eta), SCENE_DATA))
+        e = data[key]
+        n = e["n_alpha"]
+        table = np.frombuffer(base64.b64decode(e["table_f32_b64"]), dtype="<f4").reshape(n, abi.TRANS_SAMPLES)
+        diffuse = np.frombuffer(base64.b64decode(e["diffuse_f32_b64"]), dtype="<f4")
+        _eta_slice_cache[key] = (table.astype(np.float32), diffuse.astype(np.float32),
+                                 np.array(e["alpha_range"], dtype=np.float32))
+    return _eta_slice_cache[key]
+
+
 def transmittance_table(eta: float, alpha: float):
-    """1-D rough-transmittance table and diffuse transmittance for (eta, alpha) as float32."""
-    key = _f32_key(eta, alpha)
-    data = load_scene_data()["transmittance"]
-    if key not in data:
-        raise KeyError("no rough-transmittance table for eta=%r alpha=%r in %s; run data/make_scene_data.py"
-                       % (float(eta), float(alpha), SCENE_DATA))
-    entry = data[key]
-    return np.array(entry["table"], dtype=np.float32), np.float32(entry["diffuse"])
+    """1-D rough-transmittance table and diffuse transmittance for (eta, alpha) as float32, by set_alpha
+    (liblrt's host routine) on the stored eta slice."""
+    import lrt
+    table, diffuse, rng = eta_slice(eta)
+    return lrt.rough_transmittance_at_alpha(table, diffuse, rng, float(np.float32(alpha)))
 
 
 def hosek_state(sun_direction, turbidity: float, albedo: float):

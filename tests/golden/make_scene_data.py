@@ -1,8 +1,9 @@
 """Writes ray-tracing_b200/data/scene_data.json: the caller-side inputs the workload scenes need.
 
-* rough-transmittance 1-D tables for every (eta, alpha) the seven materials use, sliced from the
-  reference's ggx.dat by liblrt's own host routine (lrt_rough_transmittance_slice, which the CPU tests
-  check bit for bit against the reference's rough_transmittance);
+* rough-transmittance eta slices (the set_eta step over ggx.dat) for every eta the seven materials
+  use, made by liblrt's own host routine (lrt_rough_transmittance_eta_slice); the 1-D table for any
+  alpha follows from a slice by lrt_rough_transmittance_at_alpha, and the CPU tests check that pair
+  bit for bit against the reference's rough_transmittance;
 * the cooked RGB Hosek-Wilkie state of the workload sky, from the reference's vendored Hosek model
   (arhosek_rgb_skymodelstate_alloc_init through the oracle build), which a reference-side caller would
   read from its env_emitter.
@@ -10,6 +11,7 @@
 Run from the repository root after `make -C oracle ref` and `make -C ray-tracing_b200/csrc`:
     python tests/golden/make_scene_data.py
 """
+import base64
 import json
 import os
 import sys
@@ -26,19 +28,22 @@ import scenes  # noqa: E402
 
 
 def main():
-    data = {"transmittance": {}, "hosek": {},
+    data = {"hosek": {},
             "note": "caller-side inputs of the workload scenes; made by tests/golden/make_scene_data.py"}
     pairs = []
     for name in scenes.MATERIAL_NAMES:
         mats, _ = scenes.material_library(name)
         pairs += scenes.required_tables(mats)
+    data["eta_slices"] = {}
     for eta, alpha in pairs:
-        key = scenes._f32_key(eta, alpha)
-        if key in data["transmittance"]:
+        key = scenes._f32_key(eta)
+        if key in data["eta_slices"]:
             continue
-        table, diffuse = lrt.rough_transmittance_slice(oracle.GGX_PATH, float(eta), float(alpha))
-        data["transmittance"][key] = {"eta": float(eta), "alpha": float(alpha),
-                                      "table": [float(x) for x in table], "diffuse": float(diffuse)}
+        table, diffuse, rng = lrt.rough_transmittance_eta_slice(oracle.GGX_PATH, float(eta))
+        data["eta_slices"][key] = {"eta": float(eta), "n_alpha": int(len(diffuse)),
+                                   "alpha_range": [float(x) for x in rng],
+                                   "table_f32_b64": base64.b64encode(table.astype("<f4").tobytes()).decode(),
+                                   "diffuse_f32_b64": base64.b64encode(diffuse.astype("<f4").tobytes()).decode()}
     sky = scenes.sky_emitter()
     key = scenes._f32_key(*sky["sun_direction"], sky["turbidity"], sky["albedo"])
     cfg, rad = oracle.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
@@ -48,7 +53,7 @@ def main():
     os.makedirs(scenes.DATA_DIR, exist_ok=True)
     with open(scenes.SCENE_DATA, "w") as f:
         json.dump(data, f, indent=1)
-    print("wrote", scenes.SCENE_DATA, len(data["transmittance"]), "tables,", len(data["hosek"]), "sky states")
+    print("wrote", scenes.SCENE_DATA, len(data["eta_slices"]), "eta slices,", len(data["hosek"]), "sky states")
 
 
 if __name__ == "__main__":

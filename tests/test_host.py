@@ -137,11 +137,25 @@ def test_scene_data_covers_workload_materials():
 
 
 @needs_ref
-def test_scene_data_tables_match_slicing():
-    data = scenes.load_scene_data()["transmittance"]
+@pytest.mark.parametrize("alpha", [0.15, 0.2, 0.05, 0.3, 0.37, 0.6, 0.2 + 1e-3, 0.15 - 1e-3])
+def test_scene_data_eta_slices_match_reference(alpha):
+    """set_alpha on a stored eta slice = the reference's rough_transmittance at (eta, alpha), for the
+    workload's alphas and the moved alphas of differentiation and optimisation"""
+    data = scenes.load_scene_data()["eta_slices"]
+    assert data
     for entry in data.values():
-        a, d = lrt.rough_transmittance_slice(oracle.GGX_PATH, np.float32(entry["eta"]), np.float32(entry["alpha"]))
-        assert np.array_equal(a, np.array(entry["table"], np.float32)) and d == np.float32(entry["diffuse"])
+        eta = np.float32(entry["eta"])
+        a, d = scenes.transmittance_table(eta, alpha)
+        b, db = oracle.rough_transmittance(eta, np.float32(alpha))
+        assert np.array_equal(a, b) and d == db
+
+
+def test_rough_transmittance_at_alpha_errors():
+    table, diffuse, rng = scenes.eta_slice(np.float32(1.49) / np.float32(1.000277))
+    with pytest.raises(lrt.LrtError):
+        lrt.rough_transmittance_at_alpha(table, diffuse, rng, float(rng[1]) + 1.0)
+    with pytest.raises(lrt.LrtError):
+        lrt.rough_transmittance_at_alpha(table[:1], diffuse[:1], rng, 0.2)
 
 
 @needs_ref
@@ -150,3 +164,19 @@ def test_scene_data_hosek_matches_reference():
     cfg, rad = scenes.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
     rcfg, rrad = oracle.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
     assert np.array_equal(cfg, rcfg) and np.array_equal(rad, rrad)
+
+
+def test_diff_params_of_material_library():
+    import diff
+    scene, sphere, index = scenes.open_box_library(level=1)
+    params = diff.scene_params(scene.materials)
+    assert len(params) == 32
+    assert diff.param_name(scene.materials, params[0]) == "m0.diffuse_reflectance[0]"
+    rp = index["rough_plastic"]
+    p = (rp, "alpha", None)
+    assert p in params
+    moved = diff.with_values(scene.materials, [p], [0.3])
+    assert moved[rp]["alpha"] == 0.3 and scene.materials[rp]["alpha"] == 0.15
+    assert not np.array_equal(moved[rp]["trans_table"], scene.materials[rp]["trans_table"])
+    back = diff.with_values(moved, [p], [0.15])
+    assert np.array_equal(back[rp]["trans_table"], scene.materials[rp]["trans_table"])
