@@ -404,6 +404,126 @@ def run_batch(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+# differentiation workload: L2 image loss of the seven-material scene against a target at alpha 0.3,
+# sphere albedo (0.7, 0.5, 0.3); Adam (lr 0.01) from alpha 0.6 on the 32 material parameters
+
+ADJ_METRIC = "grad-steps/s (7 materials x 256x256 x 32 spp, depth 6, 32 material parameters, Adam)"
+
+
+def run_adjoint(args):
+    import torch
+    import diff
+    import lrt
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    w = h = 256
+    spp, depth, rr = 32, 6, 3
+    scene, sphere, index = scenes.open_box_library()
+    ctx = lrt.Context(local, stream.cuda_stream)
+    ctx.upload(scene)
+    dm = diff.Differentiable(ctx, scene)
+    params = dm.params
+    names = dm.names()
+
+    def jobs_at(spp_, offset):
+        out, off = [], 0
+        for name in MATERIALS:
+            out.append(scenes.job_desc(scene.camera, w, h, spp_, offset, sphere, index[name], off))
+            off += 3 * w * h
+        return out, off
+
+    _, floats = jobs_at(spp, 0)
+    n_paths = len(MATERIALS) * w * h * spp
+    # target: every roughness 0.3, the diffuse sphere's albedo (0.7, 0.5, 0.3), copper as in the scene
+    target_values = dm.values()
+    start_values = dm.values()
+    for j, (m, field, c) in enumerate(params):
+        if field == "alpha":
+            target_values[j], start_values[j] = 0.3, 0.6
+        if m == index["diffuse"] and field == "diffuse_reflectance":
+            target_values[j] = (0.7, 0.5, 0.3)[c]
+    img = torch.empty(floats, dtype=torch.float32, device=dev)
+    target = torch.empty(floats, dtype=torch.float32, device=dev)
+    dm.set_values(target_values, setup=False)
+    ctx.render_batch_dev(jobs_at(256, 1 << 24)[0], depth, rr, target.data_ptr())
+    grad = torch.zeros(len(params), dtype=torch.float64, device=dev)
+
+    def clean_loss(values):
+        dm.set_values(values, setup=False)
+        ctx.render_batch_dev(jobs_at(128, 1 << 26)[0], depth, rr, img.data_ptr())
+        return float(((img - target) ** 2).mean())
+
+    loss_start = clean_loss(start_values)
+    dm.set_values(start_values)
+    m1 = np.zeros(len(params))
+    m2 = np.zeros(len(params))
+    lr, b1, b2, eps = 0.01, 0.9, 0.999, 1e-8
+    values = start_values.copy()
+    fwd_ms, adj_ms, step_s, losses = [], [], [], []
+    steps = args.adjoint_steps
+    clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+    clocks.start()
+    ctx.reset_stats()
+    for it in range(steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        ctx.render_batch_dev(jobs_at(spp, 2 * spp * it)[0], depth, rr, img.data_ptr())
+        e[1].record(stream)
+        adjoint = (2.0 / floats) * (img - target)
+        grad.zero_()
+        dm.adjoint_dev(jobs_at(spp, 2 * spp * it + spp)[0], depth, rr, adjoint.data_ptr(), grad.data_ptr())
+        e[2].record(stream)
+        g = grad.cpu().numpy()
+        losses.append(float(((img - target) ** 2).mean()))
+        m1 = b1 * m1 + (1 - b1) * g
+        m2 = b2 * m2 + (1 - b2) * g * g
+        values = values - lr * (m1 / (1 - b1 ** (it + 1))) / (np.sqrt(m2 / (1 - b2 ** (it + 1))) + eps)
+        for j, (m, field, c) in enumerate(params):
+            values[j] = np.clip(values[j], 0.05, 1.0) if field == "alpha" else max(values[j], 1e-3)
+        dm.set_values(values)
+        torch.cuda.synchronize(dev)
+        step_s.append(time.perf_counter() - t0)
+        fwd_ms.append(e[0].elapsed_time(e[1]))
+        adj_ms.append(e[1].elapsed_time(e[2]))
+    clock_info = clocks.stop()
+    launches = int(ctx.stats()["kernel_launches"])
+    loss_end = clean_loss(values)
+    timed = slice(min(3, steps - 1), steps)  # the first steps include one-time set-up
+    total = float(sum(step_s[timed]))
+    n_timed = len(step_s[timed])
+    alpha_idx = [j for j, p in enumerate(params) if p[1] == "alpha"]
+    line = {"metric": ADJ_METRIC, "value": n_timed / total, "unit": "grad-steps/s", "n_gpus": 1,
+            "steps": n_timed, "warmup": steps - n_timed, "ms_per_step": 1000 * total / n_timed,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scenes.open_box_library)",
+            "config": {"workload": "adjoint_7x256x256x32spp_depth6_adam200", "paths_per_render": n_paths,
+                       "parameters": len(params), "adam_steps": steps, "lr": lr,
+                       "forward_ms": statistics.median(fwd_ms[timed]), "adjoint_ms": statistics.median(adj_ms[timed]),
+                       "adjoint_over_forward": statistics.median(adj_ms[timed]) / statistics.median(fwd_ms[timed]),
+                       "forward_mpaths_s": n_paths / statistics.median(fwd_ms[timed]) / 1e3,
+                       "adjoint_mpaths_s": n_paths / statistics.median(adj_ms[timed]) / 1e3,
+                       "clean_loss_start": loss_start, "clean_loss_end": loss_end,
+                       "loss_first": losses[0], "loss_last": losses[-1],
+                       "alphas_end": {names[j]: float(values[j]) for j in alpha_idx},
+                       "sphere_albedo_end": [float(values[j]) for j, p in enumerate(params)
+                                             if p[0] == index["diffuse"]],
+                       "l2": "inputs (scene, 7 x 256x256 images) are L2-resident; not flushed"},
+            "e2e": {"value": n_timed / total, "unit": "grad-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * len(params),
+                    "path": "render_batch_dev + adjoint_dev + host Adam + lrt_scene_update_materials + lrt_diff_setup"},
+            "clocks": clock_info, "gpu_launches": launches}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def abi_stage_names():
     import lrt_abi
     return lrt_abi.STAGE_NAMES
@@ -416,14 +536,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lrt", choices=["lrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="paths", choices=["paths", "batch"],
-                    help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison")
+    ap.add_argument("--workload", default="paths", choices=["paths", "batch", "adjoint"],
+                    help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison; "
+                         "adjoint: gradient steps of the material optimisation")
     ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--adjoint-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_lrt(args)
 
 

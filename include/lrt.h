@@ -380,22 +380,30 @@ int lrt_render_plain_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_
 /* ---- differentiation: path-replay adjoint of the path tracer ----
  *
  * Parameters are scalars of the material list (an albedo channel, a roughness, a conductor eta/k
- * channel ...). The caller describes parameter j by two full material lists, the scene's list with
- * that scalar moved by +steps[j] and by -steps[j] (rough-transmittance tables re-sliced where alpha
- * moved), which the library packs like lrt_scene_upload. The adjoint replays every path of the jobs
- * from its sampler state and adds sum over paths of <adjoint[pixel] / spp, dL_path / dparam> into
- * grad, with dL_path/dparam from the derivative of each BSDF value on the path (central difference of
- * the packed +/- records) under detached sampling: sampled directions, lobe choices, Russian roulette
- * and MIS weights do not move with the parameters. No counterpart in the reference. */
+ * channel ...). They are moved in groups: group g is described by two full material lists, the
+ * scene's list with every parameter of g moved by +steps[g] and by -steps[g] (rough-transmittance
+ * tables re-sliced where alpha moved), which the library packs like lrt_scene_upload. A parameter
+ * names its group and a colour channel: channel c (0..2) when it moves only channel c of every BSDF
+ * value (the three channels of an albedo, of a conductor's eta or k, which therefore share one
+ * group), -1 when it moves all channels (then it is its group's only parameter). The adjoint replays
+ * every path of the jobs from its sampler state and adds sum over paths of
+ * <adjoint[pixel] / spp, dL_path / dparam> into grad, with dL_path/dparam from the derivative of each
+ * BSDF value on the path (central difference of the packed +/- records) under detached sampling:
+ * sampled directions, lobe choices, Russian roulette and MIS weights do not move with the
+ * parameters. No counterpart in the reference. */
 #define LRT_MAX_DIFF_PARAMS 64
 #define LRT_MAX_ADJOINT_DEPTH 16
-#define LRT_MAX_PARAMS_PER_MATERIAL 8
+#define LRT_MAX_GROUPS_PER_MATERIAL 8
+typedef struct lrt_diff_param {
+    uint32_t group;
+    int32_t channel;
+} lrt_diff_param;
 /* replace the material values of the uploaded scene (same count, types, nesting and BSDF flags);
  * clears the differentiation setup */
 int lrt_scene_update_materials(lrt_context* ctx, const lrt_material_desc* materials, uint32_t n_materials);
-/* plus / minus: n_params consecutive material lists of the scene's material count each */
-int lrt_diff_setup(lrt_context* ctx, uint32_t n_params, const float* steps, const lrt_material_desc* plus,
-                   const lrt_material_desc* minus);
+/* plus / minus: n_groups consecutive material lists of the scene's material count each */
+int lrt_diff_setup(lrt_context* ctx, uint32_t n_groups, const float* steps, const lrt_material_desc* plus,
+                   const lrt_material_desc* minus, uint32_t n_params, const lrt_diff_param* params);
 /* adjoint: dLoss/dimage in the batch output layout of `jobs`; grad: n_params doubles, added to */
 int lrt_render_adjoint(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
                        int32_t rr_depth, const float* adjoint, double* grad);
@@ -405,6 +413,9 @@ int lrt_render_adjoint_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t 
 /* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
 int lrt_render_stats_reset(lrt_context* ctx);
+/* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26),
+ * "photon_tree_device" (0/1), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
+ * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one) */
 int lrt_set_option(lrt_context* ctx, const char* name, int64_t value);
 
 /* photons: particles [0, ...) traced in index order until `requested` photons are stored */

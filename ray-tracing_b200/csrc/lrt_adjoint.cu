@@ -11,15 +11,17 @@
 // the value's derivative. The kernel replays each path once from its sampler state — the same
 // samples, rays and operations as the renderers — keeping c_d and dE_d/E_d of the parameters that
 // move vertex d's material in local arrays, then sums the suffix products backwards. The BSDF
-// derivative is the central difference of the packed +step / -step material records, so every
-// material type (and the rough-transmittance tables of rough plastic and rough coating) is covered
-// by the BSDF code the renderer runs. Per-thread sums are warp-reduced before one double atomic per
-// parameter and warp.
+// derivative is the central difference of the packed +step / -step material records of a parameter
+// group, so every material type (and the rough-transmittance tables of rough plastic and rough
+// coating) is covered by the BSDF code the renderer runs; one pair of evaluations serves the three
+// channel parameters of an albedo, eta or k, since channel c of a BSDF value moves only with channel c
+// of those. Per-thread sums are warp-reduced before one double atomic per parameter and warp.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
+#include "lrt_adjoint.cuh"
 #include "lrt_bsdf.cuh"
 #include "lrt_context.cuh"
 #include "lrt_scene.cuh"
@@ -29,40 +31,23 @@ using namespace lrt;
 namespace {
 
 constexpr int kMaxParams = LRT_MAX_DIFF_PARAMS;
-constexpr int kMaxAff = LRT_MAX_PARAMS_PER_MATERIAL;
+constexpr int kMaxAff = LRT_MAX_GROUPS_PER_MATERIAL;
 constexpr int kMaxAdjDepth = LRT_MAX_ADJOINT_DEPTH;
 
 struct AdjArgs {
     DeviceScene s;
+    DiffDev d;
     const JobRec* jobs;
     uint32_t n_jobs;
     unsigned long long total_paths;
-    const float* adjoint;     // dLoss/dimage, batch output layout
-    const MatRec* pert;       // 2 * n_params lists of n_materials records: [2j] +step, [2j+1] -step
-    const float* pert_tables;
-    const float* inv2step;    // 1 / (2 step_j)
-    const int32_t* aff_begin; // per material: its parameters are aff_list[aff_begin[m] .. aff_begin[m+1])
-    const int32_t* aff_list;
-    uint32_t n_params;
+    const float* adjoint;  // dLoss/dimage, batch output layout
     int32_t max_depth, rr_depth;
     double* grad;
 };
 
-__device__ __forceinline__ f3 d_eval(const AdjArgs& a, int32_t mid, const BsdfCtx& c, const BRec& rec, int32_t j) {
-    const MatRec* plus = a.pert + static_cast<size_t>(2 * j) * a.s.n_materials;
-    const MatRec* minus = plus + a.s.n_materials;
-    const f3 ep = bsdf_eval(plus, a.pert_tables, mid, c, rec, kSolidAngle);
-    const f3 em = bsdf_eval(minus, a.pert_tables, mid, c, rec, kSolidAngle);
-    return (ep - em) * a.inv2step[j];
-}
-
-__device__ __forceinline__ float dot_rgb(f3 a, f3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
-
-__device__ __forceinline__ float safe_ratio(float num, float den) { return den != 0.0f ? num / den : 0.0f; }
-
 __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
     float g[kMaxParams];
-    for(uint32_t j = 0; j < a.n_params; ++j) g[j] = 0.0f;
+    for(uint32_t j = 0; j < a.d.n_params; ++j) g[j] = 0.0f;
     f3 vc[kMaxAdjDepth];
     f3 vd[kMaxAdjDepth][kMaxAff];
     int32_t vmid[kMaxAdjDepth];
@@ -132,8 +117,8 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
                 vc[depth] = c;
                 break;
             }
-            const int32_t ab = a.aff_begin[mid];
-            const int32_t an = a.aff_begin[mid + 1] - ab;
+            const int32_t ab = a.d.aff_begin[mid];
+            const int32_t an = a.d.aff_begin[mid + 1] - ab;
             const Onb basis = onb_from_normal(h.normal);
             BRec rec{};
             rec.wi = to_local(basis, -normalize(ray.d));
@@ -177,10 +162,10 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
                                 if(!scene_occluded<false>(s, Ray{shadow_origin, shadow_dir}, 0.001f, tmax,
                                                           light.emitter, cnt)) {
                                     c += throughput * f_cos * light.radiance * (w / light_pdf);
-                                    const f3 scale = throughput * light.radiance * (w / light_pdf);
+                                    const f3 scale = delta * (throughput * light.radiance * (w / light_pdf));
                                     for(int32_t k = 0; k < an; ++k) {
-                                        const int32_t j = a.aff_list[ab + k];
-                                        g[j] += dot_rgb(delta, scale * d_eval(a, mid, bctx, rec, j));
+                                        const int32_t grp = a.d.aff_list[ab + k];
+                                        add_group<false>(a.d, g, grp, scale * group_d_eval(a.d, mid, bctx, rec, grp));
                                     }
                                 }
                             }
@@ -195,7 +180,7 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
             if(measure_of(rec.sampled_type) == kSolidAngle && an > 0) {
                 const f3 e0 = bsdf_eval(s.materials, s.tables, mid, bctx, rec, kSolidAngle);
                 for(int32_t k = 0; k < an; ++k) {
-                    const f3 de = d_eval(a, mid, bctx, rec, a.aff_list[ab + k]);
+                    const f3 de = group_d_eval(a.d, mid, bctx, rec, a.d.aff_list[ab + k]);
                     vd[depth][k] = f3{safe_ratio(de.x, e0.x), safe_ratio(de.y, e0.y), safe_ratio(de.z, e0.z)};
                 }
                 vn[depth] = an;
@@ -218,13 +203,13 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
         for(int d = n_vertices - 1; d >= 0; --d) {
             if(vn[d] > 0) {
                 const f3 ds = delta * suffix;
-                const int32_t ab = a.aff_begin[vmid[d]];
-                for(int32_t k = 0; k < vn[d]; ++k) g[a.aff_list[ab + k]] += dot_rgb(ds, vd[d][k]);
+                const int32_t ab = a.d.aff_begin[vmid[d]];
+                for(int32_t k = 0; k < vn[d]; ++k) add_group<false>(a.d, g, a.d.aff_list[ab + k], ds * vd[d][k]);
             }
             suffix += vc[d];
         }
     }
-    for(uint32_t j = 0; j < a.n_params; ++j) {
+    for(uint32_t j = 0; j < a.d.n_params; ++j) {
         float x = g[j];
         for(int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if(lane_id() == 0 && x != 0.0f) atomicAdd(a.grad + j, static_cast<double>(x));
@@ -291,27 +276,53 @@ int lrt_scene_update_materials(lrt_context* ctx, const lrt_material_desc* materi
     return LRT_OK;
 }
 
-int lrt_diff_setup(lrt_context* ctx, uint32_t n_params, const float* steps, const lrt_material_desc* plus,
-                   const lrt_material_desc* minus) {
+int lrt_diff_setup(lrt_context* ctx, uint32_t n_groups, const float* steps, const lrt_material_desc* plus,
+                   const lrt_material_desc* minus, uint32_t n_params, const lrt_diff_param* params) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
     ctx->diff_params = 0;
+    ctx->diff_groups = 0;
     if(n_params == 0 || n_params > kMaxParams) {
         return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "n_params must be in [1, %d]", kMaxParams);
     }
-    if(!steps || !plus || !minus) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    if(n_groups == 0 || n_groups > n_params) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "n_groups must be in [1, n_params]");
+    if(!steps || !plus || !minus || !params) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
     LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    // parameters per group: channels 0..2 at most once each, or one scalar (-1) alone
+    std::vector<std::vector<int32_t>> members(n_groups);
+    for(uint32_t j = 0; j < n_params; ++j) {
+        const lrt_diff_param& p = params[j];
+        if(p.group >= n_groups || p.channel < -1 || p.channel > 2) {
+            return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "parameter %u: group or channel out of range", j);
+        }
+        for(int32_t e : members[p.group]) {
+            const int ch = (e & 3) - 1;
+            if(ch < 0 || p.channel < 0 || ch == p.channel) {
+                return fail(ctx, LRT_ERR_INVALID_ARGUMENT,
+                            "parameter %u: a group holds one scalar parameter or distinct channels", j);
+            }
+        }
+        members[p.group].push_back(static_cast<int32_t>(j << 2) | (p.channel + 1));
+    }
+    std::vector<int32_t> group_begin(n_groups + 1, 0), group_params;
+    for(uint32_t gi = 0; gi < n_groups; ++gi) {
+        if(members[gi].empty()) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "group %u has no parameter", gi);
+        group_begin[gi] = static_cast<int32_t>(group_params.size());
+        group_params.insert(group_params.end(), members[gi].begin(), members[gi].end());
+    }
+    group_begin[n_groups] = static_cast<int32_t>(group_params.size());
+
     const std::vector<MatRec>& base = ctx->host.materials;
     const std::vector<float>& base_tables = ctx->host.tables;
     const uint32_t nm = static_cast<uint32_t>(base.size());
     std::vector<MatRec> all;
     std::vector<float> tables;
-    std::vector<float> inv2step(n_params);
-    std::vector<std::vector<uint8_t>> affected(nm, std::vector<uint8_t>(n_params, 0));
-    all.reserve(2ull * n_params * nm);
-    for(uint32_t j = 0; j < n_params; ++j) {
+    std::vector<float> inv2step(n_groups);
+    std::vector<std::vector<uint8_t>> affected(nm, std::vector<uint8_t>(n_groups, 0));
+    all.reserve(2ull * n_groups * nm);
+    for(uint32_t j = 0; j < n_groups; ++j) {
         if(!(steps[j] > 0.0f) || !std::isfinite(steps[j])) {
-            return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "parameter %u: step must be positive", j);
+            return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "group %u: step must be positive", j);
         }
         inv2step[j] = 1.0f / (2.0f * steps[j]);
         for(int sign = 0; sign < 2; ++sign) {
@@ -320,12 +331,11 @@ int lrt_diff_setup(lrt_context* ctx, uint32_t n_params, const float* steps, cons
             std::vector<float> tabs;
             std::string err;
             const int st = pack_materials(list, nm, recs, tabs, err);
-            if(st != LRT_OK) return fail(ctx, st, "parameter %u: %s", j, err.c_str());
+            if(st != LRT_OK) return fail(ctx, st, "group %u: %s", j, err.c_str());
             const int32_t offset = static_cast<int32_t>(tables.size() / LRT_TRANS_SAMPLES);
             for(uint32_t i = 0; i < nm; ++i) {
                 if(!same_structure(recs[i], base[i])) {
-                    return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "parameter %u: material %u changes type, nesting or flags",
-                                j, i);
+                    return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "group %u: material %u changes type, nesting or flags", j, i);
                 }
                 if(record_differs(recs[i], tabs.data(), base[i], base_tables.data())) affected[i][j] = 1;
                 if(recs[i].table >= 0) recs[i].table += offset;
@@ -334,31 +344,37 @@ int lrt_diff_setup(lrt_context* ctx, uint32_t n_params, const float* steps, cons
             all.insert(all.end(), recs.begin(), recs.end());
         }
     }
-    // a coating moves with the parameters of its nested material (nested index < coating index)
+    // a coating moves with the groups of its nested material (nested index < coating index)
     for(uint32_t i = 0; i < nm; ++i) {
         if(base[i].nested >= 0) {
-            for(uint32_t j = 0; j < n_params; ++j) affected[i][j] |= affected[base[i].nested][j];
+            for(uint32_t j = 0; j < n_groups; ++j) affected[i][j] |= affected[base[i].nested][j];
         }
     }
     std::vector<int32_t> aff_begin(nm + 1, 0), aff_list;
     for(uint32_t i = 0; i < nm; ++i) {
         aff_begin[i] = static_cast<int32_t>(aff_list.size());
-        for(uint32_t j = 0; j < n_params; ++j) {
+        for(uint32_t j = 0; j < n_groups; ++j) {
             if(affected[i][j]) aff_list.push_back(static_cast<int32_t>(j));
         }
         if(aff_list.size() - aff_begin[i] > static_cast<size_t>(kMaxAff)) {
-            return fail(ctx, LRT_ERR_RANGE, "material %u depends on more than %d parameters", i, kMaxAff);
+            return fail(ctx, LRT_ERR_RANGE, "material %u depends on more than %d groups", i, kMaxAff);
         }
     }
     aff_begin[nm] = static_cast<int32_t>(aff_list.size());
+    uint32_t kmax = 0;
+    for(uint32_t i = 0; i < nm; ++i) kmax = std::max<uint32_t>(kmax, aff_begin[i + 1] - aff_begin[i]);
     if(tables.empty()) tables.assign(LRT_TRANS_SAMPLES, 0.0f);
     LRT_CUDA(ctx, put(ctx->diff_mats, all, ctx->stream));
     LRT_CUDA(ctx, put(ctx->diff_tables, tables, ctx->stream));
     LRT_CUDA(ctx, put(ctx->diff_inv2step, inv2step, ctx->stream));
     LRT_CUDA(ctx, put(ctx->diff_aff_begin, aff_begin, ctx->stream));
     LRT_CUDA(ctx, put(ctx->diff_aff_list, aff_list, ctx->stream));
+    LRT_CUDA(ctx, put(ctx->diff_group_begin, group_begin, ctx->stream));
+    LRT_CUDA(ctx, put(ctx->diff_group_params, group_params, ctx->stream));
     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->diff_params = n_params;
+    ctx->diff_groups = n_groups;
+    ctx->diff_kmax = kmax;
     return LRT_OK;
 }
 
@@ -377,6 +393,7 @@ int lrt_render_adjoint_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t 
     unsigned long long total = 0, out_floats = 0;
     const int st = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
     if(st != LRT_OK) return st;
+    if(!ctx->adjoint_megakernel) return adjoint_wavefront(ctx, recs, total, max_depth, rr_depth, adjoint_dev, grad_dev);
     LRT_CUDA(ctx, ctx->batch_jobs.ensure(sizeof(JobRec) * n_jobs));
     LRT_CUDA(ctx, cudaMemcpyAsync(ctx->batch_jobs.ptr, recs.data(), sizeof(JobRec) * n_jobs, cudaMemcpyHostToDevice,
                                   ctx->stream));
@@ -386,12 +403,7 @@ int lrt_render_adjoint_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t 
     a.n_jobs = n_jobs;
     a.total_paths = total;
     a.adjoint = adjoint_dev;
-    a.pert = ctx->diff_mats.as<MatRec>();
-    a.pert_tables = ctx->diff_tables.as<float>();
-    a.inv2step = ctx->diff_inv2step.as<float>();
-    a.aff_begin = ctx->diff_aff_begin.as<int32_t>();
-    a.aff_list = ctx->diff_aff_list.as<int32_t>();
-    a.n_params = ctx->diff_params;
+    a.d = diff_dev(ctx);
     a.max_depth = max_depth;
     a.rr_depth = rr_depth;
     a.grad = grad_dev;

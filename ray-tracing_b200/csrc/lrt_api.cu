@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "lrt_adjoint.cuh"
 #include "lrt_context.cuh"
 #include "lrt_scene.cuh"
 
@@ -222,6 +223,18 @@ struct WaveArgs {
     unsigned long long total_paths;
     float* batch_out;
     float* batch_sums;              // running per-pixel sums where a pixel spans waves
+    // path-replay adjoint (null for renders)
+    const float* adjoint;           // dLoss/dimage, batch output layout
+    DiffDev diff;
+    uint32_t adj_kmax;              // groups per material at most
+    uint32_t* adj_vmask;            // per slot: depths whose sampled direction carries a derivative record
+    int32_t* adj_vmid;              // [depth][capacity] material of that record
+    float4* adj_lsnap;              // [depth][capacity] radiance gathered through depth (incl. its NEE)
+    float4* adj_dlog;               // [depth][kmax][capacity] dE/E of the sampled direction per group
+    int32_t* adj_sh_mid;            // [2 capacity] material of each shadow ray's vertex, -1 none
+    uint8_t* adj_sh_vis;            // [2 capacity] shadow ray unoccluded
+    float4* adj_sh_prod;            // [kmax][2 capacity] adjoint x dNEE per group
+    double* adj_grad;
 };
 
 // the material of object `obj` for path `pid`: a batch job may replace one object's material
@@ -379,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
 
 // shadow rays with ray replacement: any-hit unless the light's own shape is reachable (then the
 // closest hit decides, scene_occluded)
-template <bool kCount>
+template <bool kCount, bool kVis = false>
 __global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int depth) {
     BounceCounters& bc = a.counters[depth];
     const uint32_t n0 = bc.shadow[0];
@@ -416,6 +429,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int de
         if(!__any_sync(0xffffffffu, active)) break;
         if(active && trav_step<kCount>(a.s, st, stack, cnt)) {
             const bool blocked = st.any_mode ? st.best >= 0 : (st.best >= 0 && a.s.objects[st.best].emitter != light);
+            if(kVis) a.adj_sh_vis[k] = blocked ? 0 : 1;
             if(!blocked) {
                 const float4 c = a.sh_c[k];
                 const uint32_t p = __float_as_uint(c.w);
@@ -435,8 +449,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int de
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
-    __shared__ uint32_t prefix[kKeys + 1];
+// one bounce of shading; kAdj adds the adjoint's derivative records (sampled direction, NEE)
+template <bool kAdj>
+__device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_t* prefix) {
     BounceCounters& bc = a.counters[depth];
     if(threadIdx.x == 0) {
         uint32_t acc = 0;
@@ -465,6 +480,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
         f3 result{L4.x, L4.y, L4.z};
         const bool have_pdf = misc.y != 0.0f;
         const float sa_pdf = misc.x;
+        f3 delta = mk(0.0f);
+        if(kAdj) {  // this path's share of dLoss/dimage; the radiance gathered through the previous depth
+            const JobRec& job = a.jobs[a.path_job[pid]];
+            delta = load3(a.adjoint + job.out_offset + 3ull * a.id[pid].x) / static_cast<float>(job.spp);
+            if(depth > 0) a.adj_lsnap[static_cast<size_t>(depth - 1) * a.capacity + pid] = L4;
+        }
 
         if(key == 0) {  // miss: environment + MIS (path_integrator.h:32-45); rec.p of a miss is (0,0,0)
             const f3 Le = eval_environment(s, rd);
@@ -551,6 +572,21 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
                             a.sh_o[si] = make_float4(shadow_origin.x, shadow_origin.y, shadow_origin.z, tmax);
                             a.sh_d[si] = make_float4(shadow_dir.x, shadow_dir.y, shadow_dir.z, __int_as_float(light.emitter));
                             a.sh_c[si] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(pid));
+                            if(kAdj) {  // delta x dNEE per group, kept until the shadow ray's visibility is known
+                                int32_t smid = -1;
+                                if(!is_zero(delta)) {
+                                    const f3 scale = delta * (throughput * light.radiance * (w / light_pdf));
+                                    const int32_t ab = a.diff.aff_begin[mid];
+                                    const int32_t an = a.diff.aff_begin[mid + 1] - ab;
+                                    for(int32_t k = 0; k < an; ++k) {
+                                        const f3 v = scale * group_d_eval(a.diff, mid, ctx, rec, a.diff.aff_list[ab + k]);
+                                        a.adj_sh_prod[static_cast<size_t>(k) * 2 * a.capacity + si] =
+                                            make_float4(v.x, v.y, v.z, 0.0f);
+                                    }
+                                    if(an > 0) smid = mid;
+                                }
+                                a.adj_sh_mid[si] = smid;
+                            }
                         }
                     }
                 }
@@ -585,9 +621,58 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
             a.misc[pid] = make_float2(rec.pdf, have ? 1.0f : 0.0f);
             const int seg = heavy_key(s, Ray{p, new_dir}, 0.001f, kInf);
             next[static_cast<size_t>(seg) * a.capacity + warp_append_keyed(nc.active, seg)] = pid;
+            if(kAdj && !is_zero(delta) && measure_of(rec.sampled_type) == kSolidAngle) {
+                // dE/E of the sampled direction per group; its suffix is known at the end of the wave
+                const int32_t ab = a.diff.aff_begin[mid];
+                const int32_t an = a.diff.aff_begin[mid + 1] - ab;
+                if(an > 0) {
+                    const f3 e0 = bsdf_eval(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                    for(int32_t k = 0; k < an; ++k) {
+                        const f3 de = group_d_eval(a.diff, mid, ctx, rec, a.diff.aff_list[ab + k]);
+                        a.adj_dlog[(static_cast<size_t>(depth) * a.adj_kmax + k) * a.capacity + pid] =
+                            make_float4(safe_ratio(de.x, e0.x), safe_ratio(de.y, e0.y), safe_ratio(de.z, e0.z), 0.0f);
+                    }
+                    a.adj_vmid[static_cast<size_t>(depth) * a.capacity + pid] = mid;
+                    a.adj_vmask[pid] |= 1u << depth;
+                }
+            }
         }
     }
     if(a.work) add_count(&a.work[2], shading);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
+    __shared__ uint32_t prefix[kKeys + 1];
+    shade_wave<false>(a, depth, prefix);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
+    __shared__ uint32_t prefix[kKeys + 1];
+    shade_wave<true>(a, depth, prefix);
+}
+
+// adjoint: the NEE derivatives of the shadow rays of one depth that reached their light
+__global__ void __launch_bounds__(kBlock) k_adj_nee(WaveArgs a, int depth) {
+    __shared__ float acc[LRT_MAX_DIFF_PARAMS];
+    for(uint32_t j = threadIdx.x; j < a.diff.n_params; j += blockDim.x) acc[j] = 0.0f;
+    __syncthreads();
+    const uint32_t n0 = a.counters[depth].shadow[0];
+    const uint32_t n = n0 + a.counters[depth].shadow[1];
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t k = i < n0 ? i : a.capacity + (i - n0);
+        const int32_t mid = a.adj_sh_mid[k];
+        if(mid < 0 || !a.adj_sh_vis[k]) continue;
+        const int32_t ab = a.diff.aff_begin[mid];
+        const int32_t an = a.diff.aff_begin[mid + 1] - ab;
+        for(int32_t g = 0; g < an; ++g) {
+            const float4 v = a.adj_sh_prod[static_cast<size_t>(g) * 2 * a.capacity + k];
+            add_group<true>(a.diff, acc, a.diff.aff_list[ab + g], f3{v.x, v.y, v.z});
+        }
+    }
+    __syncthreads();
+    for(uint32_t j = threadIdx.x; j < a.diff.n_params; j += blockDim.x) {
+        if(acc[j] != 0.0f) atomicAdd(a.adj_grad + j, static_cast<double>(acc[j]));
+    }
 }
 
 template <bool kCount>
@@ -709,6 +794,39 @@ __global__ void __launch_bounds__(kBlock) k_accumulate_batch(WaveArgs a) {
 
 __global__ void k_wave_advance(WaveArgs a) {
     if(blockIdx.x == 0 && threadIdx.x == 0) *a.wave_base += a.capacity;
+}
+
+// adjoint, once per wave after its last depth: every derivative record of a sampled direction times
+// what the path gathered after that depth (its final radiance minus the radiance through the depth)
+__global__ void __launch_bounds__(kBlock) k_adj_suffix(WaveArgs a) {
+    __shared__ float acc[LRT_MAX_DIFF_PARAMS];
+    for(uint32_t j = threadIdx.x; j < a.diff.n_params; j += blockDim.x) acc[j] = 0.0f;
+    __syncthreads();
+    const uint32_t n = wave_slots(a);
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        uint32_t mask = a.adj_vmask[slot];
+        if(mask == 0) continue;
+        const JobRec& job = a.jobs[a.path_job[slot]];
+        const f3 delta = load3(a.adjoint + job.out_offset + 3ull * a.id[slot].x) / static_cast<float>(job.spp);
+        const float4 L = a.L[slot];
+        while(mask != 0) {
+            const int d = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float4 before = a.adj_lsnap[static_cast<size_t>(d) * a.capacity + slot];
+            const f3 w = delta * f3{L.x - before.x, L.y - before.y, L.z - before.z};
+            const int32_t mid = a.adj_vmid[static_cast<size_t>(d) * a.capacity + slot];
+            const int32_t ab = a.diff.aff_begin[mid];
+            const int32_t an = a.diff.aff_begin[mid + 1] - ab;
+            for(int32_t g = 0; g < an; ++g) {
+                const float4 v = a.adj_dlog[(static_cast<size_t>(d) * a.adj_kmax + g) * a.capacity + slot];
+                add_group<true>(a.diff, acc, a.diff.aff_list[ab + g], w * f3{v.x, v.y, v.z});
+            }
+        }
+    }
+    __syncthreads();
+    for(uint32_t j = threadIdx.x; j < a.diff.n_params; j += blockDim.x) {
+        if(acc[j] != 0.0f) atomicAdd(a.adj_grad + j, static_cast<double>(acc[j]));
+    }
 }
 
 int ensure_wave(lrt_context* ctx, uint32_t cap) {
@@ -904,30 +1022,23 @@ void launch_batch_wave(lrt_context* ctx, const WaveArgs& a, size_t counters_byte
     k_wave_advance<<<1, 32, 0, ctx->stream>>>(a);
 }
 
-int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
-                      float* rgb_dev) {
-    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
-    if(n_jobs == 0) return LRT_OK;
-    if(!jobs || !rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
-    if(max_depth < 1 || max_depth > 1024) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "max_depth out of range");
-    std::vector<JobRec> recs;
-    unsigned long long total = 0, out_floats = 0;
-    const int jst = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
-    if(jst != LRT_OK) return jst;
+// the wave state, counters and job table of a batch of paths (jobs already validated)
+int batch_wave_args(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned long long total, int32_t max_depth,
+                    int32_t rr_depth, WaveArgs& a) {
     const uint32_t cap = ctx->wave_capacity;
+    const uint32_t n_jobs = static_cast<uint32_t>(recs.size());
     int st = ensure_wave(ctx, cap);
     if(st != LRT_OK) return st;
     const size_t counters_bytes = sizeof(BounceCounters) * (max_depth + 1);
     LRT_CUDA(ctx, ctx->counters.ensure(counters_bytes));
     LRT_CUDA(ctx, ctx->batch_jobs.ensure(sizeof(JobRec) * n_jobs));
     LRT_CUDA(ctx, ctx->batch_path_job.ensure(4ull * cap));
-    LRT_CUDA(ctx, ctx->batch_sums.ensure(4ull * out_floats));
     LRT_CUDA(ctx, ctx->batch_cursor.ensure(8));
     LRT_CUDA(ctx, cudaMemcpyAsync(ctx->batch_jobs.ptr, recs.data(), sizeof(JobRec) * n_jobs, cudaMemcpyHostToDevice,
                                   ctx->stream));
     LRT_CUDA(ctx, cudaMemsetAsync(ctx->batch_cursor.ptr, 0, 8, ctx->stream));
     WaveState& w = ctx->wave;
-    WaveArgs a{};
+    a = WaveArgs{};
     a.s = ctx->ds;
     a.o = w.o.as<float4>();
     a.d = w.d.as<float4>();
@@ -954,21 +1065,18 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
     a.path_job = ctx->batch_path_job.as<uint32_t>();
     a.wave_base = ctx->batch_cursor.as<unsigned long long>();
     a.total_paths = total;
-    a.batch_out = rgb_dev;
-    a.batch_sums = ctx->batch_sums.as<float>();
-    const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
-    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
-    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
-    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
-    const int g_accum = grid_for(ctx, (const void*)k_accumulate_batch, kBlock);
-    const unsigned long long waves = (total + cap - 1) / cap;
-    const uint64_t per_wave = 3 + 4ull * max_depth;
+    return LRT_OK;
+}
+
+// replays `launch_one` (the launch sequence of one wave, which advances the device cursor) `waves`
+// times: captured once into a CUDA graph, or launched directly when the batch_graph option is off
+template <typename F>
+int run_waves(lrt_context* ctx, unsigned long long waves, F launch_one) {
     if(ctx->batch_graph) {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         LRT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
+        launch_one();
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if(ce != cudaSuccess) return fail(ctx, LRT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
         const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
@@ -982,11 +1090,41 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
         cudaGraphDestroy(graph);
         if(le != cudaSuccess) return fail(ctx, LRT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(le));
     } else {
-        for(unsigned long long i = 0; i < waves; ++i) {
-            launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
-        }
+        for(unsigned long long i = 0; i < waves; ++i) launch_one();
         LRT_CUDA(ctx, cudaGetLastError());
     }
+    return LRT_OK;
+}
+
+int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
+                      float* rgb_dev) {
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    if(n_jobs == 0) return LRT_OK;
+    if(!jobs || !rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    if(max_depth < 1 || max_depth > 1024) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "max_depth out of range");
+    std::vector<JobRec> recs;
+    unsigned long long total = 0, out_floats = 0;
+    const int jst = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
+    if(jst != LRT_OK) return jst;
+    WaveArgs a;
+    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, a);
+    if(st != LRT_OK) return st;
+    LRT_CUDA(ctx, ctx->batch_sums.ensure(4ull * out_floats));
+    a.batch_out = rgb_dev;
+    a.batch_sums = ctx->batch_sums.as<float>();
+    const size_t counters_bytes = sizeof(BounceCounters) * (max_depth + 1);
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
+    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
+    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
+    const int g_accum = grid_for(ctx, (const void*)k_accumulate_batch, kBlock);
+    const unsigned long long waves = (total + a.capacity - 1) / a.capacity;
+    const uint64_t per_wave = 3 + 4ull * max_depth;
+    const int rst = run_waves(ctx, waves, [&]() {
+        launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
+    });
+    if(rst != LRT_OK) return rst;
     ctx->stats.paths += total;
     ctx->stats.kernel_launches += waves * per_wave;
     return LRT_OK;
@@ -994,6 +1132,65 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
 
 }  // namespace
 
+
+namespace lrt {
+
+int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned long long total, int32_t max_depth,
+                      int32_t rr_depth, const float* adjoint_dev, double* grad_dev) {
+    WaveArgs a;
+    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, a);
+    if(st != LRT_OK) return st;
+    const size_t cap = a.capacity;
+    const uint32_t kmax = std::max<uint32_t>(1, ctx->diff_kmax);
+    LRT_CUDA(ctx, ctx->adj_vmask.ensure(4 * cap));
+    LRT_CUDA(ctx, ctx->adj_vmid.ensure(4 * cap * max_depth));
+    LRT_CUDA(ctx, ctx->adj_lsnap.ensure(16 * cap * max_depth));
+    LRT_CUDA(ctx, ctx->adj_dlog.ensure(16 * cap * max_depth * kmax));
+    LRT_CUDA(ctx, ctx->adj_sh_mid.ensure(4 * 2 * cap));
+    LRT_CUDA(ctx, ctx->adj_sh_vis.ensure(2 * cap));
+    LRT_CUDA(ctx, ctx->adj_sh_prod.ensure(16 * 2 * cap * kmax));
+    a.adjoint = adjoint_dev;
+    a.diff = diff_dev(ctx);
+    a.adj_kmax = kmax;
+    a.adj_vmask = ctx->adj_vmask.as<uint32_t>();
+    a.adj_vmid = ctx->adj_vmid.as<int32_t>();
+    a.adj_lsnap = ctx->adj_lsnap.as<float4>();
+    a.adj_dlog = ctx->adj_dlog.as<float4>();
+    a.adj_sh_mid = ctx->adj_sh_mid.as<int32_t>();
+    a.adj_sh_vis = ctx->adj_sh_vis.as<uint8_t>();
+    a.adj_sh_prod = ctx->adj_sh_prod.as<float4>();
+    a.adj_grad = grad_dev;
+    const size_t counters_bytes = sizeof(BounceCounters) * (max_depth + 1);
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
+    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
+    const int g_shade = grid_for(ctx, (const void*)k_shade_adj, kBlock);
+    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false, true>, kBlock);
+    const int g_nee = grid_for(ctx, (const void*)k_adj_nee, kBlock);
+    const int g_suffix = grid_for(ctx, (const void*)k_adj_suffix, kBlock);
+    cudaStream_t sm = ctx->stream;
+    const unsigned long long waves = (total + cap - 1) / cap;
+    const int rst = run_waves(ctx, waves, [&]() {
+        cudaMemsetAsync(a.counters, 0, counters_bytes, sm);
+        cudaMemsetAsync(a.adj_vmask, 0, 4 * cap, sm);
+        k_raygen_batch<<<g_raygen, kBlock, 0, sm>>>(a);
+        for(int depth = 0; depth < max_depth; ++depth) {
+            k_extend_persistent<false><<<g_extend, kBlock, 0, sm>>>(a, depth);
+            k_hitrec<<<g_hitrec, kBlock, 0, sm>>>(a, depth);
+            k_shade_adj<<<g_shade, kBlock, 0, sm>>>(a, depth);
+            k_shadow_persistent<false, true><<<g_shadow, kBlock, 0, sm>>>(a, depth);
+            k_adj_nee<<<g_nee, kBlock, 0, sm>>>(a, depth);
+        }
+        k_adj_suffix<<<g_suffix, kBlock, 0, sm>>>(a);
+        k_wave_advance<<<1, 32, 0, sm>>>(a);
+    });
+    if(rst != LRT_OK) return rst;
+    ctx->stats.paths += total;
+    ctx->stats.kernel_launches += waves * (3 + 5ull * max_depth);
+    return LRT_OK;
+}
+
+}  // namespace lrt
 // ======================================= C ABI =======================================
 
 extern "C" {
@@ -1376,6 +1573,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->count_work = value != 0;
     } else if(strcmp(name, "batch_graph") == 0) {
         ctx->batch_graph = value != 0;
+    } else if(strcmp(name, "adjoint_megakernel") == 0) {
+        ctx->adjoint_megakernel = value != 0;
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
     } else if(strcmp(name, "wave_capacity") == 0) {

@@ -101,7 +101,12 @@ struct lrt_context {
     bool batch_graph = true;
     // differentiation: per parameter the material list moved by +step and by -step
     uint32_t diff_params = 0;  // 0: no lrt_diff_setup for the current materials
-    lrt::DevBuf diff_mats, diff_tables, diff_inv2step, diff_aff_begin, diff_aff_list, diff_adjoint, diff_grad;
+    uint32_t diff_groups = 0;
+    uint32_t diff_kmax = 0;             // most groups that move one material
+    bool adjoint_megakernel = false;    // true: the one-thread-per-path adjoint kernel
+    lrt::DevBuf adj_vmask, adj_vmid, adj_lsnap, adj_dlog, adj_sh_mid, adj_sh_vis, adj_sh_prod;
+    lrt::DevBuf diff_mats, diff_tables, diff_inv2step, diff_aff_begin, diff_aff_list, diff_group_begin,
+        diff_group_params, diff_adjoint, diff_grad;
     lrt_render_stats stats{};
     bool stage_timing = false;
     bool count_work = false;

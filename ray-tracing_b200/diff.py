@@ -1,10 +1,12 @@
 """Material parameters of a scene as a flat vector, and the caller side of liblrt's path-replay adjoint.
 
 A parameter is one scalar of one material: an albedo channel (diffuse_reflectance of diffuse, plastic
-and rough plastic), a roughness (alpha of the rough materials) or a conductor eta / k channel. For
-each parameter the library receives the scene's material list moved by +step and by -step (with the
-rough-transmittance tables re-sliced where alpha moves) and differentiates the BSDF values on every
-path by those records (lrt_diff_setup, lrt_render_adjoint).
+and rough plastic), a roughness (alpha of the rough materials) or a conductor eta / k channel. The
+channels of one field form a group, moved together, since channel c of a BSDF value moves only with
+channel c of the field; a roughness is a group of its own. For each group the library receives the
+scene's material list moved by +step and by -step (with the rough-transmittance tables re-sliced
+where alpha moves) and differentiates the BSDF values on every path by those records
+(lrt_diff_setup, lrt_render_adjoint).
 """
 from __future__ import annotations
 
@@ -59,6 +61,18 @@ def set_value(materials, p, value) -> None:
         materials[i][field] = tuple(v)
 
 
+def param_groups(params):
+    """(group of each parameter, channel of each parameter (-1: scalar), number of groups)"""
+    keys, group, chan = {}, [], []
+    for (m, field, c) in params:
+        key = (m, field) if c is not None else (m, field, "scalar")
+        if key not in keys:
+            keys[key] = len(keys)
+        group.append(keys[key])
+        chan.append(-1 if c is None else int(c))
+    return group, chan, len(keys)
+
+
 def with_values(materials, params, values):
     """a copy of the material list with the parameters set (tables re-sliced)"""
     mats = copy.deepcopy(materials)
@@ -100,18 +114,23 @@ class Differentiable:
 
     def _setup(self) -> None:
         nm = len(self.materials)
-        n = len(self.params)
-        plus = (abi.MaterialDesc * (n * nm))()
-        minus = (abi.MaterialDesc * (n * nm))()
+        group, chan, n_groups = param_groups(self.params)
+        plus = (abi.MaterialDesc * (n_groups * nm))()
+        minus = (abi.MaterialDesc * (n_groups * nm))()
         base = self.values()
-        for j, p in enumerate(self.params):
-            h = float(self.steps[j])
+        steps = np.zeros(n_groups, dtype=np.float32)
+        for g in range(n_groups):
+            members = [j for j in range(len(self.params)) if group[j] == g]
+            steps[g] = self.steps[members[0]]
             for arr, sign in ((plus, 1.0), (minus, -1.0)):
                 moved = copy.deepcopy(self.materials)
-                set_value(moved, p, base[j] + sign * h)
+                for j in members:
+                    set_value(moved, self.params[j], base[j] + sign * float(steps[g]))
                 scenes.attach_tables(moved)
-                abi.material_descs(moved, arr, j * nm)
-        self.ctx._check(lrt.lib().lrt_diff_setup(self.ctx.handle, n, lrt.ptr(self.steps, C.c_float), plus, minus))
+                abi.material_descs(moved, arr, g * nm)
+        desc = (abi.DiffParam * len(self.params))(*[abi.DiffParam(g, c) for g, c in zip(group, chan)])
+        self.ctx._check(lrt.lib().lrt_diff_setup(self.ctx.handle, n_groups, lrt.ptr(steps, C.c_float), plus, minus,
+                                                 len(self.params), desc))
 
     def adjoint(self, jobs, max_depth: int, rr_depth: int, adjoint_image: np.ndarray) -> np.ndarray:
         arr = (abi.JobDesc * len(jobs))(*jobs)

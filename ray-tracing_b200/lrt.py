@@ -86,7 +86,8 @@ def lib():
         L.lrt_rough_transmittance_eta_slice.argtypes = [C.c_char_p, f32, P(f32), P(f32), u32, P(u32), P(f32)]
         L.lrt_rough_transmittance_at_alpha.argtypes = [P(f32), P(f32), u32, P(f32), f32, P(f32), P(f32)]
         L.lrt_scene_update_materials.argtypes = [vp, P(abi.MaterialDesc), u32]
-        L.lrt_diff_setup.argtypes = [vp, u32, P(f32), P(abi.MaterialDesc), P(abi.MaterialDesc)]
+        L.lrt_diff_setup.argtypes = [vp, u32, P(f32), P(abi.MaterialDesc), P(abi.MaterialDesc), u32,
+                                     P(abi.DiffParam)]
         L.lrt_render_adjoint.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32), P(C.c_double)]
         L.lrt_render_adjoint_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp, vp]
         L.lrt_render_stats_get.argtypes = [vp, P(abi.RenderStats)]

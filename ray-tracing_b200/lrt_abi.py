@@ -122,6 +122,10 @@ def camera_desc(camera: dict) -> CameraDesc:
     return cam
 
 
+class DiffParam(C.Structure):
+    _fields_ = [("group", C.c_uint32), ("channel", C.c_int32)]
+
+
 class JobDesc(C.Structure):
     _fields_ = [("camera", CameraDesc), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
                 ("sample_offset", C.c_uint32), ("override_object", C.c_int32), ("override_material", C.c_int32),

@@ -210,3 +210,25 @@ def test_adam_moves_roughness_to_target(ctx):
     loss_end = clean_loss(final)
     assert np.abs(final - 0.3).mean() < 0.5 * np.abs(start - 0.3).mean(), final
     assert loss_end < loss_start, (loss_start, loss_end)
+
+
+@pytest.mark.parametrize("cap", [1 << 21, 4096])
+def test_wavefront_adjoint_equals_megakernel(ctx, library3, cap):
+    """the wavefront adjoint (per-depth records, suffix pass per wave) and the one-thread-per-path
+    kernel replay the same paths; with roulette on and, at the small capacity, pixels split across
+    waves, their gradients differ only by float summation order"""
+    scene, sphere, index = library3
+    ctx.upload(scene)
+    dm = diff.Differentiable(ctx, scene)
+    jobs, floats = fd_jobs(scene, sphere, index, 24, 20, 6, 1)
+    w = np.random.default_rng(9).uniform(-1, 1, floats).astype(np.float32)
+    try:
+        ctx.set_option("wave_capacity", cap)
+        wave = dm.adjoint(jobs, DEPTH, RR, w)
+        ctx.set_option("adjoint_megakernel", 1)
+        mega = dm.adjoint(jobs, DEPTH, RR, w)
+    finally:
+        ctx.set_option("adjoint_megakernel", 0)
+        ctx.set_option("wave_capacity", 1 << 21)
+    assert np.abs(mega).max() > 0
+    np.testing.assert_allclose(wave, mega, rtol=1e-3, atol=1e-5 * np.abs(mega).max())

@@ -180,3 +180,13 @@ def test_diff_params_of_material_library():
     assert not np.array_equal(moved[rp]["trans_table"], scene.materials[rp]["trans_table"])
     back = diff.with_values(moved, [p], [0.15])
     assert np.array_equal(back[rp]["trans_table"], scene.materials[rp]["trans_table"])
+
+
+def test_diff_param_groups():
+    import diff
+    params = [(0, "diffuse_reflectance", 0), (0, "diffuse_reflectance", 1), (5, "alpha", None), (5, "eta", 2),
+              (0, "diffuse_reflectance", 2), (5, "eta", 0), (7, "alpha", None)]
+    group, chan, n = diff.param_groups(params)
+    assert n == 4
+    assert group == [0, 0, 1, 2, 0, 2, 3]
+    assert chan == [0, 1, -1, 2, 2, 0, -1]
