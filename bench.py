@@ -379,7 +379,9 @@ def run_batch(args):
                          "gpu_launches": int(ctx.stats()["kernel_launches"])}
         images[name] = out.cpu().numpy()
     clock_info = clocks.stop()
-    same = all(np.array_equal(images["batched"], images[k]) for k in images)
+    same = all(np.array_equal(images["batched"], images[k], equal_nan=True) for k in images)
+    nonfinite = {k: int((~np.isfinite(v)).sum()) for k, v in images.items()}
+    max_diff = {k: float(np.nanmax(np.abs(images["batched"] - v))) for k, v in images.items()}
 
     # end to end: lrt_render_batch with the host output buffer
     host = np.zeros(floats, dtype=np.float32)
@@ -395,7 +397,8 @@ def run_batch(args):
             "config": {"workload": "batch_%d_jobs_seed_%d" % (len(jobs), scenes.BATCH_SEED), "jobs": len(jobs),
                        "paths_per_step": n_paths, "max_depth": DEPTH, "rr_depth": RR,
                        "l2": "flushed (256 MB write) between timed steps", "arms": results,
-                       "images_identical_across_arms": same},
+                       "images_identical_across_arms": same, "nonfinite_floats": nonfinite,
+                       "max_abs_diff_to_batched": max_diff},
             "e2e": {"value": e2e, "unit": "jobs/s", "h2d_bytes_per_step": 80 * len(jobs),
                     "d2h_bytes_per_step": 4 * floats, "path": "lrt_render_batch (host output buffer)"},
             "clocks": clock_info, "gpu_launches": b["gpu_launches"]}
