@@ -324,6 +324,7 @@ BATCH_METRIC = "jobs/s (64 seeded jobs: 128^2..1024x768, 4-256 spp, 7 materials,
 
 def run_batch(args):
     import torch
+    import autotune
     import lrt
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -339,6 +340,10 @@ def run_batch(args):
     ctx.upload(scene)
     out = torch.zeros(floats, dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    tuned = {"launch_config": dict(autotune.DEFAULTS), "autotune": "off"}
+    if not args.no_autotune:
+        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), lambda: torch.cuda.synchronize(dev))
+        tuned = {"launch_config": cfg, "autotune": "cache hit" if hit else "tuned now", "autotune_key": key}
 
     def batched():
         ctx.render_batch_dev(jobs, DEPTH, RR, out.data_ptr())
@@ -398,7 +403,7 @@ def run_batch(args):
                        "paths_per_step": n_paths, "max_depth": DEPTH, "rr_depth": RR,
                        "l2": "flushed (256 MB write) between timed steps", "arms": results,
                        "images_identical_across_arms": same, "nonfinite_floats": nonfinite,
-                       "max_abs_diff_to_batched": max_diff},
+                       "max_abs_diff_to_batched": max_diff, **tuned},
             "e2e": {"value": e2e, "unit": "jobs/s", "h2d_bytes_per_step": 80 * len(jobs),
                     "d2h_bytes_per_step": 4 * floats, "path": "lrt_render_batch (host output buffer)"},
             "clocks": clock_info, "gpu_launches": b["gpu_launches"]}
@@ -543,6 +548,7 @@ def main():
                     help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison; "
                          "adjoint: gradient steps of the material optimisation")
     ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--no-autotune", action="store_true", help="batch workload: default launch shapes")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":

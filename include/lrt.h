@@ -415,7 +415,10 @@ int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
 int lrt_render_stats_reset(lrt_context* ctx);
 /* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26),
  * "photon_tree_device" (0/1), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
- * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one) */
+ * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
+ * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
+ * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major).
+ * The last four change speed only, never an image. */
 int lrt_set_option(lrt_context* ctx, const char* name, int64_t value);
 
 /* photons: particles [0, ...) traced in index order until `requested` photons are stored */

@@ -223,6 +223,7 @@ struct WaveArgs {
     unsigned long long total_paths;
     float* batch_out;
     float* batch_sums;              // running per-pixel sums where a pixel spans waves
+    uint32_t pixel_tile;            // path order within a job: bands of this many rows, column by column
     // path-replay adjoint (null for renders)
     const float* adjoint;           // dLoss/dimage, batch output layout
     DiffDev diff;
@@ -746,7 +747,15 @@ __global__ void __launch_bounds__(kBlock) k_raygen_batch(WaveArgs a) {
         }
         const JobRec& job = a.jobs[lo];
         const unsigned long long local = g - job.path_begin;
-        const uint32_t pix = static_cast<uint32_t>(local / job.spp);
+        const uint32_t q = static_cast<uint32_t>(local / job.spp);  // the job's q-th pixel in path order
+        uint32_t pix = q;
+        if(a.pixel_tile > 1) {  // bands of pixel_tile rows, each band column by column
+            const uint32_t band = q / (a.pixel_tile * job.width);
+            const uint32_t y0 = band * a.pixel_tile;
+            const uint32_t bh = min(a.pixel_tile, job.height - y0);
+            const uint32_t r = q - y0 * job.width;
+            pix = (y0 + r % bh) * job.width + r / bh;
+        }
         const uint32_t sample = job.sample_offset + static_cast<uint32_t>(local % job.spp);
         Sampler smp = sampler_start(pix, sample);
         const F2 off = sampler_next_2d(sobol_table(a.s), smp);
@@ -1065,6 +1074,7 @@ int batch_wave_args(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned 
     a.path_job = ctx->batch_path_job.as<uint32_t>();
     a.wave_base = ctx->batch_cursor.as<unsigned long long>();
     a.total_paths = total;
+    a.pixel_tile = ctx->pixel_tile;
     return LRT_OK;
 }
 
@@ -1575,6 +1585,12 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->batch_graph = value != 0;
     } else if(strcmp(name, "adjoint_megakernel") == 0) {
         ctx->adjoint_megakernel = value != 0;
+    } else if(strcmp(name, "blocks_per_sm") == 0) {
+        if(value < 0 || value > 32) return fail(ctx, LRT_ERR_RANGE, "blocks_per_sm must be in [0, 32]");
+        ctx->blocks_per_sm_cap = static_cast<uint32_t>(value);
+    } else if(strcmp(name, "pixel_tile") == 0) {
+        if(value < 1 || value > 64) return fail(ctx, LRT_ERR_RANGE, "pixel_tile must be in [1, 64]");
+        ctx->pixel_tile = static_cast<uint32_t>(value);
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
     } else if(strcmp(name, "wave_capacity") == 0) {

@@ -111,6 +111,8 @@ struct lrt_context {
     bool stage_timing = false;
     bool count_work = false;
     uint32_t wave_capacity = 1u << 21;
+    uint32_t blocks_per_sm_cap = 0;  // 0: as many resident blocks per SM as occupancy allows
+    uint32_t pixel_tile = 1;         // batch path order: bands of this many rows, column by column
     std::vector<cudaEvent_t> events;
     std::vector<int> event_stage;
     // photons
@@ -150,6 +152,9 @@ inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 inline int grid_for(lrt_context* ctx, const void* kernel, int block) {
     int per_sm = 0;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    if(ctx->blocks_per_sm_cap > 0 && per_sm > static_cast<int>(ctx->blocks_per_sm_cap)) {
+        per_sm = static_cast<int>(ctx->blocks_per_sm_cap);
+    }
     return ctx->sm_count * per_sm;
 }
 

@@ -141,3 +141,32 @@ def test_plain_path_tracer_equals_batch(ctx, library):
     plain = ctx.render_plain(jobs, DEPTH, RR)
     batch = ctx.render_batch(jobs, DEPTH, RR)
     assert np.array_equal(plain, batch)
+
+
+def test_launch_knobs_keep_images(ctx, library, tmp_path):
+    """pixel_tile (a path-order bijection, here on sizes that are not multiples of the tile),
+    blocks_per_sm and wave_capacity change speed only; the autotuner picks among them and caches"""
+    import autotune
+    scene, sphere, index = library
+    jobs = [scenes.job_desc(scene.camera, 37, 29, 5, 0, sphere, index["rough_plastic"], 0),
+            scenes.job_desc(scene.camera, 21, 34, 3, 4, sphere, index["coating"], 3 * 37 * 29)]
+    ctx.upload(scene)
+    ref = ctx.render_batch(jobs, DEPTH, RR)
+    try:
+        for knob, v in [("pixel_tile", 3), ("pixel_tile", 8), ("pixel_tile", 64), ("blocks_per_sm", 1),
+                        ("blocks_per_sm", 2), ("wave_capacity", 2048)]:
+            ctx.set_option(knob, v)
+            assert np.array_equal(ctx.render_batch(jobs, DEPTH, RR), ref), (knob, v)
+            autotune.apply(ctx, autotune.DEFAULTS)
+        import torch
+        out = torch.zeros(ref.size, dtype=torch.float32, device="cuda")
+        cache = str(tmp_path / "cache.json")
+        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), torch.cuda.synchronize,
+                                       cache_path=cache)
+        assert not hit and all(cfg[k] in autotune.CANDIDATES[k] for k in autotune.ORDER)
+        cfg2, key2, hit2 = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), torch.cuda.synchronize,
+                                          cache_path=cache)
+        assert hit2 and cfg2 == cfg and key2 == key
+        assert np.array_equal(ctx.render_batch(jobs, DEPTH, RR), ref)
+    finally:
+        autotune.apply(ctx, autotune.DEFAULTS)

@@ -2,6 +2,7 @@
 restatements (SAH kd-tree build, ggx.dat slicing, Fdr quadrature, Sobol table) match the reference.
 No GPU work is launched here."""
 import ctypes as C
+import math
 import os
 import re
 
@@ -190,3 +191,24 @@ def test_diff_param_groups():
     assert n == 4
     assert group == [0, 0, 1, 2, 0, 2, 3]
     assert chan == [0, 1, -1, 2, 2, 0, -1]
+
+
+def test_autotune_coordinate_descent_and_keys():
+    import autotune
+    # a separable cost with its minimum at capacity 2^20, tile 8, blocks 2
+    target = {"wave_capacity": 1 << 20, "pixel_tile": 8, "blocks_per_sm": 2}
+    calls = []
+
+    def measure(cfg):
+        calls.append(dict(cfg))
+        return sum(abs(math.log2(max(1, cfg[k])) - math.log2(max(1, target[k]))) for k in target) + 1.0
+
+    best, t, trials = autotune.coordinate_descent(measure)
+    assert best == target and t == 1.0 and len(trials) == len(calls)
+    scene, sphere, index = scenes.open_box_library(level=1)
+    jobs, _ = scenes.batch_jobs(index, sphere, n_jobs=4)
+    k1 = autotune.scene_key(scene, jobs)
+    assert k1 == autotune.scene_key(scene, jobs) and k1.startswith("tris2^")
+    small = autotune.scaled_jobs(jobs, 1000)
+    assert all(j.spp >= 1 for j in small) and sum(j.width * j.height * j.spp for j in small) < \
+        sum(j.width * j.height * j.spp for j in jobs)
