@@ -417,8 +417,10 @@ int lrt_render_stats_reset(lrt_context* ctx);
  * "photon_tree_device" (0/1), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
  * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
- * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major).
- * The last four change speed only, never an image. */
+ * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major),
+ * "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
+ * boxes; 0: the object list in order, as hittable_list::hit does). The last five change speed only,
+ * never an image or a hit. */
 int lrt_set_option(lrt_context* ctx, const char* name, int64_t value);
 
 /* photons: particles [0, ...) traced in index order until `requested` photons are stored */

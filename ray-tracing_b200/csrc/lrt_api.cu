@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(WaveArgs a, int de
     const uint32_t n0 = bc.active[0];
     const uint32_t n = n0 + bc.active[1];
     TravItem stack[kStackSize];
+    int32_t tl_stack[kTlasStack];
     TravState st;
     TraceCount cnt{0, 0};
     uint32_t rays = 0;
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(WaveArgs a, int de
             }
         }
         if(!__any_sync(0xffffffffu, active)) break;
-        if(active && trav_step<kCount>(a.s, st, stack, cnt)) {
+        if(active && trav_step<kCount>(a.s, st, stack, tl_stack, cnt)) {
             a.hit_p[pid] = make_float4(st.closest_so_far, st.best_mesh.u, st.best_mesh.v, __int_as_float(st.best));
             a.hit_n[pid] = make_float4(__uint_as_float(st.best_mesh.ref), 0.0f, 0.0f, 0.0f);
             active = false;
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int de
     const uint32_t n0 = bc.shadow[0];
     const uint32_t n = n0 + bc.shadow[1];
     TravItem stack[kStackSize];
+    int32_t tl_stack[kTlasStack];
     TravState st;
     TraceCount cnt{0, 0};
     uint32_t rays = 0;
@@ -428,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int de
             }
         }
         if(!__any_sync(0xffffffffu, active)) break;
-        if(active && trav_step<kCount>(a.s, st, stack, cnt)) {
+        if(active && trav_step<kCount>(a.s, st, stack, tl_stack, cnt)) {
             const bool blocked = st.any_mode ? st.best >= 0 : (st.best >= 0 && a.s.objects[st.best].emitter != light);
             if(kVis) a.adj_sh_vis[k] = blocked ? 0 : 1;
             if(!blocked) {
@@ -1343,6 +1345,8 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
         memcpy(&emission[h.emission_cdf.size() + i], &h.emission_index[i], 4);
     }
     LRT_CUDA(ctx, upload(ctx->emission, emission, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->tlas, h.tlas, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->tlas_objs, h.tlas_objs, s, bytes));
     LRT_CUDA(ctx, cudaStreamSynchronize(s));
     DeviceScene& ds = ctx->ds;
     ds.nodes = ctx->nodes.as<uint2>();
@@ -1365,6 +1369,9 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     ds.n_heavy = h.n_heavy;
     for(int i = 0; i < 4; ++i) ds.heavy[i] = h.heavy[i];
     ds.cam = h.cam;
+    ds.tlas = ctx->tlas.as<float4>();
+    ds.tlas_objs = ctx->tlas_objs.as<int32_t>();
+    ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(h.tlas.size() / 2) : 0;
     ctx->scene_bytes = bytes;
     ctx->has_scene = true;
     return LRT_OK;
@@ -1585,6 +1592,9 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->batch_graph = value != 0;
     } else if(strcmp(name, "adjoint_megakernel") == 0) {
         ctx->adjoint_megakernel = value != 0;
+    } else if(strcmp(name, "object_bvh") == 0) {
+        ctx->object_bvh = value != 0;
+        if(ctx->has_scene) ctx->ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(ctx->host.tlas.size() / 2) : 0;
     } else if(strcmp(name, "blocks_per_sm") == 0) {
         if(value < 0 || value > 32) return fail(ctx, LRT_ERR_RANGE, "blocks_per_sm must be in [0, 32]");
         ctx->blocks_per_sm_cap = static_cast<uint32_t>(value);

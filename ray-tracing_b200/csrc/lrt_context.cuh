@@ -92,7 +92,8 @@ struct lrt_context {
     bool has_scene = false;
     lrt::HostScene host;
     lrt::DeviceScene ds{};
-    lrt::DevBuf nodes, tris, ref_prim, normals, objects, materials, tables, emitters, emission, sobol;
+    lrt::DevBuf nodes, tris, ref_prim, normals, objects, materials, tables, emitters, emission, sobol, tlas, tlas_objs;
+    bool object_bvh = true;  // false: walk the object list in order even where a hierarchy was built
     uint64_t scene_bytes = 0;
     // render
     lrt::WaveState wave;

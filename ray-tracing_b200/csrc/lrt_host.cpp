@@ -7,9 +7,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <fstream>
 #include <limits>
+#include <thread>
 #include <utility>
 
 #include "lrt_math.cuh"
@@ -529,6 +531,57 @@ bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1])
 
 // ------------------------------------------------------------------------------------------------
 
+namespace {
+
+// Median-split hierarchy over object boxes: leaves of at most 4 objects, children ordered as built.
+// The traversal visits every object whose box it may reach and resolves ties by object index, so the
+// closest hit does not depend on this tree's shape.
+struct TlasBuilder {
+    const std::vector<Box>& boxes;
+    std::vector<int32_t> idx;
+    std::vector<float4>& nodes;
+    std::vector<int32_t>& objs;
+
+    static float bits(int32_t v) {
+        float f;
+        memcpy(&f, &v, 4);
+        return f;
+    }
+
+    int32_t build(int32_t lo, int32_t hi, int depth) {
+        const int32_t node = static_cast<int32_t>(nodes.size() / 2);
+        nodes.push_back(float4{});
+        nodes.push_back(float4{});
+        Box bounds, centroids;
+        for(int32_t i = lo; i < hi; ++i) {
+            bounds.extend(boxes[idx[i]]);
+            centroids.extend((boxes[idx[i]].lo + boxes[idx[i]].hi) * 0.5f);
+        }
+        const int32_t count = hi - lo;
+        if(count <= 4 || depth >= kTlasStack - 2) {
+            const int32_t first = static_cast<int32_t>(objs.size());
+            objs.insert(objs.end(), idx.begin() + lo, idx.begin() + hi);
+            nodes[2 * node] = float4{bounds.lo.x, bounds.lo.y, bounds.lo.z, bits(first)};
+            nodes[2 * node + 1] = float4{bounds.hi.x, bounds.hi.y, bounds.hi.z, bits(-count)};
+            return node;
+        }
+        const f3 ext = centroids.hi - centroids.lo;
+        const int axis = ext.x >= ext.y && ext.x >= ext.z ? 0 : (ext.y >= ext.z ? 1 : 2);
+        const int32_t mid = lo + count / 2;
+        std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int32_t a, int32_t b) {
+            const float ca = comp(boxes[a].lo + boxes[a].hi, axis), cb = comp(boxes[b].lo + boxes[b].hi, axis);
+            return ca < cb || (ca == cb && a < b);
+        });
+        const int32_t left = build(lo, mid, depth + 1);
+        const int32_t right = build(mid, hi, depth + 1);
+        nodes[2 * node] = float4{bounds.lo.x, bounds.lo.y, bounds.lo.z, bits(left)};
+        nodes[2 * node + 1] = float4{bounds.hi.x, bounds.hi.y, bounds.hi.z, bits(right)};
+        return node;
+    }
+};
+
+}  // namespace
+
 void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out) {
     out = PackedTree{};
     if(count == 0) {
@@ -809,6 +862,46 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
     }
 
     // ---- objects ----
+    // the meshes' kd-trees are independent: validate every mesh, then build the trees on all host cores
+    std::vector<PackedTree> trees(d->n_objects);
+    {
+        std::vector<uint32_t> meshes;
+        for(uint32_t i = 0; i < d->n_objects; ++i) {
+            const lrt_object_desc& o = d->objects[i];
+            if(o.kind != LRT_OBJECT_MESH) continue;
+            if(o.n_indices % 3 != 0 || (o.n_indices && (!o.indices || !o.positions || !o.corner_normals))) {
+                err = "object " + std::to_string(i) + ": malformed mesh";
+                return LRT_ERR_INVALID_ARGUMENT;
+            }
+            for(uint32_t k = 0; k < o.n_indices; ++k) {
+                if(o.indices[k] >= o.n_vertices) {
+                    err = "object " + std::to_string(i) + ": vertex index out of range";
+                    return LRT_ERR_INVALID_ARGUMENT;
+                }
+            }
+            meshes.push_back(i);
+        }
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for(size_t m = next++; m < meshes.size(); m = next++) {
+                const lrt_object_desc& o = d->objects[meshes[m]];
+                const uint32_t n_tris = o.n_indices / 3;
+                std::vector<float> bmin(3ull * n_tris), bmax(3ull * n_tris);
+                for(uint32_t t = 0; t < n_tris; ++t) {
+                    Box b;
+                    for(int c = 0; c < 3; ++c) b.extend(load3(o.positions + 3ull * o.indices[3 * t + c]));
+                    store3(&bmin[3ull * t], b.lo);
+                    store3(&bmax[3ull * t], b.hi);
+                }
+                build_kdtree(bmin.data(), bmax.data(), n_tris, trees[meshes[m]]);
+            }
+        };
+        const size_t n_threads = std::min<size_t>(meshes.size(), std::max(1u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for(size_t t = 1; t < n_threads; ++t) pool.emplace_back(worker);
+        worker();
+        for(std::thread& t : pool) t.join();
+    }
     Box scene_box;
     for(uint32_t i = 0; i < d->n_objects; ++i) {
         const lrt_object_desc& o = d->objects[i];
@@ -822,26 +915,8 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
         }
         MeshTreeInfo info{0, 0, 0};
         if(o.kind == LRT_OBJECT_MESH) {
-            if(o.n_indices % 3 != 0 || (o.n_indices && (!o.indices || !o.positions || !o.corner_normals))) {
-                err = "object " + std::to_string(i) + ": malformed mesh";
-                return LRT_ERR_INVALID_ARGUMENT;
-            }
             const uint32_t n_tris = o.n_indices / 3;
-            for(uint32_t k = 0; k < o.n_indices; ++k) {
-                if(o.indices[k] >= o.n_vertices) {
-                    err = "object " + std::to_string(i) + ": vertex index out of range";
-                    return LRT_ERR_INVALID_ARGUMENT;
-                }
-            }
-            std::vector<float> bmin(3ull * n_tris), bmax(3ull * n_tris);
-            for(uint32_t t = 0; t < n_tris; ++t) {
-                Box b;
-                for(int c = 0; c < 3; ++c) b.extend(load3(o.positions + 3ull * o.indices[3 * t + c]));
-                store3(&bmin[3ull * t], b.lo);
-                store3(&bmax[3ull * t], b.hi);
-            }
-            PackedTree tree;
-            build_kdtree(bmin.data(), bmax.data(), n_tris, tree);
+            const PackedTree& tree = trees[i];
             r.node_base = static_cast<uint32_t>(s.nodes.size());
             r.ref_base = static_cast<uint32_t>(s.ref_prim.size());
             r.tri_base = static_cast<uint32_t>(s.normals.size() / 3);
@@ -918,6 +993,32 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
     {
         const f3 half = (scene_box.hi - scene_box.lo) * 0.5f;
         s.bounding_radius = length(half);
+    }
+    if(s.objects.size() > kTlasMinObjects) {
+        std::vector<Box> boxes(s.objects.size());
+        for(size_t i = 0; i < s.objects.size(); ++i) {
+            const ObjRec& r = s.objects[i];
+            Box b;
+            if(r.kind == LRT_OBJECT_MESH) {
+                b.extend(load3(r.bmin));
+                b.extend(load3(r.bmax));
+            } else if(r.kind == LRT_OBJECT_RECTANGLE) {
+                const f3 c = load3(r.corner), u = load3(r.edge_u), v = load3(r.edge_v);
+                b.extend(c);
+                b.extend(c + u);
+                b.extend(c + v);
+                b.extend(c + u + v);
+            } else {
+                b.extend(load3(r.center) - mk(r.radius));
+                b.extend(load3(r.center) + mk(r.radius));
+            }
+            if(!(b.lo.x <= b.hi.x)) b = Box{f3{0, 0, 0}, f3{0, 0, 0}};  // an empty mesh: a point box
+            boxes[i] = b;
+        }
+        TlasBuilder tb{boxes, {}, s.tlas, s.tlas_objs};
+        tb.idx.resize(s.objects.size());
+        for(size_t i = 0; i < s.objects.size(); ++i) tb.idx[i] = static_cast<int32_t>(i);
+        tb.build(0, static_cast<int32_t>(s.objects.size()), 0);
     }
     {
         std::vector<std::pair<uint32_t, int32_t>> heavy;

@@ -39,7 +39,11 @@ struct HostScene {
     // meshes of more than 64 triangles, largest first; queue segmentation is off when there are > 4
     int32_t n_heavy = 0;
     int32_t heavy[4] = {-1, -1, -1, -1};
+    // object hierarchy (empty when the list is short): nodes as the device reads them, leaf objects
+    std::vector<float4> tlas;
+    std::vector<int32_t> tlas_objs;
 };
+
 
 // Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message.
 int build_host_scene(const lrt_scene_desc* desc, HostScene& out, std::string& error);

@@ -76,14 +76,15 @@ struct MeshHit {
     uint32_t ref;  // leaf reference of the last accepted triangle
 };
 
-// Conservative object cull: false only when the ray's [t_min, t_max] interval cannot reach the mesh's
-// bounding box grown by 1e-3 (+ 1e-4 relative), so no triangle of the mesh can be accepted and its
-// traversal would test nothing that hits. Directions with a zero component are handled per slab.
-__device__ __forceinline__ bool ray_may_hit_box(const ObjRec& o, const Ray& r, float t_min, float t_max) {
+// Conservative box cull: false only when the ray's [t_min, t_max] interval cannot reach the box
+// [lo, hi] grown by 1e-3 (+ 1e-4 relative), so nothing inside it can be accepted. Directions with a zero
+// component are handled per slab. t_entry: where the interval enters the grown box.
+__device__ __forceinline__ bool box_reach(const float* lo_v, const float* hi_v, const Ray& r, float t_min, float t_max,
+                                          float& t_entry) {
     float tn = t_min, tf = t_max;
 #pragma unroll
     for(int a = 0; a < 3; ++a) {
-        const float lo = o.bmin[a], hi = o.bmax[a];
+        const float lo = lo_v[a], hi = hi_v[a];
         const float pad = 1e-3f + 1e-4f * (fabsf(lo) + fabsf(hi));
         const float oa = comp(r.o, a), da = comp(r.d, a);
         if(da == 0.0f) {
@@ -101,7 +102,64 @@ __device__ __forceinline__ bool ray_may_hit_box(const ObjRec& o, const Ray& r, f
         tn = fmaxf(tn, t0 - 1e-4f * fabsf(t0));
         tf = fminf(tf, t1 + 1e-4f * fabsf(t1));
     }
+    t_entry = tn;
     return !(tn > tf);
+}
+
+// the object cull: a mesh none of whose triangles the ray's interval can reach is skipped
+__device__ __forceinline__ bool ray_may_hit_box(const ObjRec& o, const Ray& r, float t_min, float t_max) {
+    float t_entry;
+    return box_reach(o.bmin, o.bmax, r, t_min, t_max, t_entry);
+}
+
+// Object-list walk: f(object) for every object the ray may reach, in list order, or -- when the scene
+// has an object hierarchy -- in front-to-back node order, pruned by limit() (the current closest hit,
+// read at every node). f returns true to stop (any-hit queries). The closest-hit callers resolve equal
+// t by object index, the list's "later object wins", so both orders give the same hit.
+template <typename Limit, typename F>
+__device__ __forceinline__ void for_each_object(const DeviceScene& s, const Ray& r, float t_min, Limit limit, F f) {
+    if(s.n_tlas == 0) {
+        for(int32_t i = 0; i < s.n_objects; ++i) {
+            if(f(i)) return;
+        }
+        return;
+    }
+    int32_t stack[kTlasStack];
+    int top = 0;
+    stack[top++] = 0;
+    while(top > 0) {
+        const int32_t node = stack[--top];
+        const float4 a = __ldg(s.tlas + 2 * node), b = __ldg(s.tlas + 2 * node + 1);
+        const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+        float t_entry;
+        if(!box_reach(lo, hi, r, t_min, limit(), t_entry)) continue;
+        const int32_t right = __float_as_int(b.w);
+        if(right < 0) {
+            const int32_t first = __float_as_int(a.w);
+            for(int32_t k = first; k < first - right; ++k) {
+                if(f(__ldg(s.tlas_objs + k))) return;
+            }
+            continue;
+        }
+        const int32_t left = __float_as_int(a.w);
+        // nearer child on top
+        const float4 la = __ldg(s.tlas + 2 * left), ra = __ldg(s.tlas + 2 * right);
+        const float4 lb = __ldg(s.tlas + 2 * left + 1), rb = __ldg(s.tlas + 2 * right + 1);
+        const float llo[3] = {la.x, la.y, la.z}, lhi[3] = {lb.x, lb.y, lb.z};
+        const float rlo[3] = {ra.x, ra.y, ra.z}, rhi[3] = {rb.x, rb.y, rb.z};
+        float tl = kInf, tr = kInf;
+        const bool hl = box_reach(llo, lhi, r, t_min, limit(), tl);
+        const bool hr = box_reach(rlo, rhi, r, t_min, limit(), tr);
+        if(top + 2 > kTlasStack) continue;  // unreachable: the build caps the depth below the stack size
+        if(hl && hr) {
+            stack[top++] = tl <= tr ? right : left;
+            stack[top++] = tl <= tr ? left : right;
+        } else if(hl) {
+            stack[top++] = left;
+        } else if(hr) {
+            stack[top++] = right;
+        }
+    }
 }
 
 // Queue segment of a ray: 1 when it may reach the box of one of the scene's heavy meshes (the ones whose
@@ -246,12 +304,14 @@ __device__ __forceinline__ bool scene_hit(const DeviceScene& s, const Ray& r, fl
     float closest_so_far = t_max;
     int32_t best = -1;
     MeshHit best_mesh{};
-    for(int32_t i = 0; i < s.n_objects; ++i) {
+    // hittable_list::hit: an object replaces the best on a nearer hit, or an equal one later in the list
+    for_each_object(s, r, t_min, [&]() { return closest_so_far; }, [&](int32_t i) {
         const ObjRec& o = s.objects[i];
         if(o.kind == LRT_OBJECT_MESH) {
             MeshHit mh;
             if(ray_may_hit_box(o, r, t_min, closest_so_far) &&
-               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt) &&
+               (mh.t < closest_so_far || i > best)) {
                 closest_so_far = mh.t;
                 best = i;
                 best_mesh = mh;
@@ -259,18 +319,19 @@ __device__ __forceinline__ bool scene_hit(const DeviceScene& s, const Ray& r, fl
         } else if(o.kind == LRT_OBJECT_RECTANGLE) {
             float t;
             f3 p;
-            if(hit_rectangle(o, r, t_min, closest_so_far, t, p)) {
+            if(hit_rectangle(o, r, t_min, closest_so_far, t, p) && (t < closest_so_far || i > best)) {
                 closest_so_far = t;
                 best = i;
             }
         } else {
             float t;
-            if(hit_sphere(o, r, t_min, closest_so_far, t)) {
+            if(hit_sphere(o, r, t_min, closest_so_far, t) && (t < closest_so_far || i > best)) {
                 closest_so_far = t;
                 best = i;
             }
         }
-    }
+        return false;
+    });
     out.object = best;
     out.prim = -1;
     if(best < 0) return false;
@@ -321,30 +382,32 @@ __device__ __forceinline__ int32_t scene_hit_emitter(const DeviceScene& s, const
                                                      TraceCount& cnt) {
     float closest_so_far = t_max;
     int32_t best = -1;
-    for(int32_t i = 0; i < s.n_objects; ++i) {
+    for_each_object(s, r, t_min, [&]() { return closest_so_far; }, [&](int32_t i) {
         const ObjRec& o = s.objects[i];
         if(o.kind == LRT_OBJECT_MESH) {
             MeshHit mh;
             if(ray_may_hit_box(o, r, t_min, closest_so_far) &&
-               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt)) {
+               trace_mesh<kCount, false>(s, o, r, t_min, closest_so_far, mh, cnt) &&
+               (mh.t < closest_so_far || i > best)) {
                 closest_so_far = mh.t;
                 best = i;
             }
         } else if(o.kind == LRT_OBJECT_RECTANGLE) {
             float t;
             f3 p;
-            if(hit_rectangle(o, r, t_min, closest_so_far, t, p)) {
+            if(hit_rectangle(o, r, t_min, closest_so_far, t, p) && (t < closest_so_far || i > best)) {
                 closest_so_far = t;
                 best = i;
             }
         } else {
             float t;
-            if(hit_sphere(o, r, t_min, closest_so_far, t)) {
+            if(hit_sphere(o, r, t_min, closest_so_far, t) && (t < closest_so_far || i > best)) {
                 closest_so_far = t;
                 best = i;
             }
         }
-    }
+        return false;
+    });
     if(best < 0) return -2;
     return s.objects[best].emitter;
 }
@@ -369,21 +432,23 @@ __device__ __forceinline__ bool scene_occluded(const DeviceScene& s, const Ray& 
             return hit != -2 && hit != light;
         }
     }
-    for(int32_t i = 0; i < s.n_objects; ++i) {
+    bool blocked = false;
+    for_each_object(s, r, t_min, [&]() { return t_max; }, [&](int32_t i) {
         const ObjRec& o = s.objects[i];
         if(o.kind == LRT_OBJECT_MESH) {
             MeshHit mh;
-            if(ray_may_hit_box(o, r, t_min, t_max) && trace_mesh<kCount, true>(s, o, r, t_min, t_max, mh, cnt)) return true;
+            blocked = ray_may_hit_box(o, r, t_min, t_max) && trace_mesh<kCount, true>(s, o, r, t_min, t_max, mh, cnt);
         } else if(o.kind == LRT_OBJECT_RECTANGLE) {
             float t;
             f3 p;
-            if(hit_rectangle(o, r, t_min, t_max, t, p)) return true;
+            blocked = hit_rectangle(o, r, t_min, t_max, t, p);
         } else {
             float t;
-            if(hit_sphere(o, r, t_min, t_max, t)) return true;
+            blocked = hit_sphere(o, r, t_min, t_max, t);
         }
-    }
-    return false;
+        return blocked;
+    });
+    return blocked;
 }
 
 // ---- resumable traversal (persistent kernels) ----
@@ -402,7 +467,10 @@ struct TravState {
     Ray r;
     float t_min;
     float t_max;          // occlusion: the shadow ray's tmax; closest hit: +inf
-    int32_t obj;          // next (or current) object of the list
+    int32_t obj;          // the mesh being traversed
+    int32_t cursor;       // list walk: next object; hierarchy walk: next entry of the current leaf
+    int32_t leaf_end;
+    int32_t tl_top;       // hierarchy stack depth, -1 before the root is pushed
     bool in_mesh;
     bool any_mode;        // occlusion without a reachable light: stop at the first accepted hit
     uint32_t node;
@@ -421,7 +489,10 @@ __device__ __forceinline__ void trav_begin(TravState& st, const Ray& r, float t_
     st.r = r;
     st.t_min = t_min;
     st.t_max = t_max;
-    st.obj = 0;
+    st.obj = -1;
+    st.cursor = 0;
+    st.leaf_end = 0;
+    st.tl_top = -1;
     st.in_mesh = false;
     st.any_mode = any_mode;
     st.closest_so_far = t_max;
@@ -432,15 +503,61 @@ __device__ __forceinline__ void trav_begin(TravState& st, const Ray& r, float t_
     st.inv_z = 1.0f / r.d.z;
 }
 
+// The next object of the walk that the ray may reach (-1: none left): the list in order, or the
+// hierarchy's leaves front to back, pruned by the closest hit so far.
+__device__ __forceinline__ int32_t trav_next_object(const DeviceScene& s, TravState& st, int32_t* tl_stack) {
+    if(s.n_tlas == 0) return st.cursor < s.n_objects ? st.cursor++ : -1;
+    while(true) {
+        if(st.cursor < st.leaf_end) return __ldg(s.tlas_objs + st.cursor++);
+        if(st.tl_top < 0) {
+            tl_stack[0] = 0;
+            st.tl_top = 1;
+        }
+        if(st.tl_top == 0) return -1;
+        const int32_t node = tl_stack[--st.tl_top];
+        const float4 a = __ldg(s.tlas + 2 * node), b = __ldg(s.tlas + 2 * node + 1);
+        const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+        float t_entry;
+        if(!box_reach(lo, hi, st.r, st.t_min, st.closest_so_far, t_entry)) continue;
+        const int32_t right = __float_as_int(b.w);
+        if(right < 0) {
+            st.cursor = __float_as_int(a.w);
+            st.leaf_end = st.cursor - right;
+            continue;
+        }
+        const int32_t left = __float_as_int(a.w);
+        const float4 la = __ldg(s.tlas + 2 * left), ra = __ldg(s.tlas + 2 * right);
+        const float4 lb = __ldg(s.tlas + 2 * left + 1), rb = __ldg(s.tlas + 2 * right + 1);
+        const float llo[3] = {la.x, la.y, la.z}, lhi[3] = {lb.x, lb.y, lb.z};
+        const float rlo[3] = {ra.x, ra.y, ra.z}, rhi[3] = {rb.x, rb.y, rb.z};
+        float tl = kInf, tr = kInf;
+        const bool hl = box_reach(llo, lhi, st.r, st.t_min, st.closest_so_far, tl);
+        const bool hr = box_reach(rlo, rhi, st.r, st.t_min, st.closest_so_far, tr);
+        if(st.tl_top + 2 > kTlasStack) continue;  // unreachable: the build caps the depth below the stack size
+        if(hl && hr) {
+            tl_stack[st.tl_top++] = tl <= tr ? right : left;
+            tl_stack[st.tl_top++] = tl <= tr ? left : right;
+        } else if(hl) {
+            tl_stack[st.tl_top++] = left;
+        } else if(hr) {
+            tl_stack[st.tl_top++] = right;
+        }
+    }
+}
+
 // One unit of work; returns true when the ray is finished (result in best / best_mesh / closest_so_far;
-// in any_mode best >= 0 means "hit").
+// in any_mode best >= 0 means "hit"). Equal t is resolved by object index, as the list's order does.
 template <bool kCount>
-__device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, TravItem* stack, TraceCount& cnt) {
+__device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, TravItem* stack, int32_t* tl_stack,
+                                          TraceCount& cnt) {
     if(!st.in_mesh) {
-        while(st.obj < s.n_objects) {
-            const ObjRec& o = s.objects[st.obj];
+        while(true) {
+            const int32_t i = trav_next_object(s, st, tl_stack);
+            if(i < 0) return true;
+            const ObjRec& o = s.objects[i];
             if(o.kind == LRT_OBJECT_MESH) {
                 if(ray_may_hit_box(o, st.r, st.t_min, st.closest_so_far)) {
+                    st.obj = i;
                     st.in_mesh = true;
                     st.node = 0;
                     st.mint = st.t_min;
@@ -453,22 +570,20 @@ __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, T
             } else if(o.kind == LRT_OBJECT_RECTANGLE) {
                 float t;
                 f3 p;
-                if(hit_rectangle(o, st.r, st.t_min, st.closest_so_far, t, p)) {
+                if(hit_rectangle(o, st.r, st.t_min, st.closest_so_far, t, p) && (t < st.closest_so_far || i > st.best)) {
                     st.closest_so_far = t;
-                    st.best = st.obj;
+                    st.best = i;
                     if(st.any_mode) return true;
                 }
             } else {
                 float t;
-                if(hit_sphere(o, st.r, st.t_min, st.closest_so_far, t)) {
+                if(hit_sphere(o, st.r, st.t_min, st.closest_so_far, t) && (t < st.closest_so_far || i > st.best)) {
                     st.closest_so_far = t;
-                    st.best = st.obj;
+                    st.best = i;
                     if(st.any_mode) return true;
                 }
             }
-            ++st.obj;
         }
-        return true;
     }
     const ObjRec& o = s.objects[st.obj];
     const uint2* nodes = s.nodes + o.node_base;
@@ -537,13 +652,12 @@ __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, T
         }
     }
     if(mesh_done) {
-        if(st.cur_hit) {
+        if(st.cur_hit && (st.cur.t < st.closest_so_far || st.obj > st.best)) {
             st.closest_so_far = st.cur.t;
             st.best = st.obj;
             st.best_mesh = st.cur;
         }
         st.in_mesh = false;
-        ++st.obj;
     }
     return false;
 }

@@ -10,6 +10,8 @@
 //   materials  MatRec [n_materials]
 //   tables     float  [100 * n_tables]   rough-transmittance 1-D tables
 //   emitters   EmitRec[n_emitters]
+//   tlas       float4 [2 * nodes]       bounding-volume hierarchy over the objects (scenes of > 16 objects)
+//   tlas_objs  int32  [n_objects]       object indices in leaf order
 #pragma once
 
 #include <stdint.h>
@@ -21,6 +23,10 @@ namespace lrt {
 //   interior: word0 = split (float bits), word1 = (right_child << 2) | axis; left child = this + 1
 //   leaf:     word0 = first reference,    word1 = (count << 2) | 3
 constexpr uint32_t kLeafTag = 3u;
+
+// object-list hierarchies are built above this many objects; their depth stays below the stack size
+constexpr uint32_t kTlasMinObjects = 16;
+constexpr int kTlasStack = 32;
 
 struct ObjRec {
     int32_t kind;        // LRT_OBJECT_*
@@ -122,6 +128,11 @@ struct DeviceScene {
     int32_t n_heavy;         // meshes large enough that rays reaching their box are queued apart
     int32_t heavy[4];
     CamRec cam;
+    // bounding-volume hierarchy over the object list (scenes with many objects); n_tlas = 0: the
+    // object list is walked in order
+    const float4* tlas;      // 2 per node: (bmin, first object | left child), (bmax, -count | right child)
+    const int32_t* tlas_objs;
+    int32_t n_tlas;
 };
 
 }  // namespace lrt

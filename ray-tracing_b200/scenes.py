@@ -19,6 +19,7 @@ reference computes them on the host at material/emitter construction). They are 
 from __future__ import annotations
 
 import base64
+import functools
 import json
 import math
 import os
@@ -197,6 +198,7 @@ def fbm(p: np.ndarray, seed: int, octaves: int = 3) -> np.ndarray:
     return total / norm
 
 
+@functools.lru_cache(maxsize=8)
 def icosphere(level: int):
     """Unit icosphere: 20 * 4**level triangles (float64 vertices, int64 faces)."""
     t = (1.0 + math.sqrt(5.0)) / 2.0
@@ -397,9 +399,60 @@ def job_desc(camera: dict, width: int, height: int, spp: int, sample_offset: int
                        override_material, output_offset)
 
 
+def large_scene(level: int = 5, grid=(8, 8, 4), seed: int = 20261206, spacing: float = 1.15, aspect: float = 1.0,
+                attach: bool = True) -> Scene:
+    """The large photon-mapping scene: an 8 x 8 x 4 grid of seeded displaced icospheres (level 5,
+    20,480 triangles each, radii uniform in [0.2, 0.5], each carrying one of the seven materials at
+    random) above a ground quad, lit by the Hosek sky and four quad lights facing down. Each sphere is
+    its own mesh object, as a reference scene built from triangle_mesh objects would hold them
+    (256 x 20,480 = 5,242,880 sphere triangles)."""
+    rng = np.random.default_rng(seed)
+    mats = [{"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.5, 0.5, 0.5)}]  # ground
+    index = {}
+    for name in MATERIAL_NAMES:
+        lib_mats, sphere = material_library(name)
+        offset = len(mats) - 3
+        for m in lib_mats[3:]:
+            m = dict(m)
+            if "nested" in m:
+                m["nested"] += offset
+            mats.append(m)
+        index[name] = sphere + offset
+    nx, nz, ny = grid
+    S = 0.5 * spacing * max(nx, nz) + 2.0
+    objects = [quad_mesh((-S, 0.0, S), (S, 0.0, S), (S, 0.0, -S), (-S, 0.0, -S), 0)]
+    for iy in range(ny):
+        for iz in range(nz):
+            for ix in range(nx):
+                center = ((ix - 0.5 * (nx - 1)) * spacing, 0.55 + iy * spacing, (iz - 0.5 * (nz - 1)) * spacing)
+                radius = float(rng.uniform(0.2, 0.5))
+                material = MATERIAL_NAMES[int(rng.integers(len(MATERIAL_NAMES)))]
+                sphere_seed = int(rng.integers(1 << 30))
+                pos, idx, nrm = displaced_icosphere(level, center, radius, 0.05, sphere_seed)
+                objects.append({"kind": abi.OBJ_MESH, "material": index[material], "positions": pos,
+                                "indices": idx, "corner_normals": nrm})
+    emitters = []
+    top = 0.55 + ny * spacing + 1.5
+    h = 0.75
+    for cx, cz in ((-2.5, -2.5), (2.5, -2.5), (-2.5, 2.5), (2.5, 2.5)):
+        objects.append({"kind": abi.OBJ_RECTANGLE, "material": -1, "corner": (cx - h, top, cz - h),
+                        "edge_u": (2 * h, 0.0, 0.0), "edge_v": (0.0, 0.0, 2 * h)})
+        emitters.append({"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (12.0, 11.0, 9.0)})
+    emitters.append(sky_emitter())
+    camera = {"origin": (10.0, 4.0, 12.0), "look_at": (0.0, 2.2, 0.0), "up": (0.0, 1.0, 0.0), "fov": 45.0,
+              "aspect": aspect}
+    scene = Scene(objects, mats, emitters, camera, name="large_grid_%dx%dx%d_level%d" % (nx, nz, ny, level))
+    if attach:
+        attach_tables(scene.materials)
+        attach_hosek(scene.emitters)
+    return scene
+
+
 # workloads -----------------------------------------------------------------------------------
 
 CONFIG0 = {"width": 256, "height": 256, "spp": 16, "max_depth": 6, "rr_depth": 3}
+CONFIG3 = {"width": 1024, "height": 1024, "spp": 32, "photons": 16_000_000, "photon_depth": 8, "k": 100,
+           "radius_cap": 0.05}
 CONFIG1 = {"width": 512, "height": 512, "spp": 64, "max_depth": 8, "rr_depth": 3,
            "photons": 1_000_000, "k": 64}
 
