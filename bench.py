@@ -532,6 +532,78 @@ def run_adjoint(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+# large photon-mapping scene: 256 displaced level-5 icospheres (5.24M triangles) on a ground quad, sky
+# + 4 quad lights; 16M photons (depth 8), k = 100, radius cap 0.05; 1024x1024 x 32 spp
+
+LARGE_METRIC = "Mpaths/s (photon mapper eye pass, 1024x1024 x 32 spp, 5.24M-triangle 256-sphere scene, 16M photons, k=100)"
+
+
+def run_large(args):
+    import torch
+    import lrt
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    c3 = scenes.CONFIG3
+    w, h, spp = c3["width"], c3["height"], args.large_spp or c3["spp"]
+    t0 = time.perf_counter()
+    scene = scenes.large_scene()
+    t_gen = time.perf_counter() - t0
+    ctx = lrt.Context(local, stream.cuda_stream)
+    t0 = time.perf_counter()
+    ctx.upload(scene)
+    t_upload = time.perf_counter() - t0
+    out = torch.zeros(w * h * 3, dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1000.0
+
+    clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+    clocks.start()
+    t0 = time.perf_counter()
+    pp, shots = ctx.photon_preprocess(c3["photons"], 0, max_depth=c3["photon_depth"], rr_depth=5,
+                                      radius_cap=c3["radius_cap"], lookup_size=c3["k"])
+    torch.cuda.synchronize(dev)
+    t_photons = time.perf_counter() - t0
+    pt_params = scenes.render_params(w, h, spp, 8, 3)
+    ctx.render_dev(scenes.render_params(w, h, 1, 8, 3), out.data_ptr())  # warm
+    t_pt = timed(lambda: ctx.render_dev(pt_params, out.data_ptr()))
+    ctx.reset_stats()
+    t_eye = timed(lambda: ctx.render_photon_dev(pt_params, pp, out.data_ptr()))
+    launches = int(ctx.stats()["kernel_launches"])
+    clock_info = clocks.stop()
+    img = out.view(h, w, 3).cpu().numpy()
+    paths = w * h * spp
+    line = {"metric": LARGE_METRIC, "value": paths / t_eye / 1e6, "unit": "Mpaths/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": 1000 * t_eye, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes.large_scene)",
+            "config": {"workload": "large_grid_8x8x4_level5_photon_1024x1024x%dspp" % spp,
+                       "triangles": scene.triangle_count(), "objects": len(scene.objects),
+                       "scene_gen_s": t_gen, "upload_s (kd-trees + object hierarchy + copy)": t_upload,
+                       "device_scene_mb": ctx.scene_bytes() / 1e6,
+                       "photons": c3["photons"], "photon_particles_shot": shots[0],
+                       "photon_preprocess_s (trace + map build)": t_photons, "k": c3["k"],
+                       "radius": pp.global_radius, "photon_depth": c3["photon_depth"],
+                       "path_tracer_mpaths_s (same scene, 1024x1024, depth 8)": paths / t_pt / 1e6,
+                       "image_mean": [float(x) for x in img.reshape(-1, 3).mean(axis=0)],
+                       "nonfinite": int((~np.isfinite(img)).sum())},
+            "clocks": clock_info, "gpu_launches": launches}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def abi_stage_names():
     import lrt_abi
     return lrt_abi.STAGE_NAMES
@@ -544,12 +616,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lrt", choices=["lrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="paths", choices=["paths", "batch", "adjoint"],
+    ap.add_argument("--workload", default="paths", choices=["paths", "batch", "adjoint", "large"],
                     help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison; "
                          "adjoint: gradient steps of the material optimisation")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: default launch shapes")
     ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--large-spp", type=int, default=0, help="large workload: spp (0: the configuration's 32)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -557,6 +630,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "large":
+        return run_large(args)
     return run_lrt(args)
 
 
