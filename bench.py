@@ -289,6 +289,21 @@ def run_lrt(args):
         traffic = tr["dram_bytes_per_extension_ray"] * work["extension_rays_per_path"] * timed_paths / extend_launches
     cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
 
+    # equal RMSE: the same samples give the reference's image, so the error against a converged render
+    # is the reference's (the cornell box fixture: 32x32, 64 spp vs the reference's 4096 spp)
+    rmse = None
+    gpath = os.path.join(ROOT, "tests", "golden", "image_kat.npz")
+    if rank == 0 and os.path.exists(gpath):
+        g = np.load(gpath)
+        c = lrt.Context(local, stream.cuda_stream)
+        c.upload(scenes.cornell_box())
+        img = c.render(scenes.render_params(32, 32, 64, 6, 3))
+        c.close()
+        ref4096 = g["cornell_4096"].astype(np.float64)
+        rmse = {"gpu_64spp": float(np.sqrt(np.mean((img - ref4096) ** 2))),
+                "reference_64spp": float(np.sqrt(np.mean((g["cornell_64"] - ref4096) ** 2))),
+                "against": "the reference renderer's 4096-spp cornell box (32x32, depth 6, tests/golden)"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -305,6 +320,7 @@ def run_lrt(args):
                          "algorithmic_bytes": "per extension ray 8*nodes + 48*triangles + 32 ray + 16 hit",
                          "avg_launch_ms": extend_ms / max(1, extend_launches)},
             "cpu_baseline": cpu,
+            "rmse": rmse,
             "clocks": clock_info,
             "gpu_launches": launches,
         }

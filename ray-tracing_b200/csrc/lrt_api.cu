@@ -1592,6 +1592,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->batch_graph = value != 0;
     } else if(strcmp(name, "adjoint_megakernel") == 0) {
         ctx->adjoint_megakernel = value != 0;
+    } else if(strcmp(name, "photon_eye_persistent") == 0) {
+        ctx->photon_eye_persistent = value != 0;
     } else if(strcmp(name, "object_bvh") == 0) {
         ctx->object_bvh = value != 0;
         if(ctx->has_scene) ctx->ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(ctx->host.tlas.size() / 2) : 0;

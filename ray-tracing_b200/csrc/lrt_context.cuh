@@ -118,6 +118,7 @@ struct lrt_context {
     std::vector<int> event_stage;
     // photons
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
+    bool photon_eye_persistent = true;  // false: one camera sample per thread, rays traced where issued
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
     lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye;
 };

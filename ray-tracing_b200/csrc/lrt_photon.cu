@@ -701,6 +701,311 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye(DeviceScene s, EyeParams 
     }
 }
 
+// ---- persistent eye pass ----
+//
+// The same depth-first walk as eye_sample, cut at every ray query so that the rays of a warp's lanes
+// are traced together: each lane runs its walk until it needs a ray (the first hit of a frame, an NEE
+// shadow ray, a BSDF sample's ray), then all lanes advance their traversals one unit at a time
+// (trav_step, the persistent traversal of the path tracer), and a lane whose ray is done resumes its
+// walk with the result; a lane whose camera sample is done takes the next one. Samples, sampler
+// draws, rays and additions to L are those of eye_sample, in the same order.
+enum EyeQuery : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, kQueryBsdf = 3 };
+
+struct EyeLane {
+    Sampler smp;
+    f3 L;
+    int top;
+    uint32_t slot;
+    uint8_t query;
+    f3 qa;           // shadow: what L gains when the light is visible; BSDF sample: its weight
+    float qpdf;      // BSDF sample: its pdf
+    int32_t qlight;  // shadow: the light
+};
+
+struct EyeFlags {
+    bool diffuse, specular, smooth, exhaustive;
+};
+
+__device__ __forceinline__ EyeFlags eye_flags(const DeviceScene& s, const EyeParams& ep, int32_t mid, int depth) {
+    const uint32_t flags = s.materials[mid].flags;
+    EyeFlags f;
+    f.diffuse = (flags & (kDiffuse | kGlossy | kSpecular)) == kDiffuse;
+    f.specular = (flags & kSpecular) != 0;
+    f.smooth = (flags & (kDiffuse | kGlossy)) != 0;
+    f.exhaustive = f.specular && depth < ep.max_specular_depth;
+    return f;
+}
+
+// Advances the lane's walk until it issues a ray query (true; ts holds the ray) or finishes its sample.
+__device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st, KnnHeap& heap,
+                            int* overflow, TravState& ts) {
+    const uint32_t(*table)[32] = sobol_table(s);
+    constexpr uint32_t kSmooth = kDiffuse | kGlossy;
+    while(ln.top >= 0) {
+        EyeFrame& F = st[ln.top];
+        if(F.stage == kEyeStart) {
+            if(!F.evaluated) {
+                ln.query = kQueryHit;
+                trav_begin(ts, Ray{F.ro, F.rd}, 0.001f, kInf, false);
+                return true;
+            }
+            if(F.obj < 0) {
+                if(F.emission) ln.L += F.tp * eval_environment(s, F.rd);
+                --ln.top;
+                continue;
+            }
+            const ObjRec& o = s.objects[F.obj];
+            if(F.emission && o.emitter >= 0 && F.front_face) {
+                ln.L += F.tp * area_emitted(s.emitters[o.emitter], F.n, -normalize(F.rd));
+            }
+            const int32_t m = o.material;
+            if(F.depth >= ep.max_depth || m < 0) {
+                --ln.top;
+                continue;
+            }
+            const uint32_t flags = s.materials[m].flags;
+            const bool diffuse = (flags & (kDiffuse | kGlossy | kSpecular)) == kDiffuse;
+            if(diffuse && dot(F.n, F.rd) < 0.0f) {  // photon lookups (photon_integrator.h:95-106)
+                const int photon_depth = ep.max_depth - F.depth;
+                const f3 reflectance = bsdf_diffuse_reflectance(s.materials, m) * (1.0f / kPi);
+                if(ep.global.n > 0) {
+                    ln.L += F.tp * (estimate_irradiance(ep.global, F.p, F.n, ep.global_radius, photon_depth, ep.lookup_size,
+                                                        heap) * reflectance);
+                }
+                if(ep.caustic.n > 0) {
+                    ln.L += F.tp * (estimate_irradiance(ep.caustic, F.p, F.n, ep.caustic_radius, photon_depth,
+                                                        ep.lookup_size, heap) * reflectance);
+                }
+            }
+            F.stage = kEyeSpecular;
+            F.iter = 0;
+            continue;
+        }
+        const int32_t mid = s.objects[F.obj].material;
+        const EyeFlags fl = eye_flags(s, ep, mid, F.depth);
+        const Onb basis = onb_from_normal(F.n);
+        BRec rec{};
+        rec.wi = to_local(basis, -normalize(F.rd));
+        rec.wo = mk(0.0f);
+        rec.front_face = F.front_face != 0;
+        rec.eta = 1.0f;
+        if(F.stage == kEyeSpecular) {  // specular_lobes (photon_integrator.h:126-155)
+            bool pushed = false;
+            if(fl.exhaustive) {
+                const int count = s.materials[mid].component_count;
+                while(F.iter < count) {
+                    const int c = F.iter++;
+                    if((bsdf_component_flags(s.materials, mid, c) & kSpecular) == 0) continue;
+                    BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                    ctx.component = c;
+                    BRec r = rec;
+                    const f3 w = bsdf_sample(s.materials, s.tables, mid, ctx, r, 0.5f, 0.5f);
+                    if(is_zero(w)) continue;
+                    if(ln.top + 1 >= kEyeFrames) {
+                        *overflow = 1;
+                        continue;
+                    }
+                    st[ln.top + 1] = EyeFrame{F.p, to_world(basis, r.wo), mk(0.0f), mk(0.0f), F.tp * w, -1,
+                                              static_cast<int16_t>(F.depth + 1), 0, kEyeStart, 0, 1, 0};
+                    ++ln.top;
+                    pushed = true;
+                    break;
+                }
+            }
+            if(pushed) continue;
+            F.stage = kEyeEmitters;
+            F.iter = 0;
+        }
+        if(F.stage == kEyeEmitters) {  // emitter_samples (photon_integrator.h:157-217), one shadow ray per visit
+            if(fl.smooth) {
+                const EyeCounts counts = eye_counts(ep, F.depth, fl.diffuse);
+                while(F.iter < counts.emitter) {
+                    ++F.iter;
+                    const F2 u = sampler_next_2d(table, ln.smp);
+                    DirectSample light{};
+                    light.distance = kInf;
+                    if(!sample_emitter_direction(s, F.p, u.x, u.y, light)) continue;
+                    const f3 shadow_origin = F.p + F.n * 1e-4f;
+                    f3 shadow_dir = light.direction;
+                    float tmax = kInf;
+                    if(!isinf(light.distance)) {
+                        const f3 to_light = light.point - shadow_origin;
+                        const float distance = length(to_light);
+                        if(distance < 1e-6f) continue;
+                        shadow_dir = to_light / distance;
+                        tmax = distance * (1.0f - 1e-4f);
+                    }
+                    BRec r = rec;
+                    r.wo = to_local(basis, shadow_dir);
+                    BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                    if(!fl.specular || fl.exhaustive) ctx.type_mask = kSmooth;
+                    const f3 value = bsdf_eval(s.materials, s.tables, mid, ctx, r, kSolidAngle);
+                    if(is_zero(value)) continue;
+                    // the pdfs do not depend on the shadow ray's outcome; a sample they reject adds nothing
+                    const float light_pdf = pdf_emitter_direction(s, F.p, shadow_dir);
+                    const float bsdf_pdf_v = bsdf_pdf(s.materials, s.tables, mid, ctx, r, kSolidAngle);
+                    if(light_pdf <= 0.0f) continue;
+                    const float weight = power_heuristic(light_pdf * static_cast<float>(counts.emitter),
+                                                         bsdf_pdf_v * static_cast<float>(counts.bsdf)) * counts.emitter_weight;
+                    ln.qa = F.tp * (value * light.radiance * (weight / light_pdf));
+                    ln.qlight = light.emitter;
+                    ln.query = kQueryShadow;
+                    const Ray sr{shadow_origin, shadow_dir};
+                    bool any_mode = true;
+                    const EmitRec& e = s.emitters[light.emitter];
+                    if(e.kind == LRT_EMITTER_AREA) {  // scene_occluded's rule
+                        const ObjRec& lo = s.objects[e.object];
+                        float t;
+                        f3 pp;
+                        any_mode = !(lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, sr, 0.001f, tmax, t, pp)
+                                                                    : hit_sphere(lo, sr, 0.001f, tmax, t));
+                    }
+                    trav_begin(ts, sr, 0.001f, tmax, any_mode);
+                    return true;
+                }
+            }
+            F.stage = kEyeBsdf;
+            F.iter = 0;
+        }
+        // bsdf_samples (photon_integrator.h:219-277), one ray per visit
+        const bool sample_direct = fl.smooth || (fl.specular && !fl.exhaustive);
+        const bool sample_indirect = !fl.diffuse && (fl.smooth || (fl.specular && !fl.exhaustive));
+        if(sample_direct || sample_indirect) {
+            const EyeCounts counts = eye_counts(ep, F.depth, fl.diffuse);
+            while(F.iter < counts.bsdf) {
+                ++F.iter;
+                BsdfCtx ctx = ctx_default(LRT_MODE_RADIANCE);
+                ctx.lobe_sample = sampler_next_1d(table, ln.smp);
+                if(!fl.specular || fl.exhaustive) ctx.type_mask = kSmooth;
+                BRec r = rec;
+                const F2 u = sampler_next_2d(table, ln.smp);
+                const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, r, u.x, u.y);
+                if(is_zero(weight) || r.pdf <= 0.0f) continue;
+                ln.qa = weight;
+                ln.qpdf = r.pdf;
+                ln.query = kQueryBsdf;
+                trav_begin(ts, Ray{F.p, to_world(basis, r.wo)}, 0.001f, kInf, false);
+                return true;
+            }
+        }
+        --ln.top;
+    }
+    return false;
+}
+
+// Hands a finished ray query's result to the lane's walk.
+__device__ void eye_resume(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st, int* overflow,
+                           const TravState& ts) {
+    EyeFrame& F = st[ln.top];
+    if(ln.query == kQueryHit) {
+        if(ts.best >= 0) {
+            HitInfo h;
+            hit_record_of(s, ts.r, ts.best, ts.closest_so_far, ts.best_mesh, h);
+            F.obj = h.object;
+            F.p = h.p;
+            F.n = h.normal;
+            F.front_face = h.front_face ? 1 : 0;
+        } else {
+            F.obj = -1;
+        }
+        F.evaluated = 1;
+    } else if(ln.query == kQueryShadow) {
+        const bool blocked = ts.any_mode ? ts.best >= 0 : (ts.best >= 0 && s.objects[ts.best].emitter != ln.qlight);
+        if(!blocked) ln.L += ln.qa;
+    } else if(ln.query == kQueryBsdf) {
+        const int32_t mid = s.objects[F.obj].material;
+        const EyeFlags fl = eye_flags(s, ep, mid, F.depth);
+        const EyeCounts counts = eye_counts(ep, F.depth, fl.diffuse);
+        const bool sample_direct = fl.smooth || (fl.specular && !fl.exhaustive);
+        const bool sample_indirect = !fl.diffuse && (fl.smooth || (fl.specular && !fl.exhaustive));
+        const bool hit = ts.best >= 0;
+        HitInfo occluder{};
+        if(hit) hit_record_of(s, ts.r, ts.best, ts.closest_so_far, ts.best_mesh, occluder);
+        const f3 weight = ln.qa;
+        if(sample_direct) {
+            f3 emission = mk(0.0f);
+            float light_pdf = 0.0f;
+            if(hit) {
+                const ObjRec& oo = s.objects[occluder.object];
+                if(oo.emitter >= 0 && occluder.front_face) {
+                    emission = area_emitted(s.emitters[oo.emitter], occluder.normal, -normalize(ts.r.d));
+                    light_pdf = pdf_emitter_direction(s, F.p, ts.r.d);
+                }
+            } else {
+                emission = eval_environment(s, ts.r.d);
+                light_pdf = pdf_emitter_direction(s, F.p, ts.r.d);
+            }
+            if(!is_zero(emission)) {
+                const float mis = power_heuristic(ln.qpdf * static_cast<float>(counts.bsdf),
+                                                  light_pdf * static_cast<float>(counts.emitter)) * counts.bsdf_weight;
+                ln.L += F.tp * (emission * weight * mis);
+            }
+        }
+        if(sample_indirect) {
+            if(ln.top + 1 >= kEyeFrames) {
+                *overflow = 1;
+            } else {
+                st[ln.top + 1] = EyeFrame{ts.r.o, ts.r.d, occluder.p, occluder.normal, F.tp * weight * counts.bsdf_weight,
+                                          hit ? occluder.object : -1, static_cast<int16_t>(F.depth + 1), 0, kEyeStart, 1,
+                                          0, static_cast<uint8_t>(hit && occluder.front_face ? 1 : 0)};
+                ++ln.top;
+            }
+        }
+    }
+    ln.query = kQueryNone;
+}
+
+__global__ void __launch_bounds__(kBlock) k_photon_eye_persistent(DeviceScene s, EyeParams ep, uint32_t width,
+                                                                  uint32_t height, uint32_t pixel_begin,
+                                                                  uint32_t n_pixels, uint32_t sample_begin,
+                                                                  uint32_t n_samples, float4* L_out, int* overflow,
+                                                                  uint32_t* fetch) {
+    EyeFrame frames[kEyeFrames];
+    KnnHeap heap;
+    TravItem stack[kStackSize];
+    int32_t tl_stack[kTlasStack];
+    TravState ts;
+    EyeLane ln;
+    TraceCount cnt{0, 0};
+    const uint32_t n = n_pixels * n_samples;
+    bool have = false, tracing = false, done = false;
+    while(true) {
+        while(!tracing && !done) {
+            if(!have) {
+                const uint32_t i = atomicAdd(fetch, 1u);
+                if(i >= n) {
+                    done = true;
+                    break;
+                }
+                const uint32_t pix = pixel_begin + i / n_samples;
+                const uint32_t sample = sample_begin + i % n_samples;
+                ln.smp = sampler_start(pix, sample);
+                const F2 off = sampler_next_2d(sobol_table(s), ln.smp);
+                const float u = (static_cast<float>(pix % width) + off.x) / static_cast<float>(width - 1);
+                const float v = (static_cast<float>(pix / width) + off.y) / static_cast<float>(height - 1);
+                const Ray camera = camera_ray(s.cam, u, v);
+                frames[0] = EyeFrame{camera.o, camera.d, mk(0.0f), mk(0.0f), mk(1.0f), -1, 1, 0, kEyeStart, 0, 1, 0};
+                ln.top = 0;
+                ln.L = mk(0.0f);
+                ln.slot = i;
+                ln.query = kQueryNone;
+                have = true;
+            }
+            if(eye_advance(s, ep, ln, frames, heap, overflow, ts)) {
+                tracing = true;
+            } else {
+                L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
+                have = false;
+            }
+        }
+        if(__all_sync(0xffffffffu, done)) break;
+        if(tracing && trav_step<false>(s, ts, stack, tl_stack, cnt)) {
+            tracing = false;
+            eye_resume(s, ep, ln, frames, overflow, ts);
+        }
+    }
+}
+
 __global__ void k_photon_eye_accumulate(const float4* L, uint32_t pixel_begin, uint32_t n_pixels, uint32_t n_samples,
                                         uint32_t spp, float* sum, int first, int last, float* rgb) {
     const uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1049,8 +1354,10 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     float4* L = ctx->ph_eye.as<float4>();
     float* sum = reinterpret_cast<float*>(L + cap);
     int* overflow = reinterpret_cast<int*>(sum + 3ull * cap);
+    uint32_t* fetch = reinterpret_cast<uint32_t*>(overflow + 4);
     LRT_CUDA(ctx, cudaMemsetAsync(overflow, 0, 4, ctx->stream));
-    const int grid = grid_for(ctx, (const void*)k_photon_eye, kBlock);
+    const bool persistent = ctx->photon_eye_persistent;
+    const int grid = grid_for(ctx, persistent ? (const void*)k_photon_eye_persistent : (const void*)k_photon_eye, kBlock);
     const uint32_t spp = p->spp;
     const uint32_t samples_per_wave = std::min(spp, cap);
     const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
@@ -1059,8 +1366,14 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
         const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
         for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
             const uint32_t ns = std::min(samples_per_wave, spp - sb);
-            k_photon_eye<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, ep, p->width, p->height, pb, np, p->sample_offset + sb,
-                                                           ns, L, overflow);
+            if(persistent) {
+                LRT_CUDA(ctx, cudaMemsetAsync(fetch, 0, 4, ctx->stream));
+                k_photon_eye_persistent<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, ep, p->width, p->height, pb, np,
+                                                                          p->sample_offset + sb, ns, L, overflow, fetch);
+            } else {
+                k_photon_eye<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, ep, p->width, p->height, pb, np,
+                                                               p->sample_offset + sb, ns, L, overflow);
+            }
             k_photon_eye_accumulate<<<blocks_for(np), kBlock, 0, ctx->stream>>>(L, pb, np, ns, spp, sum, sb == 0 ? 1 : 0,
                                                                                 sb + ns >= spp ? 1 : 0, rgb_dev);
             LRT_CUDA(ctx, cudaGetLastError());

@@ -104,6 +104,12 @@ def test_grid_scene_renders_identical_across_walks(ctx, grid_scene):
     pq = scenes.render_params(24, 20, 1, 8, 3)
     bvh, linear = both_walks(ctx, lambda: ctx.render_photon(pq, pp))
     assert np.array_equal(bvh, linear, equal_nan=True)
+    try:
+        ctx.set_option("photon_eye_persistent", 0)
+        per_thread = ctx.render_photon(pq, pp)
+    finally:
+        ctx.set_option("photon_eye_persistent", 1)
+    assert np.array_equal(bvh, per_thread, equal_nan=True)
 
 
 @needs_ref

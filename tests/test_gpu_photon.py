@@ -177,3 +177,22 @@ def test_empty_map(ctx):
     assert np.all(cnt == 0)
     out = ctx.photon_irradiance(2, np.zeros((3, 3), np.float32), np.ones((3, 3), np.float32), 0.1, 5, 8)
     assert np.all(out == 0)
+
+
+@pytest.mark.parametrize("material", ["coating", "rough_plastic", "rough_conductor"])
+def test_persistent_eye_pass_equals_per_thread(ctx, material):
+    """the persistent eye pass (rays of a warp traced together, lanes refilled as samples finish) makes
+    the walk, draws and additions of the one-sample-per-thread kernel: the images are identical"""
+    sc = scenes.cornell_box(material=material, level=4)
+    ctx.upload(sc)
+    pp, _ = ctx.photon_preprocess(20000, 20000, 128, 5, radius_cap=0.1, lookup_size=64)
+    params = scenes.render_params(20, 16, 3, 8, 3)
+    try:
+        ctx.set_option("photon_eye_persistent", 0)
+        per_thread = ctx.render_photon(params, pp)
+        ctx.set_option("photon_eye_persistent", 1)
+        persistent = ctx.render_photon(params, pp)
+    finally:
+        ctx.set_option("photon_eye_persistent", 1)
+    assert np.array_equal(per_thread, persistent, equal_nan=True)
+    assert persistent.mean() > 0
