@@ -419,10 +419,11 @@ int lrt_render_stats_reset(lrt_context* ctx);
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
  * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major),
  * "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
- * boxes; 0: the object list in order, as hittable_list::hit does), "photon_eye_persistent" (1: the
- * photon-mapper eye pass traces a warp's rays together through the persistent traversal; 0: one
- * camera sample per thread tracing each ray where it is issued). The last six change speed only,
- * never an image or a hit. */
+ * boxes; 0: the object list in order, as hittable_list::hit does), "photon_eye_kernel" (the
+ * photon-mapper eye pass: 2 wavefront -- samples in device-memory slots, their rays traced in queues
+ * by the persistent traversal; 1: persistent lanes tracing a warp's rays together; 0: one camera
+ * sample per thread tracing each ray where it is issued). The last six change speed only, never an
+ * image or a hit. */
 int lrt_set_option(lrt_context* ctx, const char* name, int64_t value);
 
 /* photons: particles [0, ...) traced in index order until `requested` photons are stored */

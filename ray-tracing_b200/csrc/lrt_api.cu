@@ -308,19 +308,6 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
 // its own finishes (ray replacement inside the traversal loop), so a warp's lanes stay busy while its
 // rays need very different numbers of nodes. The per-ray work is the state machine of trav_step.
 
-__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
-
-// fetch queue indices for the idle lanes of a warp: returns this lane's index (or >= n)
-__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter, bool idle, uint32_t n, bool& exhausted) {
-    const unsigned full = 0xffffffffu;
-    const unsigned want = __ballot_sync(full, idle);
-    uint32_t base = 0;
-    const int leader = __ffs(want) - 1;
-    if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(want)));
-    base = __shfl_sync(full, base, leader);
-    if(base + static_cast<uint32_t>(__popc(want)) >= n) exhausted = true;
-    return base + __popc(want & lanemask_lt());
-}
 
 // closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
 template <bool kCount>
@@ -1592,8 +1579,9 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->batch_graph = value != 0;
     } else if(strcmp(name, "adjoint_megakernel") == 0) {
         ctx->adjoint_megakernel = value != 0;
-    } else if(strcmp(name, "photon_eye_persistent") == 0) {
-        ctx->photon_eye_persistent = value != 0;
+    } else if(strcmp(name, "photon_eye_kernel") == 0) {
+        if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "photon_eye_kernel must be 0, 1 or 2");
+        ctx->photon_eye_kernel = static_cast<int>(value);
     } else if(strcmp(name, "object_bvh") == 0) {
         ctx->object_bvh = value != 0;
         if(ctx->has_scene) ctx->ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(ctx->host.tlas.size() / 2) : 0;

@@ -118,7 +118,8 @@ struct lrt_context {
     std::vector<int> event_stage;
     // photons
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
-    bool photon_eye_persistent = true;  // false: one camera sample per thread, rays traced where issued
+    int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
+    lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L;
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
     lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye;
 };
@@ -186,6 +187,20 @@ __device__ __forceinline__ uint32_t warp_append_keyed(uint32_t* counters, int ke
     if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counters + key, static_cast<uint32_t>(__popc(peers)));
     base = __shfl_sync(peers, base, leader);
     return base + __popc(peers & ((1u << lane_id()) - 1u));
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// fetch queue indices for the idle lanes of a warp (all 32 lanes call it): this lane's index, or >= n
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter, bool idle, uint32_t n, bool& exhausted) {
+    const unsigned full = 0xffffffffu;
+    const unsigned want = __ballot_sync(full, idle);
+    uint32_t base = 0;
+    const int leader = __ffs(want) - 1;
+    if(static_cast<int>(lane_id()) == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(want)));
+    base = __shfl_sync(full, base, leader);
+    if(base + static_cast<uint32_t>(__popc(want)) >= n) exhausted = true;
+    return base + __popc(want & lanemask_lt());
 }
 
 // warp reduce then one atomic per warp

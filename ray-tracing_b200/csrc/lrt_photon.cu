@@ -738,7 +738,7 @@ __device__ __forceinline__ EyeFlags eye_flags(const DeviceScene& s, const EyePar
 
 // Advances the lane's walk until it issues a ray query (true; ts holds the ray) or finishes its sample.
 __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st, KnnHeap& heap,
-                            int* overflow, TravState& ts) {
+                            int* overflow, TravState& ts, int frame_limit) {
     const uint32_t(*table)[32] = sobol_table(s);
     constexpr uint32_t kSmooth = kDiffuse | kGlossy;
     while(ln.top >= 0) {
@@ -801,7 +801,7 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
                     BRec r = rec;
                     const f3 w = bsdf_sample(s.materials, s.tables, mid, ctx, r, 0.5f, 0.5f);
                     if(is_zero(w)) continue;
-                    if(ln.top + 1 >= kEyeFrames) {
+                    if(ln.top + 1 >= frame_limit) {
                         *overflow = 1;
                         continue;
                     }
@@ -895,7 +895,7 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
 
 // Hands a finished ray query's result to the lane's walk.
 __device__ void eye_resume(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st, int* overflow,
-                           const TravState& ts) {
+                           const TravState& ts, int frame_limit) {
     EyeFrame& F = st[ln.top];
     if(ln.query == kQueryHit) {
         if(ts.best >= 0) {
@@ -942,7 +942,7 @@ __device__ void eye_resume(const DeviceScene& s, const EyeParams& ep, EyeLane& l
             }
         }
         if(sample_indirect) {
-            if(ln.top + 1 >= kEyeFrames) {
+            if(ln.top + 1 >= frame_limit) {
                 *overflow = 1;
             } else {
                 st[ln.top + 1] = EyeFrame{ts.r.o, ts.r.d, occluder.p, occluder.normal, F.tp * weight * counts.bsdf_weight,
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye_persistent(DeviceScene s,
                 ln.query = kQueryNone;
                 have = true;
             }
-            if(eye_advance(s, ep, ln, frames, heap, overflow, ts)) {
+            if(eye_advance(s, ep, ln, frames, heap, overflow, ts, kEyeFrames)) {
                 tracing = true;
             } else {
                 L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
@@ -1001,7 +1001,124 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye_persistent(DeviceScene s,
         if(__all_sync(0xffffffffu, done)) break;
         if(tracing && trav_step<false>(s, ts, stack, tl_stack, cnt)) {
             tracing = false;
-            eye_resume(s, ep, ln, frames, overflow, ts);
+            eye_resume(s, ep, ln, frames, overflow, ts, kEyeFrames);
+        }
+    }
+}
+
+// ---- wavefront eye pass ----
+//
+// Camera samples in flight live in slots in device memory: the walk's frames, the lane record, the
+// pending ray query and its result. Each iteration k_eye_shade resumes every slot whose ray was traced
+// and advances it to its next query (a finished sample writes its radiance and the slot starts the
+// next sample of the wave), queueing the slot; k_eye_trace then traces the queue with the persistent
+// traversal. Every sample's walk is the sequential program of eye_sample: the same draws, rays and
+// additions in the same order.
+enum EyeSlotState : uint32_t { kSlotIdle = 0, kSlotTracing = 1, kSlotDone = 2 };
+
+struct EyeSlot {
+    EyeLane ln;
+    float4 qo;  // query ray origin, t_min
+    float4 qd;  // query ray direction, t_max
+    int32_t any_mode;
+    int32_t best;
+    float closest;
+    uint32_t state;
+    MeshHit best_mesh;
+};
+
+struct EyeWave {
+    EyeSlot* slots;
+    EyeFrame* frames;      // frame_limit frames per slot
+    uint32_t* queue;       // slots with a ray to trace
+    uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch
+    float4* L_out;
+    int* overflow;
+    uint32_t n_slots;
+    uint32_t n_total;      // samples of the wave
+    int frame_limit;
+    uint32_t width, height, pixel_begin, n_samples, sample_begin;
+};
+
+__global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams ep, EyeWave w) {
+    KnnHeap heap;
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
+        EyeSlot& S = w.slots[slot];
+        if(S.state == kSlotDone) continue;
+        EyeFrame* st = w.frames + static_cast<size_t>(slot) * w.frame_limit;
+        EyeLane ln = S.ln;
+        bool have = false;
+        if(S.state == kSlotTracing) {
+            TravState ts;
+            ts.r = Ray{f3{S.qo.x, S.qo.y, S.qo.z}, f3{S.qd.x, S.qd.y, S.qd.z}};
+            ts.any_mode = S.any_mode != 0;
+            ts.best = S.best;
+            ts.closest_so_far = S.closest;
+            ts.best_mesh = S.best_mesh;
+            eye_resume(s, ep, ln, st, w.overflow, ts, w.frame_limit);
+            have = true;
+        }
+        uint32_t state = kSlotDone;
+        while(true) {
+            if(!have) {
+                const uint32_t i = atomicAdd(&w.counters[1], 1u);
+                if(i >= w.n_total) break;
+                const uint32_t pix = w.pixel_begin + i / w.n_samples;
+                const uint32_t sample = w.sample_begin + i % w.n_samples;
+                ln.smp = sampler_start(pix, sample);
+                const F2 off = sampler_next_2d(sobol_table(s), ln.smp);
+                const float u = (static_cast<float>(pix % w.width) + off.x) / static_cast<float>(w.width - 1);
+                const float v = (static_cast<float>(pix / w.width) + off.y) / static_cast<float>(w.height - 1);
+                const Ray camera = camera_ray(s.cam, u, v);
+                st[0] = EyeFrame{camera.o, camera.d, mk(0.0f), mk(0.0f), mk(1.0f), -1, 1, 0, kEyeStart, 0, 1, 0};
+                ln.top = 0;
+                ln.L = mk(0.0f);
+                ln.slot = i;
+                ln.query = kQueryNone;
+                have = true;
+            }
+            TravState ts;
+            if(eye_advance(s, ep, ln, st, heap, w.overflow, ts, w.frame_limit)) {
+                S.qo = make_float4(ts.r.o.x, ts.r.o.y, ts.r.o.z, ts.t_min);
+                S.qd = make_float4(ts.r.d.x, ts.r.d.y, ts.r.d.z, ts.t_max);
+                S.any_mode = ts.any_mode ? 1 : 0;
+                state = kSlotTracing;
+                w.queue[warp_append(&w.counters[0])] = slot;
+                break;
+            }
+            w.L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
+            have = false;
+        }
+        S.ln = ln;
+        S.state = state;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) {
+    const uint32_t n = w.counters[0];
+    TravItem stack[kStackSize];
+    int32_t tl_stack[kTlasStack];
+    TravState st;
+    TraceCount cnt{0, 0};
+    bool active = false, exhausted = n == 0;
+    uint32_t slot = 0;
+    while(true) {
+        if(!exhausted && __any_sync(0xffffffffu, !active)) {
+            const uint32_t i = warp_fetch(&w.counters[2], !active, n, exhausted);
+            if(!active && i < n) {
+                slot = w.queue[i];
+                const EyeSlot& S = w.slots[slot];
+                trav_begin(st, Ray{f3{S.qo.x, S.qo.y, S.qo.z}, f3{S.qd.x, S.qd.y, S.qd.z}}, S.qo.w, S.qd.w, S.any_mode != 0);
+                active = true;
+            }
+        }
+        if(!__any_sync(0xffffffffu, active)) break;
+        if(active && trav_step<false>(s, st, stack, tl_stack, cnt)) {
+            EyeSlot& S = w.slots[slot];
+            S.best = st.best;
+            S.closest = st.closest_so_far;
+            S.best_mesh = st.best_mesh;
+            active = false;
         }
     }
 }
@@ -1353,20 +1470,73 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     LRT_CUDA(ctx, ctx->ph_eye.ensure(16ull * cap + 12ull * cap + 64));
     float4* L = ctx->ph_eye.as<float4>();
     float* sum = reinterpret_cast<float*>(L + cap);
-    int* overflow = reinterpret_cast<int*>(sum + 3ull * cap);
+    int* overflow = reinterpret_cast<int*>(L + cap) + 3 * cap;
     uint32_t* fetch = reinterpret_cast<uint32_t*>(overflow + 4);
     LRT_CUDA(ctx, cudaMemsetAsync(overflow, 0, 4, ctx->stream));
-    const bool persistent = ctx->photon_eye_persistent;
+    const int mode = ctx->photon_eye_kernel;
+    const bool persistent = mode == 1;
     const int grid = grid_for(ctx, persistent ? (const void*)k_photon_eye_persistent : (const void*)k_photon_eye, kBlock);
+    // wavefront slots: frames up to max_depth deep (a child is pushed only below max_depth)
+    const int frame_limit = pp->max_depth;
+    const uint64_t slot_bytes = sizeof(EyeSlot) + sizeof(EyeFrame) * static_cast<uint64_t>(frame_limit);
+    const uint32_t n_slots = static_cast<uint32_t>(std::min<uint64_t>(1u << 20, (2ull << 30) / slot_bytes));
+    EyeWave w{};
+    if(mode == 2) {
+        LRT_CUDA(ctx, ctx->eye_slots.ensure(sizeof(EyeSlot) * n_slots));
+        LRT_CUDA(ctx, ctx->eye_frames.ensure(sizeof(EyeFrame) * static_cast<size_t>(n_slots) * frame_limit));
+        LRT_CUDA(ctx, ctx->eye_queue.ensure(4ull * n_slots + 64));
+        w.slots = ctx->eye_slots.as<EyeSlot>();
+        w.frames = ctx->eye_frames.as<EyeFrame>();
+        w.queue = ctx->eye_queue.as<uint32_t>();
+        w.counters = w.queue + n_slots;
+        w.L_out = L;
+        w.overflow = overflow;
+        w.frame_limit = frame_limit;
+        w.width = p->width;
+        w.height = p->height;
+    }
+    const int g_shade = grid_for(ctx, (const void*)k_eye_shade, kBlock);
+    const int g_trace = grid_for(ctx, (const void*)k_eye_trace, kBlock);
     const uint32_t spp = p->spp;
-    const uint32_t samples_per_wave = std::min(spp, cap);
-    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
+    // the wavefront form keeps refilling its slots from one large pool of samples, so that the slow drain
+    // of the longest walks happens once per pool rather than once per 2^20 samples
+    const uint32_t wave_cap = mode == 2 ? (1u << 26) : cap;
+    const uint32_t samples_per_wave = std::min(spp, wave_cap);
+    const uint32_t pixels_per_wave = std::max(1u, wave_cap / samples_per_wave);
     const uint32_t pix0 = row_begin * p->width, pix1 = row_end * p->width;
+    if(mode == 2) {
+        const uint64_t pool = std::min<uint64_t>(wave_cap, static_cast<uint64_t>(pix1 - pix0) * spp);
+        const uint64_t pixels = std::min<uint64_t>(pixels_per_wave, pix1 - pix0);
+        LRT_CUDA(ctx, ctx->eye_L.ensure(16 * pool + 12 * pixels));
+        L = ctx->eye_L.as<float4>();
+        sum = reinterpret_cast<float*>(L + pool);
+        w.L_out = L;
+    }
     for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
         const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
         for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
             const uint32_t ns = std::min(samples_per_wave, spp - sb);
-            if(persistent) {
+            if(mode == 2) {
+                w.n_total = np * ns;
+                w.n_slots = std::min(n_slots, w.n_total);
+                w.pixel_begin = pb;
+                w.n_samples = ns;
+                w.sample_begin = p->sample_offset + sb;
+                LRT_CUDA(ctx, cudaMemsetAsync(w.slots, 0, sizeof(EyeSlot) * w.n_slots, ctx->stream));
+                LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 16, ctx->stream));
+                while(true) {
+                    LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 4, ctx->stream));
+                    LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 4, ctx->stream));
+                    k_eye_shade<<<g_shade, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
+                    uint32_t queued = 0;
+                    LRT_CUDA(ctx, cudaMemcpyAsync(&queued, w.counters, 4, cudaMemcpyDeviceToHost, ctx->stream));
+                    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                    ctx->stats.kernel_launches += 1;
+                    if(queued == 0) break;
+                    k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
+                    ctx->stats.kernel_launches += 1;
+                }
+            } else if(persistent) {
                 LRT_CUDA(ctx, cudaMemsetAsync(fetch, 0, 4, ctx->stream));
                 k_photon_eye_persistent<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, ep, p->width, p->height, pb, np,
                                                                           p->sample_offset + sb, ns, L, overflow, fetch);
@@ -1377,7 +1547,7 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
             k_photon_eye_accumulate<<<blocks_for(np), kBlock, 0, ctx->stream>>>(L, pb, np, ns, spp, sum, sb == 0 ? 1 : 0,
                                                                                 sb + ns >= spp ? 1 : 0, rgb_dev);
             LRT_CUDA(ctx, cudaGetLastError());
-            ctx->stats.kernel_launches += 2;
+            ctx->stats.kernel_launches += mode == 2 ? 1 : 2;
         }
     }
     int h_overflow = 0;

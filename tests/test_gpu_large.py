@@ -105,11 +105,14 @@ def test_grid_scene_renders_identical_across_walks(ctx, grid_scene):
     bvh, linear = both_walks(ctx, lambda: ctx.render_photon(pq, pp))
     assert np.array_equal(bvh, linear, equal_nan=True)
     try:
-        ctx.set_option("photon_eye_persistent", 0)
+        ctx.set_option("photon_eye_kernel", 0)
         per_thread = ctx.render_photon(pq, pp)
+        ctx.set_option("photon_eye_kernel", 1)
+        persistent = ctx.render_photon(pq, pp)
     finally:
-        ctx.set_option("photon_eye_persistent", 1)
+        ctx.set_option("photon_eye_kernel", 2)
     assert np.array_equal(bvh, per_thread, equal_nan=True)
+    assert np.array_equal(bvh, persistent, equal_nan=True)
 
 
 @needs_ref

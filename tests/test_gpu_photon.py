@@ -180,19 +180,21 @@ def test_empty_map(ctx):
 
 
 @pytest.mark.parametrize("material", ["coating", "rough_plastic", "rough_conductor"])
-def test_persistent_eye_pass_equals_per_thread(ctx, material):
-    """the persistent eye pass (rays of a warp traced together, lanes refilled as samples finish) makes
-    the walk, draws and additions of the one-sample-per-thread kernel: the images are identical"""
+def test_eye_pass_kernels_agree(ctx, material):
+    """the three forms of the eye pass -- one sample per thread, persistent lanes tracing a warp's rays
+    together, wavefront slots with queued rays -- make the same walk, draws and additions: identical
+    images"""
     sc = scenes.cornell_box(material=material, level=4)
     ctx.upload(sc)
     pp, _ = ctx.photon_preprocess(20000, 20000, 128, 5, radius_cap=0.1, lookup_size=64)
     params = scenes.render_params(20, 16, 3, 8, 3)
+    images = []
     try:
-        ctx.set_option("photon_eye_persistent", 0)
-        per_thread = ctx.render_photon(params, pp)
-        ctx.set_option("photon_eye_persistent", 1)
-        persistent = ctx.render_photon(params, pp)
+        for mode in (0, 1, 2):
+            ctx.set_option("photon_eye_kernel", mode)
+            images.append(ctx.render_photon(params, pp))
     finally:
-        ctx.set_option("photon_eye_persistent", 1)
-    assert np.array_equal(per_thread, persistent, equal_nan=True)
-    assert persistent.mean() > 0
+        ctx.set_option("photon_eye_kernel", 2)
+    assert np.array_equal(images[0], images[1], equal_nan=True)
+    assert np.array_equal(images[0], images[2], equal_nan=True)
+    assert images[2].mean() > 0
