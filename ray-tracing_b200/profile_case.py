@@ -1,13 +1,19 @@
-"""Small, fixed render case for profiler captures (ncu) of the wavefront kernels.
+"""Small, fixed cases for profiler captures (ncu) of the library's kernels.
 
-    python ray-tracing_b200/profile_case.py [--material rough_plastic] [--size 512] [--spp 4] [--frames 2]
+    python ray-tracing_b200/profile_case.py [--case render|eye|adjoint|batch] [options]
 
-Renders `frames` frames of one open-box scene (the benchmark geometry) on cuda:0, then re-renders the
-last frame with work counting on and prints the extension rays of every bounce of that frame, so that
-DRAM bytes an ncu capture reports for one k_extend launch of the last frame can be divided by the rays
-that launch traced. One frame at 512x512x4 spp is one wave of 1M paths: max_depth x 3 + 2 launches,
-about 0.5 GB of device memory. With the defaults, k_extend launch number 9 (0-based, `ncu -k
-regex:k_extend -s 9 -c 1`) is bounce 1 of the last frame.
+render (default): `frames` frames of one open-box scene (the benchmark geometry), then the last frame
+  again with work counting on, printing the extension rays of every bounce of that frame, so that DRAM
+  bytes an ncu capture reports for one k_extend launch can be divided by the rays it traced. One frame
+  at 512x512x4 spp is one wave of 1M paths: max_depth x 3 + 2 launches, about 0.5 GB of device memory.
+  With the defaults, k_extend launch number 9 (0-based, `ncu -k regex:k_extend -s 9 -c 1`) is bounce 1
+  of the last frame.
+eye: the large photon-mapping scene (256 level-5 spheres, 5.24M triangles), `photons` photons, one
+  photon-mapper image of size x size x 1 with the wavefront eye pass (k_eye_shade / k_eye_trace), about
+  2 GB of device memory with the defaults.
+adjoint: the seven-material scene at size x size x spp per material (7 jobs), one render and one
+  path-replay adjoint (k_shade_adj, k_adj_nee, k_adj_suffix).
+batch: 16 seeded jobs of the batched workload with spp scaled down (one graph-replayed wave sequence).
 """
 import argparse
 import json
@@ -22,14 +28,55 @@ import lrt  # noqa: E402
 import scenes  # noqa: E402
 
 
+def eye_case(args):
+    with lrt.Context(0) as ctx:
+        ctx.upload(scenes.large_scene())
+        pp, shots = ctx.photon_preprocess(args.photons, 0, max_depth=8, rr_depth=5, radius_cap=0.05, lookup_size=100)
+        img = ctx.render_photon(scenes.render_params(args.size, args.size, 1, 8, 3), pp)
+        print(json.dumps({"photons": args.photons, "shot": shots[0], "launches": ctx.stats()["kernel_launches"],
+                          "mean": float(img.mean())}))
+
+
+def adjoint_case(args):
+    import diff
+    scene, sphere, index = scenes.open_box_library()
+    with lrt.Context(0) as ctx:
+        ctx.upload(scene)
+        dm = diff.Differentiable(ctx, scene)
+        jobs, off = [], 0
+        for name in scenes.MATERIAL_NAMES:
+            jobs.append(scenes.job_desc(scene.camera, args.size, args.size, args.spp, 0, sphere, index[name], off))
+            off += 3 * args.size * args.size
+        img = ctx.render_batch(jobs, 6, 3)
+        g = dm.adjoint(jobs, 6, 3, np.ones(off, np.float32) / off)
+        print(json.dumps({"mean": float(img.mean()), "grad_norm": float(np.linalg.norm(g))}))
+
+
+def batch_case(args):
+    scene, sphere, index = scenes.open_box_library()
+    jobs, specs = scenes.batch_jobs(index, sphere, n_jobs=16, spp_range=(1, 16))
+    with lrt.Context(0) as ctx:
+        ctx.upload(scene)
+        out = ctx.render_batch(jobs, 8, 3)
+        print(json.dumps({"jobs": len(jobs), "launches": ctx.stats()["kernel_launches"], "mean": float(np.nanmean(out))}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="render", choices=["render", "eye", "adjoint", "batch"])
     ap.add_argument("--material", default="rough_plastic", choices=scenes.MATERIAL_NAMES)
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--spp", type=int, default=4)
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--depth", type=int, default=8)
+    ap.add_argument("--photons", type=int, default=2_000_000)
     args = ap.parse_args()
+    if args.case == "eye":
+        return eye_case(args)
+    if args.case == "adjoint":
+        return adjoint_case(args)
+    if args.case == "batch":
+        return batch_case(args)
     with lrt.Context(0) as ctx:
         ctx.upload(scenes.open_box(args.material))
         img = np.zeros((args.size, args.size, 3), np.float32)
