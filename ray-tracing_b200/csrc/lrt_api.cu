@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
 
 // closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
 template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_extend_persistent(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(WaveArgs a, int depth) {
     const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
     BounceCounters& bc = a.counters[depth];
     const uint32_t n0 = bc.active[0];
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
 // shadow rays with ray replacement: any-hit unless the light's own shape is reachable (then the
 // closest hit decides, scene_occluded)
 template <bool kCount, bool kVis = false>
-__global__ void __launch_bounds__(kBlock) k_shadow_persistent(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int depth) {
     BounceCounters& bc = a.counters[depth];
     const uint32_t n0 = bc.shadow[0];
     const uint32_t n = n0 + bc.shadow[1];
