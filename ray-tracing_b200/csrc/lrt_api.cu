@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
             }
         }
         if(!__any_sync(0xffffffffu, active)) break;
-        if(active && trav_step<kCount>(a.s, st, stack, tl_stack, cnt)) {
+        if(active && trav_step<kCount, true>(a.s, st, stack, tl_stack, cnt)) {
             const bool blocked = st.any_mode ? st.best >= 0 : (st.best >= 0 && a.s.objects[st.best].emitter != light);
             if(kVis) a.adj_sh_vis[k] = blocked ? 0 : 1;
             if(!blocked) {

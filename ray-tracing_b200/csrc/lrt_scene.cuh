@@ -547,7 +547,9 @@ __device__ __forceinline__ int32_t trav_next_object(const DeviceScene& s, TravSt
 
 // One unit of work; returns true when the ray is finished (result in best / best_mesh / closest_so_far;
 // in any_mode best >= 0 means "hit"). Equal t is resolved by object index, as the list's order does.
-template <bool kCount>
+// kLeafInline: one-leaf meshes are tested during the object scan (faster for occlusion rays; for
+// closest-hit rays the longer scan loop costs more than the saved steps).
+template <bool kCount, bool kLeafInline = false>
 __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, TravItem* stack, int32_t* tl_stack,
                                           TraceCount& cnt) {
     if(!st.in_mesh) {
@@ -556,6 +558,35 @@ __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, T
             if(i < 0) return true;
             const ObjRec& o = s.objects[i];
             if(o.kind == LRT_OBJECT_MESH) {
+                if(kLeafInline && o.n_nodes == 1 && ray_may_hit_box(o, st.r, st.t_min, st.closest_so_far)) {
+                    // a tree that is one leaf (a quad, a few triangles): its traversal is that leaf's
+                    // triangles in order over [t_min, closest] -- done here, without entering the mesh
+                    const uint2 n = ld_node(s.nodes + o.node_base);
+                    if(kCount) ++cnt.nodes;
+                    const float4* tris = s.tris + 3ull * o.ref_base;
+                    const uint32_t count = n.y >> 2;
+                    float closest = st.closest_so_far;
+                    bool hit = false;
+                    MeshHit mh{};
+                    for(uint32_t k = 0; k < count; ++k) {
+                        if(kCount) ++cnt.tris;
+                        float u, v;
+                        if(hit_tri_record(tris + 3ull * (n.x + k), st.r, st.t_min, closest, closest, u, v)) {
+                            hit = true;
+                            mh = MeshHit{closest, u, v, n.x + k};
+                            if(st.any_mode) {
+                                st.best = i;
+                                return true;
+                            }
+                        }
+                    }
+                    if(hit && (mh.t < st.closest_so_far || i > st.best)) {
+                        st.closest_so_far = mh.t;
+                        st.best = i;
+                        st.best_mesh = mh;
+                    }
+                    continue;
+                }
                 if(ray_may_hit_box(o, st.r, st.t_min, st.closest_so_far)) {
                     st.obj = i;
                     st.in_mesh = true;
