@@ -168,6 +168,29 @@ def run_reference(args):
 
 # ------------------------------------------------------------------------------------------------
 
+# ------------------------------------------------------------------------------------------------
+# replicas (N > 1): one process per GPU, disjoint sample ranges, the slowest rank's time
+
+def replica_sample_offset(rank: int, spp: int) -> int:
+    """rank r renders samples [r * spp, (r + 1) * spp) of every pixel: replicas never repeat a sample"""
+    return rank * spp
+
+
+def max_over_ranks(dist, value: float, device) -> float:
+    """the slowest rank's value (every rank takes this collective at the same point of the run)"""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mpaths(world: int, paths_per_step: int, steps: int, seconds: float) -> float:
+    """paths of all ranks over the slowest rank's time"""
+    return world * paths_per_step * steps / seconds / 1e6
+
+
 def run_lrt(args):
     import torch
     import lrt
@@ -193,7 +216,7 @@ def run_lrt(args):
         ctxs.append(c)
     out = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    offset = rank * SPP  # replicas render disjoint sample ranges
+    offset = replica_sample_offset(rank, SPP)
     params = scenes.render_params(W, H, SPP, DEPTH, RR, sample_offset=offset)
 
     # algorithmic work per path (exact traversal counts; untimed pass at 8 spp)
@@ -251,10 +274,7 @@ def run_lrt(args):
     stage_ms = {k: sum(s["stage_ms"][k] for s in st) for k in abi_stage_names()}
     for c in ctxs:
         c.set_option("stage_timing", 0)
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, total_ms, dev)
 
     # end to end: the public host-buffer call (lrt_render: render + device->host copy of the image)
     host_img = np.zeros((H, W, 3), dtype=np.float32)
@@ -268,15 +288,10 @@ def run_lrt(args):
         for c in ctxs:
             c.render(params, host_img)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_total = sum(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(dist, sum(e2e_times), dev)
 
-    paths_total = world * PATHS_PER_STEP * args.steps
-    value = paths_total / (total_ms / 1000.0) / 1e6
-    e2e_value = paths_total / e2e_total / 1e6
+    value = whole_job_mpaths(world, PATHS_PER_STEP, args.steps, total_ms / 1000.0)
+    e2e_value = whole_job_mpaths(world, PATHS_PER_STEP, args.steps, e2e_total)
     peak, peak_kind = measured_peaks()
     timed_paths = PATHS_PER_STEP * args.steps
     achieved = (work["extend_bytes_per_path"] * timed_paths / 1e9) / (extend_ms / 1000.0) if extend_ms > 0 else None
