@@ -304,6 +304,28 @@ def run_lrt(args):
         traffic = tr["dram_bytes_per_extension_ray"] * work["extension_rays_per_path"] * timed_paths / extend_launches
     cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
 
+    # the plain GPU path tracer (one launch per frame, one thread per pixel, whole path in registers) on
+    # the same frames and samples: same images, its time beside the wavefront's
+    plain = None
+    if rank == 0 and world == 1:
+        cam = scenes.open_box(MATERIALS[0], attach=False).camera
+        job = scenes.job_desc(cam, W, H, SPP, offset)
+        for c in ctxs:
+            c.render_plain_dev([job], DEPTH, RR, out.data_ptr())  # warm
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for c in ctxs:
+            c.render_plain_dev([job], DEPTH, RR, out.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        plain_s = e0.elapsed_time(e1) / 1000.0
+        plain = {"value": PATHS_PER_STEP / plain_s / 1e6, "unit": "Mpaths/s", "steps": 1,
+                 "kernel": "k_pt_plain (lrt_render_plain): one launch per frame, one thread per pixel",
+                 "wavefront_speedup": value * plain_s * 1e6 / PATHS_PER_STEP}
+
     # equal RMSE: the same samples give the reference's image, so the error against a converged render
     # is the reference's (the cornell box fixture: 32x32, 64 spp vs the reference's 4096 spp)
     rmse = None
@@ -336,6 +358,7 @@ def run_lrt(args):
                          "avg_launch_ms": extend_ms / max(1, extend_launches)},
             "cpu_baseline": cpu,
             "rmse": rmse,
+            "plain_gpu_pt": plain,
             "clocks": clock_info,
             "gpu_launches": launches,
         }
