@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
 
 
 // closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
+constexpr int kRefillLanes = 16;  // idle lanes of a warp before k_extend_persistent fetches new rays
+
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(WaveArgs a, int depth) {
     const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
@@ -324,7 +326,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(WaveArgs a, int
     bool active = false, exhausted = n == 0;
     uint32_t pid = 0;
     while(true) {
-        if(!exhausted && __any_sync(0xffffffffu, !active)) {
+        // refill only once half the warp is idle: a fetch per finished ray costs more than the idle lanes
+        if(!exhausted && __popc(__ballot_sync(0xffffffffu, !active)) >= kRefillLanes) {
             const uint32_t i = warp_fetch(&bc.pad[0], !active, n, exhausted);
             if(!active && i < n) {
                 pid = i < n0 ? queue[i] : queue[a.capacity + (i - n0)];
