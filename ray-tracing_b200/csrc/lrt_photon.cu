@@ -1103,7 +1103,7 @@ __global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) 
     bool active = false, exhausted = n == 0;
     uint32_t slot = 0;
     while(true) {
-        if(!exhausted && __any_sync(0xffffffffu, !active)) {
+        if(!exhausted && __popc(__ballot_sync(0xffffffffu, !active)) >= 16) {  // refill half-idle warps
             const uint32_t i = warp_fetch(&w.counters[2], !active, n, exhausted);
             if(!active && i < n) {
                 slot = w.queue[i];
