@@ -290,6 +290,17 @@ int lrt_rough_transmittance_at_alpha(const float* sliced_table, const float* sli
                                      const float* alpha_range /* 2 */, float alpha,
                                      float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
 
+/* Wavefront OBJ as the reference's load_obj (src/io/obj_loader.h:44-141): 'v', 'vn' and 'f' lines
+ * (faces fanned from their first corner; 1-based or negative indices; corners "p", "p/t", "p//n",
+ * "p/t/n"), triangles with a zero-length cross product dropped, corners without a normal given the
+ * triangle's unit geometric normal, positions centred on the box of the referenced positions and
+ * scaled to a longest side of 1. The arrays are those an lrt_object_desc mesh takes. Call with null
+ * arrays to get the counts, then with arrays of at least those sizes (capacities in vertices and
+ * indices). Errors: LRT_ERR_IO (file), LRT_ERR_INVALID_ARGUMENT (bad index or face, no triangle),
+ * LRT_ERR_RANGE (capacity too small). */
+int lrt_load_obj(const char* path, uint32_t* n_vertices, uint32_t* n_indices, float* positions,
+                 uint32_t vertex_capacity, uint32_t* indices, float* corner_normals, uint32_t index_capacity);
+
 /* Host-only SAH kd-tree build over n primitive bounds (3 floats each in bmin/bmax): the tree
  * sah_kdtree::build makes (src/accelerator/sah_kdtree.h:35-57,175-347), packed depth-first into
  * 8-byte nodes (2 uint32 words each: interior = split bits, right<<2|axis; leaf = first, count<<2|3)

@@ -211,6 +211,35 @@ class RefPhotonMap:
             pass
 
 
+def load_obj(path: str):
+    """the reference's load_obj: (positions [n, 3], indices [m], corner_normals [m, 3]), or None when it
+    returns no mesh. It runs in its own process (oracle/_ref/ref_obj_dump): the reference reads numbers
+    with the iostream extractors, which crash in a Python process whose numpy brought in another C++
+    runtime."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "mesh.bin")
+        rc = subprocess.run([OBJ_DUMP, path, out], capture_output=True).returncode
+        if rc == 1:
+            return None
+        if rc != 0:
+            raise RuntimeError("ref_obj_dump failed (%d)" % rc)
+        raw = open(out, "rb").read()
+    nv, ni = np.frombuffer(raw[:8], dtype="<u4")
+    o = 8
+    pos = np.frombuffer(raw[o:o + 12 * nv], dtype="<f4").reshape(nv, 3).copy()
+    o += 12 * nv
+    idx = np.frombuffer(raw[o:o + 4 * ni], dtype="<u4").copy()
+    o += 4 * ni
+    nrm = np.frombuffer(raw[o:o + 12 * ni], dtype="<f4").reshape(ni, 3).copy()
+    return pos, idx, nrm
+
+
+OBJ_DUMP = os.path.join(REF_DIR, "ref_obj_dump")
+BUNNY_PATH = os.path.join(REF_DIR, "assets", "bunny.obj")
+
+
 def sampler_values(pixel_sample, n_dims):
     ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
     out = np.zeros((len(ps), n_dims), dtype=np.float32)

@@ -268,6 +268,7 @@ extern "C" {
 
 const char* ref_last_error() { return g_error.c_str(); }
 
+
 void* ref_world_create(const lrt_scene_desc* desc, const char* data_root) {
     try {
         auto w = std::make_unique<ref_world>();

@@ -1264,6 +1264,26 @@ int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha, 
 
 float lrt_fresnel_diffuse_reflectance(float eta) { return fresnel_diffuse_reflectance(eta); }
 
+int lrt_load_obj(const char* path, uint32_t* n_vertices, uint32_t* n_indices, float* positions,
+                 uint32_t vertex_capacity, uint32_t* indices, float* corner_normals, uint32_t index_capacity) {
+    if(!path || !n_vertices || !n_indices) return LRT_ERR_INVALID_ARGUMENT;
+    std::vector<float> pos, nrm;
+    std::vector<uint32_t> idx;
+    std::string err;
+    const int st = load_obj(path, pos, idx, nrm, err);
+    if(st != LRT_OK) return st;
+    if(pos.size() / 3 > 0xffffffffull || idx.size() > 0xffffffffull) return LRT_ERR_RANGE;
+    *n_vertices = static_cast<uint32_t>(pos.size() / 3);
+    *n_indices = static_cast<uint32_t>(idx.size());
+    if(!positions && !indices && !corner_normals) return LRT_OK;
+    if(!positions || !indices || !corner_normals) return LRT_ERR_INVALID_ARGUMENT;
+    if(vertex_capacity < *n_vertices || index_capacity < *n_indices) return LRT_ERR_RANGE;
+    memcpy(positions, pos.data(), pos.size() * sizeof(float));
+    memcpy(indices, idx.data(), idx.size() * sizeof(uint32_t));
+    memcpy(corner_normals, nrm.data(), nrm.size() * sizeof(float));
+    return LRT_OK;
+}
+
 int lrt_rough_transmittance_eta_slice(const char* ggx_path, float eta, float* sliced_table, float* sliced_diffuse,
                                       uint32_t capacity, uint32_t* n_alpha_out, float* alpha_range_out) {
     if(!ggx_path || !n_alpha_out || !alpha_range_out) return LRT_ERR_INVALID_ARGUMENT;

@@ -11,6 +11,8 @@
 #include <cstdio>
 #include <fstream>
 #include <limits>
+#include <sstream>
+#include <string>
 #include <thread>
 #include <utility>
 
@@ -741,6 +743,127 @@ void sobol_direction_table(uint32_t table[16][32]) {
 }
 
 // ------------------------------------------------------------------------------------------------
+
+// ------------------------------------------------------------------------------------------------
+// Wavefront OBJ, read as load_obj does (src/io/obj_loader.h:11-141): each line without its '\r';
+// blank and '#' lines skipped; 'v' and 'vn' read three floats with the stream extractor; an 'f'
+// corner is "p", "p/t", "p//n" or "p/t/n" with 1-based or negative (from the end) indices; a face is
+// fanned from its first corner, a triangle whose cross product has zero length is dropped, and a
+// corner without a normal takes the triangle's unit geometric normal. Afterwards every position is
+// moved so that the box of the referenced positions is centred at the origin and scaled so that its
+// longest side is 1. A missing file, an index out of range, a face of fewer than three corners or no
+// triangle at all is an error.
+
+namespace {
+
+int obj_index(int index, int count) { return index < 0 ? count + index : index - 1; }
+
+}  // namespace
+
+int load_obj(const char* path, std::vector<float>& positions_out, std::vector<uint32_t>& indices,
+             std::vector<float>& normals_out, std::string& err) {
+    positions_out.clear();
+    indices.clear();
+    normals_out.clear();
+    std::ifstream file(path);
+    if(!file) {
+        err = std::string("obj: cannot open ") + path;
+        return LRT_ERR_IO;
+    }
+    std::vector<f3> positions, normals, corner_normals;
+    std::string line;
+    uint64_t line_no = 0;
+    while(std::getline(file, line)) {
+        ++line_no;
+        if(!line.empty() && line.back() == '\r') line.pop_back();
+        if(line.empty() || line[0] == '#') continue;
+        std::istringstream stream(line);
+        std::string tag;
+        stream >> tag;
+        if(tag == "v" || tag == "vn") {
+            float x = 0.0f, y = 0.0f, z = 0.0f;
+            stream >> x >> y >> z;
+            (tag == "v" ? positions : normals).push_back(f3{x, y, z});
+        } else if(tag == "f") {
+            std::vector<uint32_t> face_p;
+            std::vector<int> face_n;
+            std::string corner;
+            while(stream >> corner) {
+                int pi = 0, ni = 0;
+                try {
+                    const size_t slash = corner.find('/');
+                    if(slash == std::string::npos) {
+                        pi = std::stoi(corner);
+                    } else {
+                        pi = std::stoi(corner.substr(0, slash));
+                        const size_t slash2 = corner.find('/', slash + 1);
+                        if(slash2 != std::string::npos && slash2 + 1 < corner.size()) ni = std::stoi(corner.substr(slash2 + 1));
+                    }
+                } catch(const std::exception&) {
+                    err = "obj: line " + std::to_string(line_no) + ": malformed face corner";
+                    return LRT_ERR_INVALID_ARGUMENT;
+                }
+                const int p = obj_index(pi, static_cast<int>(positions.size()));
+                if(p < 0 || p >= static_cast<int>(positions.size())) {
+                    err = "obj: line " + std::to_string(line_no) + ": position index out of range";
+                    return LRT_ERR_INVALID_ARGUMENT;
+                }
+                face_p.push_back(static_cast<uint32_t>(p));
+                int n = -1;
+                if(ni != 0) {
+                    n = obj_index(ni, static_cast<int>(normals.size()));
+                    if(n < 0 || n >= static_cast<int>(normals.size())) {
+                        err = "obj: line " + std::to_string(line_no) + ": normal index out of range";
+                        return LRT_ERR_INVALID_ARGUMENT;
+                    }
+                }
+                face_n.push_back(n);
+            }
+            if(face_p.size() < 3) {
+                err = "obj: line " + std::to_string(line_no) + ": face with fewer than three corners";
+                return LRT_ERR_INVALID_ARGUMENT;
+            }
+            for(size_t k = 1; k + 1 < face_p.size(); ++k) {
+                const uint32_t tri[3] = {face_p[0], face_p[k], face_p[k + 1]};
+                const int tri_n[3] = {face_n[0], face_n[k], face_n[k + 1]};
+                const f3 g = cross(positions[tri[1]] - positions[tri[0]], positions[tri[2]] - positions[tri[0]]);
+                if(length_squared(g) <= 0.0f) continue;
+                const f3 unit = g / length(g);
+                for(int c = 0; c < 3; ++c) {
+                    indices.push_back(tri[c]);
+                    corner_normals.push_back(tri_n[c] < 0 ? unit : normals[static_cast<size_t>(tri_n[c])]);
+                }
+            }
+        }
+    }
+    if(indices.empty()) {
+        err = std::string("obj: no triangle in ") + path;
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+    // centre and unitise over the referenced positions (obj_loader.h:15-38)
+    f3 lo = positions[indices[0]], hi = lo;
+    for(const uint32_t i : indices) {
+        const f3 q = positions[i];
+        lo = f3{smin(lo.x, q.x), smin(lo.y, q.y), smin(lo.z, q.z)};
+        hi = f3{smax(hi.x, q.x), smax(hi.y, q.y), smax(hi.z, q.z)};
+    }
+    const f3 center = (lo + hi) * 0.5f;
+    const f3 extent = hi - lo;
+    const float longest = smax(extent.x, smax(extent.y, extent.z));
+    if(longest <= 0.0f) {
+        err = std::string("obj: degenerate bounds in ") + path;
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+    const float scale = 1.0f / longest;
+    positions_out.reserve(3 * positions.size());
+    for(const f3 q : positions) {
+        const f3 m = (q - center) * scale;
+        positions_out.insert(positions_out.end(), {m.x, m.y, m.z});
+    }
+    normals_out.reserve(3 * corner_normals.size());
+    for(const f3 n : corner_normals) normals_out.insert(normals_out.end(), {n.x, n.y, n.z});
+    return LRT_OK;
+}
 
 CamRec camera_from_desc(const lrt_camera_desc& c) {
     const f3 origin = load3(c.origin);

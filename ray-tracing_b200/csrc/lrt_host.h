@@ -57,6 +57,11 @@ struct PackedTree {
 };
 void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out);
 
+// load_obj (src/io/obj_loader.h:44-141): positions (3 floats each, centred and unitised), triangle
+// indices and per-corner normals (3 floats per index)
+int load_obj(const char* path, std::vector<float>& positions, std::vector<uint32_t>& indices,
+             std::vector<float>& corner_normals, std::string& error);
+
 // camera::update for a pinhole with focus distance 1 (src/core/camera.h:20-44)
 CamRec camera_from_desc(const lrt_camera_desc& c);
 

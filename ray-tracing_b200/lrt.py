@@ -28,7 +28,7 @@ EXPORTS = [
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
-    "lrt_render_plain", "lrt_render_plain_dev", "lrt_rough_transmittance_eta_slice",
+    "lrt_render_plain", "lrt_render_plain_dev", "lrt_load_obj", "lrt_rough_transmittance_eta_slice",
     "lrt_rough_transmittance_at_alpha", "lrt_scene_update_materials", "lrt_diff_setup", "lrt_render_adjoint",
     "lrt_render_adjoint_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
@@ -83,6 +83,7 @@ def lib():
         L.lrt_render_batch_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
         L.lrt_render_plain.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32)]
         L.lrt_render_plain_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
+        L.lrt_load_obj.argtypes = [C.c_char_p, P(u32), P(u32), P(f32), u32, P(u32), P(f32), u32]
         L.lrt_rough_transmittance_eta_slice.argtypes = [C.c_char_p, f32, P(f32), P(f32), u32, P(u32), P(f32)]
         L.lrt_rough_transmittance_at_alpha.argtypes = [P(f32), P(f32), u32, P(f32), f32, P(f32), P(f32)]
         L.lrt_scene_update_materials.argtypes = [vp, P(abi.MaterialDesc), u32]
@@ -112,6 +113,23 @@ def rough_transmittance_slice(ggx_path: str, eta: float, alpha: float):
     if st != 0:
         raise LrtError(st, "rough transmittance slice failed")
     return table, np.float32(diffuse.value)
+
+
+def load_obj(path: str):
+    """(positions [n, 3], indices [m], corner_normals [m, 3]) of a Wavefront OBJ, read as the reference's
+    load_obj reads it (centred, longest side 1)"""
+    nv, ni = C.c_uint32(0), C.c_uint32(0)
+    st = lib().lrt_load_obj(path.encode(), C.byref(nv), C.byref(ni), None, 0, None, None, 0)
+    if st != 0:
+        raise LrtError(st, "cannot load %s" % path)
+    pos = np.zeros((nv.value, 3), dtype=np.float32)
+    idx = np.zeros(ni.value, dtype=np.uint32)
+    nrm = np.zeros((ni.value, 3), dtype=np.float32)
+    st = lib().lrt_load_obj(path.encode(), C.byref(nv), C.byref(ni), ptr(pos, C.c_float), nv.value, ptr(idx, C.c_uint32),
+                            ptr(nrm, C.c_float), ni.value)
+    if st != 0:
+        raise LrtError(st, "cannot load %s" % path)
+    return pos, idx, nrm
 
 
 def rough_transmittance_eta_slice(ggx_path: str, eta: float):

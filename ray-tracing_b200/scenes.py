@@ -243,6 +243,16 @@ def displaced_icosphere(level: int, center, radius: float, amplitude: float, see
     return pos.astype(np.float32), idx, corner_normals
 
 
+def obj_mesh(path: str, material: int, scale: float = 1.0, offset=(0.0, 0.0, 0.0)) -> dict:
+    """A mesh object from a Wavefront OBJ (liblrt's lrt_load_obj: the reference's load_obj, centred and
+    scaled to a longest side of 1), then scaled and moved as given."""
+    import lrt
+    pos, idx, nrm = lrt.load_obj(path)
+    if scale != 1.0 or any(offset):
+        pos = (pos * np.float32(scale) + np.asarray(offset, dtype=np.float32)).astype(np.float32)
+    return {"kind": abi.OBJ_MESH, "material": material, "positions": pos, "indices": idx, "corner_normals": nrm}
+
+
 def quad_mesh(p0, p1, p2, p3, material: int):
     """Two-triangle mesh (p0,p1,p2), (p0,p2,p3) with flat corner normals."""
     pos = np.array([p0, p1, p2, p3], dtype=np.float32)
@@ -339,6 +349,26 @@ def cornell_box(level: int = 6, seed: int = 20261203, material: str = "diffuse",
     objects.append(light)
     emitters = [{"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (17.0, 12.0, 4.0)}]
     scene = Scene(objects, mats, emitters, default_camera(aspect), name="cornell_box_%s" % material)
+    if attach:
+        attach_tables(scene.materials)
+    return scene
+
+
+def mesh_box(path: str, material: str = "diffuse", scale: float = 0.9, aspect: float = 1.0, attach: bool = True) -> Scene:
+    """The closed box and ceiling light of cornell_box with an OBJ mesh (e.g. the reference's bunny) in
+    place of the sphere: loaded as the reference's load_obj loads it, scaled to `scale` and set on the
+    floor."""
+    mats, mesh_mat = material_library(material)
+    objects = _box_quads(0, 1, 2, roof=True)
+    mesh = obj_mesh(path, mesh_mat, scale)
+    lo = mesh["positions"].min(axis=0)
+    mesh["positions"] = (mesh["positions"] + np.array([0.0, 0.01 - lo[1], 0.0], dtype=np.float32)).astype(np.float32)
+    objects.append(mesh)
+    h = HOLE
+    objects.append({"kind": abi.OBJ_RECTANGLE, "material": -1, "corner": (-h, BOX_Y - 1e-3, -h),
+                    "edge_u": (2 * h, 0.0, 0.0), "edge_v": (0.0, 0.0, 2 * h)})
+    emitters = [{"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (17.0, 12.0, 4.0)}]
+    scene = Scene(objects, mats, emitters, default_camera(aspect), name="mesh_box_%s" % material)
     if attach:
         attach_tables(scene.materials)
     return scene

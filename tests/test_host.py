@@ -212,3 +212,68 @@ def test_autotune_coordinate_descent_and_keys():
     small = autotune.scaled_jobs(jobs, 1000)
     assert all(j.spp >= 1 for j in small) and sum(j.width * j.height * j.spp for j in small) < \
         sum(j.width * j.height * j.spp for j in jobs)
+
+
+OBJ_TEXT = """# a quad, a pentagon fan, negative indices, normals, a degenerate triangle, CRLF lines
+v 0 0 0\r
+v 2 0 0\r
+v 2 1.5 0\r
+v 0 1.5 0\r
+v 1 0.5 3.25\r
+v 5 5 5
+vn 0 0 2
+vn 0.5 0.25 -1
+vt 0.5 0.5
+
+f 1 2 3 4
+f 1//1 2//2 5//1
+f -6/1/2 -5/1/1 -4 -3 -2
+f 1 1 2
+f 2 3 5
+"""
+
+
+def _write_obj(tmp_path, text=OBJ_TEXT, name="t.obj"):
+    path = tmp_path / name
+    path.write_bytes(text.encode())
+    return str(path)
+
+
+def test_load_obj_matches_reference_loader(tmp_path):
+    path = _write_obj(tmp_path)
+    pos, idx, nrm = lrt.load_obj(path)
+    # 2 (quad) + 1 + 3 (pentagon fan) + 0 (degenerate) + 1 triangles
+    assert idx.size == 3 * 7 and pos.shape == (6, 3) and nrm.shape == (21, 3)
+    ext = pos[np.unique(idx)].max(0) - pos[np.unique(idx)].min(0)
+    assert ext.max() == np.float32(1.0)
+    if not oracle.reference_available():
+        pytest.skip("reference oracle not built")
+    rpos, ridx, rnrm = oracle.load_obj(path)
+    assert np.array_equal(pos.view(np.uint32), rpos.view(np.uint32))
+    assert np.array_equal(idx, ridx)
+    assert np.array_equal(nrm.view(np.uint32), rnrm.view(np.uint32))
+
+
+@pytest.mark.parametrize("text", ["v 0 0 0\nv 1 0 0\nf 1 2 3\n", "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2\n",
+                                  "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1//4 2 3\n", "v 0 0 0\nv 1 0 0\nf 1 1 2\n"])
+def test_load_obj_rejects_what_the_reference_rejects(tmp_path, text):
+    path = _write_obj(tmp_path, text)
+    with pytest.raises(lrt.LrtError):
+        lrt.load_obj(path)
+    if oracle.reference_available():
+        assert oracle.load_obj(path) is None
+    with pytest.raises(lrt.LrtError):
+        lrt.load_obj(str(tmp_path / "missing.obj"))
+
+
+@needs_ref
+def test_load_obj_bunny_matches_reference():
+    """the reference's own asset (src/main.cpp:69): 35,947 vertices, 69,451 faces"""
+    if not os.path.exists(oracle.BUNNY_PATH):
+        pytest.skip("bunny.obj not in the reference tree")
+    pos, idx, nrm = lrt.load_obj(oracle.BUNNY_PATH)
+    rpos, ridx, rnrm = oracle.load_obj(oracle.BUNNY_PATH)
+    assert pos.shape == (35947, 3)
+    assert np.array_equal(pos.view(np.uint32), rpos.view(np.uint32))
+    assert np.array_equal(idx, ridx)
+    assert np.array_equal(nrm.view(np.uint32), rnrm.view(np.uint32))
