@@ -296,10 +296,14 @@ def run_lrt(args):
     timed_paths = PATHS_PER_STEP * args.steps
     achieved = (work["extend_bytes_per_path"] * timed_paths / 1e9) / (extend_ms / 1000.0) if extend_ms > 0 else None
     traffic = None
+    issue = None
     tpath = os.path.join(ROOT, "profiles", "extend_traffic.json")
     if os.path.exists(tpath) and extend_launches:
         with open(tpath) as f:
             tr = json.load(f)
+        issue = {"issue_active_frac": tr.get("issue_active_frac"),
+                 "simt_lane_efficiency": tr.get("lanes_per_warp_instruction", 0) / 32.0 or None,
+                 "source": "ncu capture summarised in profiles/k_extend_persistent_open_box_bounce1.md"}
         # DRAM bytes per extension ray from an ncu capture, scaled to this run's average launch
         traffic = tr["dram_bytes_per_extension_ray"] * work["extension_rays_per_path"] * timed_paths / extend_launches
     cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
@@ -355,7 +359,8 @@ def run_lrt(args):
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": traffic,
                          "algorithmic_bytes": "per extension ray 8*nodes + 48*triangles + 32 ray + 16 hit",
-                         "avg_launch_ms": extend_ms / max(1, extend_launches)},
+                         "avg_launch_ms": extend_ms / max(1, extend_launches),
+                         "issue": issue},
             "cpu_baseline": cpu,
             "rmse": rmse,
             "plain_gpu_pt": plain,
