@@ -7,6 +7,7 @@ pixels, 64 samples per pixel, max depth 8, Russian roulette from depth 3 -- 7 x 
 paths per step. Inputs are synthetic and seeded (scenes.py).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lrt|reference]
+    python bench.py --workload batch|adjoint|large     (one GPU; see run_batch, run_adjoint, run_large)
 
 N > 1 runs as one process per GPU under torch.distributed (NCCL): every rank renders its own replica
 with a disjoint sample range (no data-path collective), the timed region is bracketed by barriers and
@@ -165,8 +166,6 @@ def run_reference(args):
     print(json.dumps(line))
     return 0
 
-
-# ------------------------------------------------------------------------------------------------
 
 # ------------------------------------------------------------------------------------------------
 # replicas (N > 1): one process per GPU, disjoint sample ranges, the slowest rank's time
