@@ -87,7 +87,31 @@ public:
         for(uint32_t i = 0; i < count; ++i) prims[i] = i;
         const int depth_limit = std::min(48, static_cast<int>(8.0f + 1.3f * log2f(static_cast<float>(count))));
         max_depth_ = std::max(depth_limit, 1);
-        build(prims, root, 1, 0);
+        // The events are sorted once here. A child's events are its primitives' unclipped boxes, so they
+        // are a subsequence of its parent's sorted list: filtering keeps them sorted, and every node sees
+        // the list it would have sorted itself (the reference sorts per node, sah_kdtree.h:196-231).
+        std::vector<Event> events;
+        events.reserve(static_cast<size_t>(count) * 6);
+        for(const uint32_t prim : prims) {
+            for(uint8_t axis = 0; axis < 3; ++axis) {
+                const float lo = bmin_[3 * prim + axis];
+                const float hi = bmax_[3 * prim + axis];
+                if(lo == hi) {
+                    events.push_back(Event{lo, prim, 1, axis});
+                } else {
+                    events.push_back(Event{lo, prim, 2, axis});
+                    events.push_back(Event{hi, prim, 0, axis});
+                }
+            }
+        }
+        // keys (axis, position, type, index) are unique per event, so the order is fully determined
+        std::sort(events.begin(), events.end(), [](const Event& a, const Event& b) {
+            if(a.axis != b.axis) return a.axis < b.axis;
+            if(a.position != b.position) return a.position < b.position;
+            if(a.type != b.type) return a.type < b.type;
+            return a.index < b.index;
+        });
+        build(prims, events, root, 1, 0);
     }
 
     std::vector<RawNode> nodes;
@@ -119,7 +143,9 @@ private:
         ordered.insert(ordered.end(), prims.begin(), prims.end());
     }
 
-    float build(const std::vector<uint32_t>& prims, const Box& voxel, int depth, int bad_refines) {
+    // events: the sorted events of `prims` (released once the children's lists are made)
+    float build(const std::vector<uint32_t>& prims, std::vector<Event>& events, const Box& voxel, int depth,
+                int bad_refines) {
         const int index = static_cast<int>(nodes.size());
         nodes.emplace_back();
         const int prim_count = static_cast<int>(prims.size());
@@ -128,28 +154,6 @@ private:
             make_leaf(index, prims);
             return leaf_cost;
         }
-
-        std::vector<Event> events;
-        events.reserve(static_cast<size_t>(prim_count) * 6);
-        for(const uint32_t prim : prims) {
-            for(uint8_t axis = 0; axis < 3; ++axis) {
-                const float lo = bmin_[3 * prim + axis];
-                const float hi = bmax_[3 * prim + axis];
-                if(lo == hi) {
-                    events.push_back(Event{lo, prim, 1, axis});
-                } else {
-                    events.push_back(Event{lo, prim, 2, axis});
-                    events.push_back(Event{hi, prim, 0, axis});
-                }
-            }
-        }
-        // keys (axis, position, type, index) are unique per event, so the order is fully determined
-        std::sort(events.begin(), events.end(), [](const Event& a, const Event& b) {
-            if(a.axis != b.axis) return a.axis < b.axis;
-            if(a.position != b.position) return a.position < b.position;
-            if(a.type != b.type) return a.type < b.type;
-            return a.index < b.index;
-        });
 
         int num_left[3] = {0, 0, 0};
         int num_right[3] = {prim_count, prim_count, prim_count};
@@ -243,6 +247,14 @@ private:
                 right_prims.push_back(prim);
             }
         }
+        std::vector<Event> left_events, right_events;
+        left_events.reserve(left_prims.size() * 6);
+        right_events.reserve(right_prims.size() * 6);
+        for(const Event& e : events) {
+            const uint8_t sd = side_[e.index];
+            if(sd != 2) left_events.push_back(e);
+            if(sd != 1) right_events.push_back(e);
+        }
         events.clear();
         events.shrink_to_fit();
 
@@ -252,9 +264,9 @@ private:
         right_voxel.set_lo(best_axis, best_position);
 
         const int left_index = static_cast<int>(nodes.size());
-        const float left_cost = build(left_prims, left_voxel, depth + 1, bad_refines);
+        const float left_cost = build(left_prims, left_events, left_voxel, depth + 1, bad_refines);
         const int right_index = static_cast<int>(nodes.size());
-        const float right_cost = build(right_prims, right_voxel, depth + 1, bad_refines);
+        const float right_cost = build(right_prims, right_events, right_voxel, depth + 1, bad_refines);
         const auto probability = split_probability(voxel, best_axis, best_position - voxel.lo_a(best_axis),
                                                    voxel.hi_a(best_axis) - best_position);
         const float final_cost = kTraversalCost + probability.first * left_cost + probability.second * right_cost;

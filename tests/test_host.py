@@ -72,7 +72,7 @@ needs_ref = pytest.mark.skipif(not oracle.reference_available(), reason="referen
 
 
 @needs_ref
-@pytest.mark.parametrize("level", [2, 4, 5])
+@pytest.mark.parametrize("level", [2, 4, 5, 6])
 def test_kdtree_identical_to_reference(level):
     bmin, bmax = _tri_bounds(level)
     nodes, refs, depth = lrt.kdtree_build(bmin, bmax)
