@@ -20,6 +20,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "lrt_context.cuh"
@@ -207,6 +209,65 @@ int32_t build_range_host(std::vector<HostPhoton>& ph, int32_t start, int32_t cou
     const int32_t right = build_range_host(ph, mid, start + count - mid, nodes, depth + 1, max_depth);
     nodes[index] = PhotonNode{left, right, axis, ph[mid].p[axis]};
     return index;
+}
+
+// Nodes of the subtree over `count` photons (a leaf at <= 8): the tree's shape depends on counts only.
+int32_t subtree_nodes(int32_t count, std::unordered_map<int32_t, int32_t>& memo) {
+    if(count <= 8) return 1;
+    const auto it = memo.find(count);
+    if(it != memo.end()) return it->second;
+    const int32_t n = 1 + subtree_nodes(count / 2, memo) + subtree_nodes(count - count / 2, memo);
+    memo[count] = n;
+    return n;
+}
+
+// build_range_host on several host threads: a node's nth_element runs before its children, which
+// work on disjoint ranges and write their nodes at the places the depth-first order gives them, so
+// the tree (photon order, nodes, splits) is the serial one.
+void build_range_parallel(std::vector<HostPhoton>& ph, int32_t start, int32_t count, PhotonNode* nodes,
+                          int32_t index, uint32_t depth, uint32_t& max_depth, int spawn_levels,
+                          std::unordered_map<int32_t, int32_t>& memo) {
+    if(spawn_levels <= 0 || count <= 8) {
+        std::vector<PhotonNode> local;
+        uint32_t md = depth;
+        build_range_host(ph, start, count, local, depth, md);
+        for(size_t i = 0; i < local.size(); ++i) {  // shift the subtree's child links to its place
+            PhotonNode nd = local[i];
+            if(nd.axis != 3) {
+                nd.a += index;
+                nd.b += index;
+            }
+            nodes[index + i] = nd;
+        }
+        max_depth = std::max(max_depth, md);
+        return;
+    }
+    float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+    for(int32_t i = 0; i < count; ++i) {
+        for(int a = 0; a < 3; ++a) {
+            lo[a] = smin(lo[a], ph[start + i].p[a]);
+            hi[a] = smax(hi[a], ph[start + i].p[a]);
+        }
+    }
+    const float extent[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    int axis = 0;
+    if(extent[1] > extent[axis]) axis = 1;
+    if(extent[2] > extent[axis]) axis = 2;
+    const int32_t mid = start + count / 2;
+    std::nth_element(ph.begin() + start, ph.begin() + mid, ph.begin() + start + count,
+                     [axis](const HostPhoton& a, const HostPhoton& b) { return a.p[axis] < b.p[axis]; });
+    const int32_t left = index + 1;
+    const int32_t right = left + subtree_nodes(mid - start, memo);
+    max_depth = std::max(max_depth, depth);
+    uint32_t md_left = depth, md_right = depth;
+    std::unordered_map<int32_t, int32_t> memo_left = memo;  // each thread its own cache
+    std::thread t([&]() {
+        build_range_parallel(ph, start, mid - start, nodes, left, depth + 1, md_left, spawn_levels - 1, memo_left);
+    });
+    build_range_parallel(ph, mid, start + count - mid, nodes, right, depth + 1, md_right, spawn_levels - 1, memo);
+    t.join();
+    max_depth = std::max(max_depth, std::max(md_left, md_right));
+    nodes[index] = PhotonNode{left, right, axis, ph[mid].p[axis]};
 }
 
 __global__ void k_photon_gather_attrs(const lrt_photon* in, const uint32_t* order, uint32_t n, float4* pos, float4* dir,
@@ -1274,10 +1335,14 @@ int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photon
         for(uint32_t i = 0; i < n; ++i) {
             ph[i] = HostPhoton{{photons[i].position[0], photons[i].position[1], photons[i].position[2]}, i};
         }
-        std::vector<PhotonNode> nodes;
-        nodes.reserve(n / 4 + 16);
+        std::unordered_map<int32_t, int32_t> memo;
+        std::vector<PhotonNode> nodes(subtree_nodes(static_cast<int32_t>(n), memo));
         uint32_t max_depth = 0;
-        build_range_host(ph, 0, static_cast<int32_t>(n), nodes, 1, max_depth);
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        int levels = 0;
+        while((1u << (levels + 1)) <= hw && levels < 6) ++levels;
+        build_range_parallel(ph, 0, static_cast<int32_t>(n), nodes.data(), 0, 1, max_depth, n >= (1u << 16) ? levels : 0,
+                             memo);
         std::vector<uint32_t> order(n);
         for(uint32_t i = 0; i < n; ++i) order[i] = ph[i].index;
         LRT_CUDA(ctx, pm.pos.ensure(16ull * n));
