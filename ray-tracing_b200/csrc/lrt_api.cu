@@ -269,44 +269,11 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
     }
 }
 
-template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_extend(WaveArgs a, int depth) {
-    const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
-    BounceCounters& bc = a.counters[depth];
-    const uint32_t n0 = bc.active[0];
-    const uint32_t n = n0 + bc.active[1];
-    TraceCount cnt{0, 0};
-    uint32_t rays = 0;
-    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t pid = i < n0 ? queue[i] : queue[a.capacity + (i - n0)];
-        const float4 o = a.o[pid];
-        const float4 d = a.d[pid];
-        HitInfo h;
-        const bool hit = scene_hit<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, kInf, h, cnt);
-        ++rays;
-        int key = 0;
-        if(hit) {
-            const int32_t mat = a.s.objects[h.object].material;
-            key = mat < 0 ? 1 : 2 + a.s.materials[mat].type;
-            a.hit_p[pid] = make_float4(h.p.x, h.p.y, h.p.z, __int_as_float(h.object));
-            a.hit_n[pid] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.front_face ? 1.0f : 0.0f);
-        }
-        const uint32_t slot = warp_append_keyed(bc.key_count, key);
-        a.keyed[static_cast<size_t>(key) * a.capacity + slot] = pid;
-    }
-    if(kCount) {
-        add_count(&a.work[0], cnt.nodes);
-        add_count(&a.work[1], cnt.tris);
-        add_count(&a.work[3], rays);
-        if(blockIdx.x == 0 && threadIdx.x == 0 && depth < LRT_MAX_STAT_DEPTH) {
-            atomicAdd(&a.work[8 + depth], static_cast<unsigned long long>(n));
-        }
-    }
-}
-
-// ---- persistent traversal: every lane keeps a ray, and takes the next one from the queue as soon as
-// its own finishes (ray replacement inside the traversal loop), so a warp's lanes stay busy while its
-// rays need very different numbers of nodes. The per-ray work is the state machine of trav_step.
+// ---- persistent traversal: every lane keeps a ray and idle lanes take new ones from the queue inside
+// the traversal loop (ray replacement), so a warp's lanes stay busy while its rays need very different
+// numbers of nodes: occlusion rays are fetched as soon as a lane is idle, closest-hit rays once half the
+// warp is (a fetch per finished ray cost more than the idle lanes). The per-ray work is the state
+// machine of trav_step.
 
 
 // closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
@@ -665,34 +632,6 @@ __global__ void __launch_bounds__(kBlock) k_adj_nee(WaveArgs a, int depth) {
     __syncthreads();
     for(uint32_t j = threadIdx.x; j < a.diff.n_params; j += blockDim.x) {
         if(acc[j] != 0.0f) atomicAdd(a.adj_grad + j, static_cast<double>(acc[j]));
-    }
-}
-
-template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs a, int depth) {
-    const uint32_t n0 = a.counters[depth].shadow[0];
-    const uint32_t n = n0 + a.counters[depth].shadow[1];
-    TraceCount cnt{0, 0};
-    uint32_t rays = 0;
-    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const size_t k = i < n0 ? i : a.capacity + (i - n0);
-        const float4 o = a.sh_o[k], d = a.sh_d[k], c = a.sh_c[k];
-        const int32_t light = __float_as_int(d.w);
-        const bool blocked = scene_occluded<kCount>(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, 0.001f, o.w, light, cnt);
-        ++rays;
-        if(!blocked) {
-            const uint32_t pid = __float_as_uint(c.w);
-            float4 L = a.L[pid];
-            L.x += c.x;
-            L.y += c.y;
-            L.z += c.z;
-            a.L[pid] = L;
-        }
-    }
-    if(kCount) {
-        add_count(&a.work[5], cnt.nodes);
-        add_count(&a.work[6], cnt.tris);
-        add_count(&a.work[4], rays);
     }
 }
 
