@@ -36,12 +36,14 @@ MATERIALS = scenes.MATERIAL_NAMES
 METRIC = "Mpaths/s (path tracer, 7 materials x 512x512 x 64 spp, depth 8, Hosek sky)"
 WORKLOAD = "open_box_7_materials_512x512_64spp_depth8"
 PATHS_PER_STEP = len(MATERIALS) * W * H * SPP
+ARGS_WAVE_CAPACITY = [0]
 
 
 def config(extra=None):
     c = {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH, "rr_depth": RR,
          "materials": MATERIALS, "triangles": 81920 + 12, "paths_per_step": PATHS_PER_STEP,
-         "l2": "flushed (256 MB write) between timed steps", "parallelism": "replicas"}
+         "l2": "flushed (256 MB write) between timed steps", "parallelism": "replicas",
+         "wave_capacity": ARGS_WAVE_CAPACITY[0] or "library default (2^24: one wave per frame)"}
     if extra:
         c.update(extra)
     return c
@@ -212,6 +214,8 @@ def run_lrt(args):
     for m in MATERIALS:
         c = lrt.Context(local, stream.cuda_stream)
         c.upload(scenes.open_box(m))
+        if args.wave_capacity:
+            c.set_option("wave_capacity", args.wave_capacity)
         ctxs.append(c)
     out = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -674,6 +678,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lrt", choices=["lrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--wave-capacity", type=int, default=0, help="paths per wave (0: the library's default)")
     ap.add_argument("--workload", default="paths", choices=["paths", "batch", "adjoint", "large"],
                     help="paths: the seven-material Mpaths/s workload; batch: the 64-job jobs/s comparison; "
                          "adjoint: gradient steps of the material optimisation")
@@ -682,6 +687,7 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--large-spp", type=int, default=0, help="large workload: spp (0: the configuration's 32)")
     args = ap.parse_args()
+    ARGS_WAVE_CAPACITY[0] = args.wave_capacity
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":

@@ -424,7 +424,9 @@ int lrt_render_adjoint_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t 
 /* statistics of the renders since the last reset; counting adds per-ray node/triangle counters */
 int lrt_render_stats_get(lrt_context* ctx, lrt_render_stats* out);
 int lrt_render_stats_reset(lrt_context* ctx);
-/* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26),
+/* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26;
+ * 0, the default: 2^24 for forward renders, 2^21 for adjoint renders; a wave never holds more paths than
+ * its call renders),
  * "photon_tree_device" (0/1), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
  * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),

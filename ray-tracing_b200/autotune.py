@@ -24,9 +24,9 @@ import lrt_abi as abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE_PATH = os.path.join(HERE, "data", "autotune_cache.json")
-DEFAULTS = {"wave_capacity": 1 << 21, "blocks_per_sm": 0, "pixel_tile": 1}
+DEFAULTS = {"wave_capacity": 1 << 24, "blocks_per_sm": 0, "pixel_tile": 1}  # the library's forward defaults
 CANDIDATES = {
-    "wave_capacity": [1 << 19, 1 << 20, 1 << 21, 1 << 22],
+    "wave_capacity": [1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24],
     "blocks_per_sm": [0, 2, 3],
     "pixel_tile": [1, 4, 8, 16],
 }

@@ -769,6 +769,19 @@ __global__ void __launch_bounds__(kBlock) k_adj_suffix(WaveArgs a) {
     }
 }
 
+// Default paths per wave. A forward wave holds about 250 bytes of state per path, so 2^24 paths (one
+// 512x512 frame at 64 spp) take 4 GB; fewer, larger waves leave less of each bounce to the tail of its
+// persistent kernel. An adjoint path also keeps records for every bounce and material group, so its
+// waves stay at 2^21 paths.
+constexpr uint32_t kForwardWaveCapacity = 1u << 24;
+constexpr uint32_t kAdjointWaveCapacity = 1u << 21;
+
+// slots of the wave that renders `paths` paths: the configured capacity, never more than the call needs
+uint32_t wave_slots(const lrt_context* ctx, unsigned long long paths, bool adjoint) {
+    const uint32_t cap = ctx->wave_capacity ? ctx->wave_capacity : adjoint ? kAdjointWaveCapacity : kForwardWaveCapacity;
+    return static_cast<uint32_t>(std::max<unsigned long long>(1, std::min<unsigned long long>(cap, paths)));
+}
+
 int ensure_wave(lrt_context* ctx, uint32_t cap) {
     WaveState& w = ctx->wave;
     if(w.capacity >= cap) return LRT_OK;
@@ -827,7 +840,7 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     const uint32_t row_end = p->row_end > p->row_begin ? std::min(p->row_end, p->height) : p->height;
     if(row_begin >= row_end) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "empty row range");
     if(static_cast<uint64_t>(p->width) * p->height > 0x3fffffffull) return fail(ctx, LRT_ERR_RANGE, "image too large");
-    const uint32_t cap = ctx->wave_capacity;
+    const uint32_t cap = wave_slots(ctx, static_cast<unsigned long long>(row_end - row_begin) * p->width * p->spp, false);
     int st = ensure_wave(ctx, cap);
     if(st != LRT_OK) return st;
     const size_t counters_bytes = sizeof(BounceCounters) * (p->max_depth + 1);
@@ -964,8 +977,8 @@ void launch_batch_wave(lrt_context* ctx, const WaveArgs& a, size_t counters_byte
 
 // the wave state, counters and job table of a batch of paths (jobs already validated)
 int batch_wave_args(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned long long total, int32_t max_depth,
-                    int32_t rr_depth, WaveArgs& a) {
-    const uint32_t cap = ctx->wave_capacity;
+                    int32_t rr_depth, bool adjoint, WaveArgs& a) {
+    const uint32_t cap = wave_slots(ctx, total, adjoint);
     const uint32_t n_jobs = static_cast<uint32_t>(recs.size());
     int st = ensure_wave(ctx, cap);
     if(st != LRT_OK) return st;
@@ -1048,7 +1061,7 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
     const int jst = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
     if(jst != LRT_OK) return jst;
     WaveArgs a;
-    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, a);
+    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, false, a);
     if(st != LRT_OK) return st;
     LRT_CUDA(ctx, ctx->batch_sums.ensure(4ull * out_floats));
     a.batch_out = rgb_dev;
@@ -1079,7 +1092,7 @@ namespace lrt {
 int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned long long total, int32_t max_depth,
                       int32_t rr_depth, const float* adjoint_dev, double* grad_dev) {
     WaveArgs a;
-    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, a);
+    const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, true, a);
     if(st != LRT_OK) return st;
     const size_t cap = a.capacity;
     const uint32_t kmax = std::max<uint32_t>(1, ctx->diff_kmax);
@@ -1556,7 +1569,9 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
     } else if(strcmp(name, "wave_capacity") == 0) {
-        if(value < 1024 || value > (1ll << 26)) return fail(ctx, LRT_ERR_RANGE, "wave_capacity must be in [1024, 2^26]");
+        if(value != 0 && (value < 1024 || value > (1ll << 26))) {
+            return fail(ctx, LRT_ERR_RANGE, "wave_capacity must be 0 (the defaults) or in [1024, 2^26]");
+        }
         ctx->wave_capacity = static_cast<uint32_t>(value);
     } else {
         return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "unknown option %s", name);

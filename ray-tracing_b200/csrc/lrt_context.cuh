@@ -111,7 +111,7 @@ struct lrt_context {
     lrt_render_stats stats{};
     bool stage_timing = false;
     bool count_work = false;
-    uint32_t wave_capacity = 1u << 21;
+    uint32_t wave_capacity = 0;      // paths per wave; 0: kForwardWaveCapacity / kAdjointWaveCapacity
     uint32_t blocks_per_sm_cap = 0;  // 0: as many resident blocks per SM as occupancy allows
     uint32_t pixel_tile = 1;         // batch path order: bands of this many rows, column by column
     std::vector<cudaEvent_t> events;
