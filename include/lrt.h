@@ -310,7 +310,21 @@ int lrt_kdtree_build(const float* bmin, const float* bmax, uint32_t n, uint32_t*
                      uint32_t max_nodes, uint32_t* refs_out, uint32_t max_refs, uint32_t* n_nodes,
                      uint32_t* n_refs, uint32_t* depth);
 
-/* scene: builds the per-mesh SAH kd-trees on the host and uploads everything to the device */
+/* The trees lrt_kdtree_build makes, for n_meshes meshes at once, built on the context's GPU: all nodes
+ * of a tree level are swept together (event lists sorted once and partitioned stably into the
+ * children, SAH costs from prefix counts, the reference's tie, leaf and retract rules). Boxes are
+ * concatenated mesh after mesh, counts[m] boxes each (at least 1). Each mesh's packed nodes (2 words
+ * each, right-child indices within the mesh) and leaf references follow the previous mesh's in
+ * nodes_out / refs_out; node_counts, ref_counts and depths (may be null) get the per-mesh sizes and
+ * *total_nodes, *total_refs the totals. LRT_ERR_RANGE when the outputs are too small (the totals are
+ * set), LRT_ERR_INVALID_ARGUMENT for a NaN bound or an empty mesh. */
+int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t* counts, const float* bmin,
+                            const float* bmax, uint32_t* nodes_out, uint64_t max_nodes, uint32_t* refs_out,
+                            uint64_t max_refs, uint32_t* node_counts, uint32_t* ref_counts, uint32_t* depths,
+                            uint64_t* total_nodes, uint64_t* total_refs);
+
+/* scene: builds the per-mesh SAH kd-trees (on the host cores, or on the GPU with the option
+ * "kd_build_device") and uploads everything to the device */
 int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc);
 /* bytes the last upload copied host->device */
 uint64_t lrt_scene_device_bytes(const lrt_context* ctx);
@@ -431,7 +445,8 @@ int lrt_render_stats_reset(lrt_context* ctx);
  * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
  * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major),
- * "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
+ * "kd_build_device" (1: lrt_scene_upload builds the meshes' kd-trees on the GPU, the same trees; 0: on
+ * the host cores), "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
  * boxes; 0: the object list in order, as hittable_list::hit does), "photon_eye_kernel" (the
  * photon-mapper eye pass: 2 wavefront -- samples in device-memory slots, their rays traced in queues
  * by the persistent traversal; 1: persistent lanes tracing a warp's rays together; 0: one camera

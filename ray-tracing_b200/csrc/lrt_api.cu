@@ -1281,13 +1281,67 @@ int lrt_kdtree_build(const float* bmin, const float* bmax, uint32_t n, uint32_t*
     return LRT_OK;
 }
 
+int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t* counts, const float* bmin,
+                            const float* bmax, uint32_t* nodes_out, uint64_t max_nodes, uint32_t* refs_out,
+                            uint64_t max_refs, uint32_t* node_counts, uint32_t* ref_counts, uint32_t* depths,
+                            uint64_t* total_nodes, uint64_t* total_refs) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if((n_meshes && !counts) || !total_nodes || !total_refs) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    uint64_t n = 0;
+    for(uint32_t m = 0; m < n_meshes; ++m) {
+        if(counts[m] == 0) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "mesh %u has no primitives", m);
+        n += counts[m];
+    }
+    if(n && (!bmin || !bmax)) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null boxes");
+    std::vector<uint32_t> cv(counts, counts + n_meshes);
+    std::vector<float> lo(bmin, bmin + 3 * n), hi(bmax, bmax + 3 * n);
+    std::vector<PackedTree> trees;
+    std::string err;
+    const int st = build_kdtrees_device(ctx, cv, lo, hi, trees, err);
+    if(st != LRT_OK) return err.empty() ? st : fail(ctx, st, "%s", err.c_str());
+    uint64_t tn = 0, tr = 0;
+    for(const PackedTree& t : trees) {
+        tn += t.nodes.size();
+        tr += t.refs.size();
+    }
+    *total_nodes = tn;
+    *total_refs = tr;
+    if(tn > max_nodes || tr > max_refs || !nodes_out || (tr && !refs_out) || (n_meshes && (!node_counts || !ref_counts))) {
+        return fail(ctx, LRT_ERR_RANGE, "output arrays too small: %llu nodes, %llu references needed",
+                    static_cast<unsigned long long>(tn), static_cast<unsigned long long>(tr));
+    }
+    uint64_t on = 0, orf = 0;
+    for(uint32_t m = 0; m < n_meshes; ++m) {
+        const PackedTree& t = trees[m];
+        for(size_t i = 0; i < t.nodes.size(); ++i) {
+            nodes_out[2 * (on + i)] = t.nodes[i].x;
+            nodes_out[2 * (on + i) + 1] = t.nodes[i].y;
+        }
+        std::copy(t.refs.begin(), t.refs.end(), refs_out + orf);
+        node_counts[m] = static_cast<uint32_t>(t.nodes.size());
+        ref_counts[m] = static_cast<uint32_t>(t.refs.size());
+        if(depths) depths[m] = t.depth;
+        on += t.nodes.size();
+        orf += t.refs.size();
+    }
+    return LRT_OK;
+}
+
 int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     LRT_CUDA(ctx, cudaSetDevice(ctx->device));
     ctx->has_scene = false;
     ctx->diff_params = 0;
     std::string err;
-    const int st = build_host_scene(desc, ctx->host, err);
+    const KdBatchBuilder device_kd = [ctx](const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
+                                           const std::vector<float>& bmax, std::vector<PackedTree>& trees,
+                                           std::string& e) {
+        const int r = build_kdtrees_device(ctx, counts, bmin, bmax, trees, e);
+        if(r != LRT_OK && e.empty()) e = ctx->error;
+        return r;
+    };
+    const int st = build_host_scene(desc, ctx->host, err, ctx->kd_build_device ? &device_kd : nullptr);
     if(st != LRT_OK) return fail(ctx, st, "%s", err.c_str());
     HostScene& h = ctx->host;
     uint64_t bytes = 0;
@@ -1557,6 +1611,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
     } else if(strcmp(name, "photon_eye_kernel") == 0) {
         if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "photon_eye_kernel must be 0, 1 or 2");
         ctx->photon_eye_kernel = static_cast<int>(value);
+    } else if(strcmp(name, "kd_build_device") == 0) {
+        ctx->kd_build_device = value != 0;
     } else if(strcmp(name, "object_bvh") == 0) {
         ctx->object_bvh = value != 0;
         if(ctx->has_scene) ctx->ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(ctx->host.tlas.size() / 2) : 0;

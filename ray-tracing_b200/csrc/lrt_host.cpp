@@ -596,6 +596,25 @@ struct TlasBuilder {
 
 }  // namespace
 
+KdRootInfo kd_root_info(const float* bmin, const float* bmax, uint32_t count) {
+    KdRootInfo r{};
+    Box root;
+    uint64_t events = 0;
+    for(uint32_t i = 0; i < count; ++i) {  // as KdBuilder::run
+        Box b;
+        b.lo = load3(bmin + 3ull * i);
+        b.hi = load3(bmax + 3ull * i);
+        root.extend(b);
+        for(int a = 0; a < 3; ++a) events += bmin[3ull * i + a] == bmax[3ull * i + a] ? 1 : 2;
+    }
+    store3(r.lo, root.lo);
+    store3(r.hi, root.hi);
+    r.depth_limit =
+        count ? std::max(std::min(48, static_cast<int>(8.0f + 1.3f * log2f(static_cast<float>(count)))), 1) : 1;
+    r.n_events = events;
+    return r;
+}
+
 void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out) {
     out = PackedTree{};
     if(count == 0) {
@@ -979,7 +998,7 @@ int pack_materials(const lrt_material_desc* mats, uint32_t n, std::vector<MatRec
     return LRT_OK;
 }
 
-int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
+int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, const KdBatchBuilder* kd) {
     s = HostScene{};
     if(!d) {
         err = "scene description is null";
@@ -1016,19 +1035,32 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
             }
             meshes.push_back(i);
         }
+        // triangle boxes (aabb::extend over the corners) of every mesh, meshes in parallel; then the trees,
+        // on the host per mesh (in the same pass) or by `kd` for all meshes at once
+        std::vector<size_t> first(meshes.size() + 1, 0);
+        for(size_t m = 0; m < meshes.size(); ++m) first[m + 1] = first[m] + d->objects[meshes[m]].n_indices / 3;
+        std::vector<float> all_min(kd ? 3 * first.back() : 0), all_max(kd ? 3 * first.back() : 0);
         std::atomic<size_t> next{0};
         auto worker = [&]() {
+            std::vector<float> own_min, own_max;
             for(size_t m = next++; m < meshes.size(); m = next++) {
                 const lrt_object_desc& o = d->objects[meshes[m]];
                 const uint32_t n_tris = o.n_indices / 3;
-                std::vector<float> bmin(3ull * n_tris), bmax(3ull * n_tris);
+                float* bmin = all_min.data() + 3 * first[m];
+                float* bmax = all_max.data() + 3 * first[m];
+                if(!kd) {
+                    own_min.resize(3ull * n_tris);
+                    own_max.resize(3ull * n_tris);
+                    bmin = own_min.data();
+                    bmax = own_max.data();
+                }
                 for(uint32_t t = 0; t < n_tris; ++t) {
                     Box b;
                     for(int c = 0; c < 3; ++c) b.extend(load3(o.positions + 3ull * o.indices[3 * t + c]));
                     store3(&bmin[3ull * t], b.lo);
                     store3(&bmax[3ull * t], b.hi);
                 }
-                build_kdtree(bmin.data(), bmax.data(), n_tris, trees[meshes[m]]);
+                if(!kd) build_kdtree(bmin, bmax, n_tris, trees[meshes[m]]);
             }
         };
         const size_t n_threads = std::min<size_t>(meshes.size(), std::max(1u, std::thread::hardware_concurrency()));
@@ -1036,6 +1068,26 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err) {
         for(size_t t = 1; t < n_threads; ++t) pool.emplace_back(worker);
         worker();
         for(std::thread& t : pool) t.join();
+        if(kd) {
+            // empty meshes get the empty leaf here; the others are built together
+            std::vector<uint32_t> counts;
+            std::vector<size_t> built_mesh;
+            for(size_t m = 0; m < meshes.size(); ++m) {
+                const uint32_t n_tris = static_cast<uint32_t>(first[m + 1] - first[m]);
+                if(n_tris == 0) {
+                    build_kdtree(nullptr, nullptr, 0, trees[meshes[m]]);
+                } else {
+                    counts.push_back(n_tris);
+                    built_mesh.push_back(meshes[m]);
+                }
+            }
+            if(!counts.empty()) {
+                std::vector<PackedTree> built;
+                const int st = (*kd)(counts, all_min, all_max, built, err);
+                if(st != LRT_OK) return st;
+                for(size_t k = 0; k < built_mesh.size(); ++k) trees[built_mesh[k]] = std::move(built[k]);
+            }
+        }
     }
     Box scene_box;
     for(uint32_t i = 0; i < d->n_objects; ++i) {

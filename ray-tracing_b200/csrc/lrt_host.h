@@ -4,6 +4,7 @@
 
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -45,9 +46,6 @@ struct HostScene {
 };
 
 
-// Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message.
-int build_host_scene(const lrt_scene_desc* desc, HostScene& out, std::string& error);
-
 // SAH kd-tree over triangle AABBs, the tree sah_kdtree::build produces (src/accelerator/sah_kdtree.h:35-57,
 // 175-347), packed depth-first into 8-byte nodes with leaf references in leaf order.
 struct PackedTree {
@@ -55,7 +53,29 @@ struct PackedTree {
     std::vector<uint32_t> refs;  // triangle index per leaf reference
     uint32_t depth = 0;
 };
+
+// Builds the kd-trees of several meshes at once: primitive boxes concatenated mesh after mesh (3 floats
+// each), `counts` primitives per mesh (each at least 1); one tree per mesh in `out`.
+using KdBatchBuilder = std::function<int(const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
+                                         const std::vector<float>& bmax, std::vector<PackedTree>& out,
+                                         std::string& error)>;
+
+// Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message. The meshes'
+// kd-trees are built on the host cores, or by `kd` when it is given.
+int build_host_scene(const lrt_scene_desc* desc, HostScene& out, std::string& error,
+                     const KdBatchBuilder* kd = nullptr);
+
 void build_kdtree(const float* bmin, const float* bmax, uint32_t count, PackedTree& out);
+
+// What a kd-tree build of `count` boxes starts from (sah_kdtree.h:35-57): the root voxel, extended box
+// by box in order; the depth limit min(48, int(8 + 1.3 log2 count)), at least 1; the number of sweep
+// events (two per axis, one where the box is flat on that axis).
+struct KdRootInfo {
+    float lo[3], hi[3];
+    int32_t depth_limit;
+    uint64_t n_events;
+};
+KdRootInfo kd_root_info(const float* bmin, const float* bmax, uint32_t count);
 
 // load_obj (src/io/obj_loader.h:44-141): positions (3 floats each, centred and unitised), triangle
 // indices and per-corner normals (3 floats per index)

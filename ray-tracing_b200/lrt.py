@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "liblrt.so")
 # every entry point include/lrt.h declares (checked by the CPU test suite)
 EXPORTS = [
     "lrt_create", "lrt_destroy", "lrt_last_error", "lrt_status_string", "lrt_rough_transmittance_slice",
-    "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_scene_upload", "lrt_scene_device_bytes",
+    "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_kdtree_build_device", "lrt_scene_upload", "lrt_scene_device_bytes",
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
@@ -64,6 +64,8 @@ def lib():
         L.lrt_fresnel_diffuse_reflectance.restype = f32
         L.lrt_fresnel_diffuse_reflectance.argtypes = [f32]
         L.lrt_kdtree_build.argtypes = [P(f32), P(f32), u32, P(u32), u32, P(u32), u32, P(u32), P(u32), P(u32)]
+        L.lrt_kdtree_build_device.argtypes = [vp, u32, P(u32), P(f32), P(f32), P(u32), u64, P(u32), u64, P(u32),
+                                              P(u32), P(u32), P(u64), P(u64)]
         L.lrt_scene_upload.argtypes = [vp, P(abi.SceneDesc)]
         L.lrt_scene_device_bytes.restype = u64
         L.lrt_scene_device_bytes.argtypes = [vp]
@@ -225,6 +227,35 @@ class Context:
 
     def scene_bytes(self) -> int:
         return int(lib().lrt_scene_device_bytes(self.handle))
+
+    def kdtree_build_device(self, meshes):
+        """GPU SAH kd-trees of several meshes at once; meshes = [(bmin, bmax), ...] with (n, 3) float32
+        boxes. Returns [(nodes (n,2) uint32, refs uint32, depth)] as kdtree_build does per mesh."""
+        counts = np.array([len(b) for b, _ in meshes], dtype=np.uint32)
+        bmin = np.ascontiguousarray(np.concatenate([np.asarray(b, np.float32).reshape(-1, 3) for b, _ in meshes]))
+        bmax = np.ascontiguousarray(np.concatenate([np.asarray(b, np.float32).reshape(-1, 3) for _, b in meshes]))
+        m = len(meshes)
+        nc, rc, dp = np.zeros(m, np.uint32), np.zeros(m, np.uint32), np.zeros(m, np.uint32)
+        tn, tr = C.c_uint64(0), C.c_uint64(0)
+        cap_n, cap_r = max(16, 8 * len(bmin)), max(16, 8 * len(bmin))
+        for _ in range(2):
+            nodes = np.zeros((cap_n, 2), dtype=np.uint32)
+            refs = np.zeros(cap_r, dtype=np.uint32)
+            st = lib().lrt_kdtree_build_device(self.handle, m, ptr(counts, C.c_uint32), ptr(bmin, C.c_float),
+                                               ptr(bmax, C.c_float), ptr(nodes, C.c_uint32), cap_n,
+                                               ptr(refs, C.c_uint32), cap_r, ptr(nc, C.c_uint32), ptr(rc, C.c_uint32),
+                                               ptr(dp, C.c_uint32), C.byref(tn), C.byref(tr))
+            if st == 0:
+                out, on, orf = [], 0, 0
+                for k in range(m):
+                    out.append((nodes[on: on + nc[k]], refs[orf: orf + rc[k]], int(dp[k])))
+                    on += int(nc[k])
+                    orf += int(rc[k])
+                return out
+            if st != -5:
+                self._check(st)
+            cap_n, cap_r = tn.value, tr.value
+        raise LrtError(-5, "kd-tree build: output sizing failed")
 
     def mesh_tree_info(self, obj: int):
         n, r, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
