@@ -323,8 +323,8 @@ int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t*
                             uint64_t max_refs, uint32_t* node_counts, uint32_t* ref_counts, uint32_t* depths,
                             uint64_t* total_nodes, uint64_t* total_refs);
 
-/* scene: builds the per-mesh SAH kd-trees (on the host cores, or on the GPU with the option
- * "kd_build_device") and uploads everything to the device */
+/* scene: builds the per-mesh SAH kd-trees (on the GPU or the host cores, option "kd_build_device") and
+ * uploads everything to the device */
 int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc);
 /* bytes the last upload copied host->device */
 uint64_t lrt_scene_device_bytes(const lrt_context* ctx);
@@ -445,8 +445,8 @@ int lrt_render_stats_reset(lrt_context* ctx);
  * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
  * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major),
- * "kd_build_device" (1: lrt_scene_upload builds the meshes' kd-trees on the GPU, the same trees; 0: on
- * the host cores), "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
+ * "kd_build_device" (where lrt_scene_upload builds the meshes' kd-trees, the same trees either way: 0 the
+ * host cores, 1 the GPU, 2 (default) the GPU for scenes of at least 2^15 triangles), "object_bvh" (1: scenes of more than 16 objects are walked through a hierarchy over the objects'
  * boxes; 0: the object list in order, as hittable_list::hit does), "photon_eye_kernel" (the
  * photon-mapper eye pass: 2 wavefront -- samples in device-memory slots, their rays traced in queues
  * by the persistent traversal; 1: persistent lanes tracing a warp's rays together; 0: one camera

@@ -62,8 +62,9 @@ int job_records(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, std
 
 namespace {
 
-template <typename T>
-cudaError_t upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t s, uint64_t& bytes) {
+template <typename V>
+cudaError_t upload(DevBuf& buf, const V& v, cudaStream_t s, uint64_t& bytes) {
+    using T = typename V::value_type;
     const size_t n = std::max<size_t>(1, v.size()) * sizeof(T);
     cudaError_t e = buf.ensure(n);
     if(e != cudaSuccess) return e;
@@ -1295,7 +1296,7 @@ int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t*
     }
     if(n && (!bmin || !bmax)) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null boxes");
     std::vector<uint32_t> cv(counts, counts + n_meshes);
-    std::vector<float> lo(bmin, bmin + 3 * n), hi(bmax, bmax + 3 * n);
+    BigVec<float> lo(bmin, bmin + 3 * n), hi(bmax, bmax + 3 * n);
     std::vector<PackedTree> trees;
     std::string err;
     const int st = build_kdtrees_device(ctx, cv, lo, hi, trees, err);
@@ -1334,14 +1335,21 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     ctx->has_scene = false;
     ctx->diff_params = 0;
     std::string err;
-    const KdBatchBuilder device_kd = [ctx](const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
-                                           const std::vector<float>& bmax, std::vector<PackedTree>& trees,
+    const KdBatchBuilder device_kd = [ctx](const std::vector<uint32_t>& counts, const BigVec<float>& bmin,
+                                           const BigVec<float>& bmax, std::vector<PackedTree>& trees,
                                            std::string& e) {
         const int r = build_kdtrees_device(ctx, counts, bmin, bmax, trees, e);
         if(r != LRT_OK && e.empty()) e = ctx->error;
         return r;
     };
-    const int st = build_host_scene(desc, ctx->host, err, ctx->kd_build_device ? &device_kd : nullptr);
+    // the GPU build pays a few milliseconds of fixed cost per tree level; below 2^15 triangles the host
+    // build is as fast
+    uint64_t n_tris = 0;
+    for(uint32_t i = 0; desc && desc->objects && i < desc->n_objects; ++i) {
+        if(desc->objects[i].kind == LRT_OBJECT_MESH) n_tris += desc->objects[i].n_indices / 3;
+    }
+    const bool device_trees = ctx->kd_build_device == 1 || (ctx->kd_build_device == 2 && n_tris >= (1u << 15));
+    const int st = build_host_scene(desc, ctx->host, err, device_trees ? &device_kd : nullptr);
     if(st != LRT_OK) return fail(ctx, st, "%s", err.c_str());
     HostScene& h = ctx->host;
     uint64_t bytes = 0;
@@ -1612,7 +1620,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "photon_eye_kernel must be 0, 1 or 2");
         ctx->photon_eye_kernel = static_cast<int>(value);
     } else if(strcmp(name, "kd_build_device") == 0) {
-        ctx->kd_build_device = value != 0;
+        if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "kd_build_device must be 0, 1 or 2");
+        ctx->kd_build_device = static_cast<int>(value);
     } else if(strcmp(name, "object_bvh") == 0) {
         ctx->object_bvh = value != 0;
         if(ctx->has_scene) ctx->ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(ctx->host.tlas.size() / 2) : 0;

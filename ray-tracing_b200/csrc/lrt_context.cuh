@@ -118,7 +118,7 @@ struct lrt_context {
     std::vector<int> event_stage;
     // photons
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
-    bool kd_build_device = false;  // true: lrt_scene_upload builds the meshes' kd-trees on the GPU
+    int kd_build_device = 2;  // lrt_scene_upload's kd-trees: 0 host cores, 1 GPU, 2 GPU from 2^15 triangles
     int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
     lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L;
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
@@ -153,8 +153,8 @@ int job_records(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, std
 
 // The kd-trees of several meshes built together on the context's GPU (lrt_kdbuild.cu); the trees are
 // those build_kdtree makes. Signature of a KdBatchBuilder.
-int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
-                         const std::vector<float>& bmax, std::vector<PackedTree>& out, std::string& err);
+int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, const BigVec<float>& bmin,
+                         const BigVec<float>& bmax, std::vector<PackedTree>& out, std::string& err);
 
 inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 

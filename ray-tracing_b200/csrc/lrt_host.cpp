@@ -998,6 +998,24 @@ int pack_materials(const lrt_material_desc* mats, uint32_t n, std::vector<MatRec
     return LRT_OK;
 }
 
+namespace {
+
+// f(i) for i in [0, n) on all host cores (items taken in order from a shared counter)
+template <typename F>
+void parallel_for(size_t n, F f) {
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for(size_t i = next++; i < n; i = next++) f(i);
+    };
+    const size_t n_threads = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for(size_t t = 1; t < n_threads; ++t) pool.emplace_back(worker);
+    worker();
+    for(std::thread& t : pool) t.join();
+}
+
+}  // namespace
+
 int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, const KdBatchBuilder* kd) {
     s = HostScene{};
     if(!d) {
@@ -1018,8 +1036,8 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
     // ---- objects ----
     // the meshes' kd-trees are independent: validate every mesh, then build the trees on all host cores
     std::vector<PackedTree> trees(d->n_objects);
+    std::vector<uint32_t> meshes;
     {
-        std::vector<uint32_t> meshes;
         for(uint32_t i = 0; i < d->n_objects; ++i) {
             const lrt_object_desc& o = d->objects[i];
             if(o.kind != LRT_OBJECT_MESH) continue;
@@ -1039,11 +1057,10 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
         // on the host per mesh (in the same pass) or by `kd` for all meshes at once
         std::vector<size_t> first(meshes.size() + 1, 0);
         for(size_t m = 0; m < meshes.size(); ++m) first[m + 1] = first[m] + d->objects[meshes[m]].n_indices / 3;
-        std::vector<float> all_min(kd ? 3 * first.back() : 0), all_max(kd ? 3 * first.back() : 0);
-        std::atomic<size_t> next{0};
-        auto worker = [&]() {
+        BigVec<float> all_min(kd ? 3 * first.back() : 0), all_max(kd ? 3 * first.back() : 0);
+        parallel_for(meshes.size(), [&](size_t m) {
             std::vector<float> own_min, own_max;
-            for(size_t m = next++; m < meshes.size(); m = next++) {
+            {
                 const lrt_object_desc& o = d->objects[meshes[m]];
                 const uint32_t n_tris = o.n_indices / 3;
                 float* bmin = all_min.data() + 3 * first[m];
@@ -1062,12 +1079,7 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
                 }
                 if(!kd) build_kdtree(bmin, bmax, n_tris, trees[meshes[m]]);
             }
-        };
-        const size_t n_threads = std::min<size_t>(meshes.size(), std::max(1u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for(size_t t = 1; t < n_threads; ++t) pool.emplace_back(worker);
-        worker();
-        for(std::thread& t : pool) t.join();
+        });
         if(kd) {
             // empty meshes get the empty leaf here; the others are built together
             std::vector<uint32_t> counts;
@@ -1089,6 +1101,60 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
             }
         }
     }
+    // every mesh's nodes, triangle records (one per leaf reference), corner normals, box and area, filled
+    // on all host cores at offsets fixed in object order
+    std::vector<size_t> node_off(d->n_objects + 1, 0), ref_off(d->n_objects + 1, 0), normal_off(d->n_objects + 1, 0);
+    for(uint32_t i = 0; i < d->n_objects; ++i) {
+        const bool mesh = d->objects[i].kind == LRT_OBJECT_MESH;
+        node_off[i + 1] = node_off[i] + (mesh ? trees[i].nodes.size() : 0);
+        ref_off[i + 1] = ref_off[i] + (mesh ? trees[i].refs.size() : 0);
+        normal_off[i + 1] = normal_off[i] + (mesh ? static_cast<size_t>(d->objects[i].n_indices / 3) * 3 : 0);
+    }
+    s.nodes.resize(node_off.back());
+    s.tris.resize(3 * ref_off.back());
+    s.ref_prim.resize(ref_off.back());
+    s.normals.resize(normal_off.back());
+    std::vector<Box> mesh_box(d->n_objects);
+    std::vector<float> mesh_area(d->n_objects, 0.0f);
+    parallel_for(meshes.size(), [&](size_t m) {
+        const uint32_t i = meshes[m];
+        const lrt_object_desc& o = d->objects[i];
+        const PackedTree& tree = trees[i];
+        std::copy(tree.nodes.begin(), tree.nodes.end(), s.nodes.begin() + node_off[i]);
+        float4* tri = s.tris.data() + 3 * ref_off[i];
+        uint32_t* ref = s.ref_prim.data() + ref_off[i];
+        for(const uint32_t t : tree.refs) {
+            const f3 p0 = load3(o.positions + 3ull * o.indices[3 * t]);
+            const f3 p1 = load3(o.positions + 3ull * o.indices[3 * t + 1]);
+            const f3 p2 = load3(o.positions + 3ull * o.indices[3 * t + 2]);
+            const f3 e1 = p1 - p0;
+            const f3 e2 = p2 - p0;
+            const float degenerate = length_squared(cross(e1, e2)) <= 0.0f ? 1.0f : 0.0f;
+            *tri++ = float4{p0.x, p0.y, p0.z, degenerate};
+            *tri++ = float4{e1.x, e1.y, e1.z, 0.0f};
+            *tri++ = float4{e2.x, e2.y, e2.z, 0.0f};
+            *ref++ = t;
+        }
+        const uint32_t n_tris = o.n_indices / 3;
+        float4* nrm = s.normals.data() + normal_off[i];
+        for(uint32_t t = 0; t < n_tris; ++t) {
+            for(int c = 0; c < 3; ++c) {
+                const float* n = o.corner_normals + 9ull * t + 3 * c;
+                *nrm++ = float4{n[0], n[1], n[2], 0.0f};
+            }
+        }
+        Box mb;
+        for(uint32_t v = 0; v < o.n_vertices; ++v) mb.extend(load3(o.positions + 3ull * v));
+        mesh_box[i] = mb;
+        float area = 0.0f;
+        for(uint32_t t = 0; t < n_tris; ++t) {
+            const f3 p0 = load3(o.positions + 3ull * o.indices[3 * t]);
+            const f3 p1 = load3(o.positions + 3ull * o.indices[3 * t + 1]);
+            const f3 p2 = load3(o.positions + 3ull * o.indices[3 * t + 2]);
+            area += 0.5f * length(cross(p1 - p0, p2 - p0));
+        }
+        mesh_area[i] = area;
+    });
     Box scene_box;
     for(uint32_t i = 0; i < d->n_objects; ++i) {
         const lrt_object_desc& o = d->objects[i];
@@ -1104,43 +1170,16 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
         if(o.kind == LRT_OBJECT_MESH) {
             const uint32_t n_tris = o.n_indices / 3;
             const PackedTree& tree = trees[i];
-            r.node_base = static_cast<uint32_t>(s.nodes.size());
-            r.ref_base = static_cast<uint32_t>(s.ref_prim.size());
-            r.tri_base = static_cast<uint32_t>(s.normals.size() / 3);
+            r.node_base = static_cast<uint32_t>(node_off[i]);
+            r.ref_base = static_cast<uint32_t>(ref_off[i]);
+            r.tri_base = static_cast<uint32_t>(normal_off[i] / 3);
             r.n_tris = n_tris;
             r.n_nodes = static_cast<uint32_t>(tree.nodes.size());
-            s.nodes.insert(s.nodes.end(), tree.nodes.begin(), tree.nodes.end());
-            for(const uint32_t t : tree.refs) {
-                const f3 p0 = load3(o.positions + 3ull * o.indices[3 * t]);
-                const f3 p1 = load3(o.positions + 3ull * o.indices[3 * t + 1]);
-                const f3 p2 = load3(o.positions + 3ull * o.indices[3 * t + 2]);
-                const f3 e1 = p1 - p0;
-                const f3 e2 = p2 - p0;
-                const float degenerate = length_squared(cross(e1, e2)) <= 0.0f ? 1.0f : 0.0f;
-                s.tris.push_back(float4{p0.x, p0.y, p0.z, degenerate});
-                s.tris.push_back(float4{e1.x, e1.y, e1.z, 0.0f});
-                s.tris.push_back(float4{e2.x, e2.y, e2.z, 0.0f});
-                s.ref_prim.push_back(t);
-            }
-            for(uint32_t t = 0; t < n_tris; ++t) {
-                for(int c = 0; c < 3; ++c) {
-                    const float* n = o.corner_normals + 9ull * t + 3 * c;
-                    s.normals.push_back(float4{n[0], n[1], n[2], 0.0f});
-                }
-            }
-            Box mb;
-            for(uint32_t v = 0; v < o.n_vertices; ++v) mb.extend(load3(o.positions + 3ull * v));
+            const Box& mb = mesh_box[i];
             store3(r.bmin, mb.lo);
             store3(r.bmax, mb.hi);
             if(o.n_vertices) scene_box.extend(mb);
-            float area = 0.0f;
-            for(uint32_t t = 0; t < n_tris; ++t) {
-                const f3 p0 = load3(o.positions + 3ull * o.indices[3 * t]);
-                const f3 p1 = load3(o.positions + 3ull * o.indices[3 * t + 1]);
-                const f3 p2 = load3(o.positions + 3ull * o.indices[3 * t + 2]);
-                area += 0.5f * length(cross(p1 - p0, p2 - p0));
-            }
-            r.area = area;
+            r.area = mesh_area[i];
             info = MeshTreeInfo{static_cast<uint32_t>(tree.nodes.size()), static_cast<uint32_t>(tree.refs.size()), tree.depth};
         } else if(o.kind == LRT_OBJECT_RECTANGLE) {
             if(!finite3(o.corner) || !finite3(o.edge_u) || !finite3(o.edge_v)) {

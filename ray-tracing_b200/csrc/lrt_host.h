@@ -5,6 +5,8 @@
 #include <stdint.h>
 
 #include <functional>
+#include <memory>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -19,11 +21,34 @@ struct MeshTreeInfo {
     uint32_t depth;  // deepest leaf (root = 1)
 };
 
+// An allocator whose resize leaves new elements uninitialised, for the large arrays that the scene
+// assembly fills on all host cores: their pages are first touched by the threads that write them.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new(static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new(static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using BigVec = std::vector<T, UninitAlloc<T>>;
+
 struct HostScene {
-    std::vector<uint2> nodes;
-    std::vector<float4> tris;
-    std::vector<uint32_t> ref_prim;
-    std::vector<float4> normals;
+    BigVec<uint2> nodes;
+    BigVec<float4> tris;
+    BigVec<uint32_t> ref_prim;
+    BigVec<float4> normals;
     std::vector<ObjRec> objects;
     std::vector<MatRec> materials;
     std::vector<float> tables;
@@ -56,8 +81,8 @@ struct PackedTree {
 
 // Builds the kd-trees of several meshes at once: primitive boxes concatenated mesh after mesh (3 floats
 // each), `counts` primitives per mesh (each at least 1); one tree per mesh in `out`.
-using KdBatchBuilder = std::function<int(const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
-                                         const std::vector<float>& bmax, std::vector<PackedTree>& out,
+using KdBatchBuilder = std::function<int(const std::vector<uint32_t>& counts, const BigVec<float>& bmin,
+                                         const BigVec<float>& bmax, std::vector<PackedTree>& out,
                                          std::string& error)>;
 
 // Validates and packs a scene description. Returns LRT_OK or an LRT_ERR_* with a message. The meshes'

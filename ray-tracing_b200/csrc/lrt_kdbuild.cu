@@ -46,6 +46,57 @@ inline int grid_of(size_t n) {
 inline int grid_each(size_t n) { return static_cast<int>(std::max<size_t>(1, (n + kThreads - 1) / kThreads)); }
 
 // ------------------------------------------------------------------------------------------------
+// device memory: the build's buffers grow level by level; they come from a stream-ordered pool of this
+// build (released at its end), so growing one neither synchronises nor returns memory to the driver
+
+struct BuildPool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaError_t create(int device, cudaStream_t s) {
+        stream = s;
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if(e != cudaSuccess) return e;
+        uint64_t keep = ~0ull;  // keep freed blocks for reuse until the pool is destroyed
+        return cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    ~BuildPool() {
+        if(pool) cudaMemPoolDestroy(pool);  // memory still in flight is released when its frees complete
+    }
+};
+thread_local BuildPool* t_pool = nullptr;
+
+struct PBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    PBuf() = default;
+    PBuf(const PBuf&) = delete;
+    PBuf& operator=(const PBuf&) = delete;
+    ~PBuf() { release(); }
+    void release() {
+        if(ptr) cudaFreeAsync(ptr, t_pool->stream);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    // at least n bytes, growing by a quarter more than asked; the contents are not kept
+    cudaError_t ensure(size_t n) {
+        if(n <= bytes) return cudaSuccess;
+        release();
+        n += n / 4;
+        const cudaError_t e = cudaMallocFromPoolAsync(&ptr, n, t_pool->pool, t_pool->stream);
+        if(e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
 // exclusive scans (out has n + 1 entries; out[n] is the total)
 
 struct U2 {
@@ -81,27 +132,34 @@ __device__ T block_exclusive(T v, T* sh, T& total) {
     return excl;
 }
 
+// a scan's input: in(i) for i in [0, n), read from an array or computed from the build's arrays
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_scan_reduce(const T* in, uint32_t n, T* sums) {
+struct ArrayIn {
+    const T* p;
+    __device__ T operator()(uint32_t i) const { return p[i]; }
+};
+
+template <typename T, typename In>
+__global__ void __launch_bounds__(kThreads) k_scan_reduce(In in, uint32_t n, T* sums) {
     __shared__ T sh[kThreads];
     const size_t base = static_cast<size_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
     T acc = zero_of(T{});
     for(int j = 0; j < kScanPer; ++j) {
-        if(base + j < n) acc = acc + in[base + j];
+        if(base + j < n) acc = acc + in(static_cast<uint32_t>(base + j));
     }
     T total;
     block_exclusive(acc, sh, total);
     if(threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_scan_apply(const T* in, T* out, uint32_t n, const T* offsets) {
+template <typename T, typename In>
+__global__ void __launch_bounds__(kThreads) k_scan_apply(In in, T* out, uint32_t n, const T* offsets) {
     __shared__ T sh[kThreads];
     const size_t base = static_cast<size_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
     T v[kScanPer];
     T acc = zero_of(T{});
     for(int j = 0; j < kScanPer; ++j) {
-        v[j] = base + j < n ? in[base + j] : zero_of(T{});
+        v[j] = base + j < n ? in(static_cast<uint32_t>(base + j)) : zero_of(T{});
         acc = acc + v[j];
     }
     T total;
@@ -116,15 +174,15 @@ __global__ void __launch_bounds__(kThreads) k_scan_apply(const T* in, T* out, ui
 }
 
 struct ScanTemp {
-    DevBuf level[8];
+    PBuf level[8];
 };
 
-template <typename T>
-cudaError_t scan_exclusive(const T* in, T* out, uint32_t n, ScanTemp& tmp, cudaStream_t s, int depth = 0) {
+template <typename T, typename In>
+cudaError_t scan_exclusive(In in, T* out, uint32_t n, ScanTemp& tmp, cudaStream_t s, int depth = 0) {
     if(n == 0) return cudaMemsetAsync(out, 0, sizeof(T), s);
     const uint32_t nb = (n + kScanTile - 1) / kScanTile;
     if(nb == 1) {
-        k_scan_apply<T><<<1, kThreads, 0, s>>>(in, out, n, nullptr);
+        k_scan_apply<T, In><<<1, kThreads, 0, s>>>(in, out, n, nullptr);
         return cudaGetLastError();
     }
     if(depth >= 7) return cudaErrorInvalidValue;
@@ -132,10 +190,10 @@ cudaError_t scan_exclusive(const T* in, T* out, uint32_t n, ScanTemp& tmp, cudaS
     if(e != cudaSuccess) return e;
     T* sums = tmp.level[depth].as<T>();
     T* scanned = sums + nb;
-    k_scan_reduce<T><<<nb, kThreads, 0, s>>>(in, n, sums);
-    e = scan_exclusive(sums, scanned, nb, tmp, s, depth + 1);
+    k_scan_reduce<T, In><<<nb, kThreads, 0, s>>>(in, n, sums);
+    e = scan_exclusive(ArrayIn<T>{sums}, scanned, nb, tmp, s, depth + 1);
     if(e != cudaSuccess) return e;
-    k_scan_apply<T><<<nb, kThreads, 0, s>>>(in, out, n, scanned);
+    k_scan_apply<T, In><<<nb, kThreads, 0, s>>>(in, out, n, scanned);
     return cudaGetLastError();
 }
 
@@ -205,7 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint64_t* kin,
 }
 
 struct SortBufs {
-    DevBuf keys2, vals2, hist;
+    PBuf keys2, vals2, hist;
 };
 
 // sorts keys[0, n) by bits [0, bits) carrying vals; the result ends in (keys, vals)
@@ -225,7 +283,7 @@ cudaError_t radix_sort(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, Sor
     int passes = 0;
     for(int shift = 0; shift < bits; shift += 8, ++passes) {
         k_radix_hist<<<n_tiles, kThreads, 0, s>>>(ka, n, shift, hist, n_tiles);
-        if((e = scan_exclusive(hist, offsets, 256u * n_tiles, st, s)) != cudaSuccess) return e;
+        if((e = scan_exclusive(ArrayIn<uint32_t>{hist}, offsets, 256u * n_tiles, st, s)) != cudaSuccess) return e;
         k_radix_scatter<<<n_tiles, kThreads, 0, s>>>(ka, va, kb, vb, n, shift, offsets, n_tiles);
         std::swap(ka, kb);
         std::swap(va, vb);
@@ -269,7 +327,7 @@ struct EventArrays {
 };
 
 struct EventBufs {
-    DevBuf node, prim, pos, at;
+    PBuf node, prim, pos, at;
     cudaError_t ensure(size_t n) {
         cudaError_t e;
         if((e = node.ensure(4 * n + 4)) != cudaSuccess) return e;
@@ -385,21 +443,24 @@ __device__ inline bool group_starts(const EventArrays& ev, uint32_t e, uint32_t 
 }
 
 // per event: start-or-planar, planar-or-end, planar, first of its (axis, position) group
-__global__ void k_event_flags(uint32_t n, EventArrays ev, const KdNode* nodes, U4* flags, uint32_t* axis_begin) {
+struct EventCounts {
+    EventArrays ev;
+    const KdNode* nodes;
+    __device__ U4 operator()(uint32_t e) const {
+        const uint32_t type = ev.at[e] & 3u;
+        const bool head = group_starts(ev, e, nodes[ev.node[e]].ev_begin);
+        return U4{type != 0u ? 1u : 0u, type != 2u ? 1u : 0u, type == 1u ? 1u : 0u, head ? 1u : 0u};
+    }
+};
+
+// the last event of each group, and the first event of each (node, axis) segment
+__global__ void k_group_tails(uint32_t n, EventArrays ev, const KdNode* nodes, const U4* scan, uint32_t* tail_of,
+                              uint32_t* axis_begin) {
     for(uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const uint32_t node = ev.node[e];
-        const uint32_t begin = nodes[node].ev_begin;
-        const uint32_t at = ev.at[e];
-        const uint32_t type = at & 3u, axis = at >> 2;
-        const bool head = group_starts(ev, e, begin);
-        if(e == begin || (ev.at[e - 1] >> 2) != axis) axis_begin[3ull * node + axis] = e;
-        flags[e] = U4{type != 0u ? 1u : 0u, type != 2u ? 1u : 0u, type == 1u ? 1u : 0u, head ? 1u : 0u};
-    }
-}
-
-__global__ void k_group_tails(uint32_t n, EventArrays ev, const KdNode* nodes, const U4* scan, uint32_t* tail_of) {
-    for(uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const KdNode& nd = nodes[ev.node[e]];
+        const KdNode& nd = nodes[node];
+        const uint32_t axis = ev.at[e] >> 2;
+        if(e == nd.ev_begin || (ev.at[e - 1] >> 2) != axis) axis_begin[3ull * node + axis] = e;
         const bool last = e + 1 == nd.ev_begin + nd.ev_count || group_starts(ev, e + 1, nd.ev_begin);
         if(last) tail_of[scan[e + 1].d - 1] = e;
     }
@@ -469,7 +530,7 @@ __global__ void __launch_bounds__(kThreads) k_group_costs(uint32_t n, EventArray
 
 // leaf or split (sah_kdtree.h:183-190, 285-288); writes the node's tree record
 __global__ void k_node_decide(uint32_t k, KdNode* nodes, const unsigned long long* best, EventArrays ev,
-                              const uint8_t* planar_left_of, KdRaw* raw, uint32_t* split_flag, uint32_t level) {
+                              const uint8_t* planar_left_of, KdRaw* raw, uint32_t level) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= k) return;
     KdNode& nd = nodes[i];
@@ -510,37 +571,37 @@ __global__ void k_node_decide(uint32_t k, KdNode* nodes, const unsigned long lon
         }
     }
     nd.split = split;
-    split_flag[i] = split;
     raw[i] = r;
 }
 
-__global__ void k_event_sides(uint32_t n, EventArrays ev, const KdNode* nodes, const float* bmin, const float* bmax,
-                              U2* flags) {
-    for(uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const KdNode& nd = nodes[ev.node[e]];
-        U2 f{0u, 0u};
-        if(nd.split) {
-            const uint32_t p = ev.prim[e];
-            const uint32_t side = side_of(bmin[3ull * p + nd.axis], bmax[3ull * p + nd.axis], nd.pos, nd.planar_left);
-            f = U2{side != 2u ? 1u : 0u, side != 1u ? 1u : 0u};
-        }
-        flags[e] = f;
-    }
+struct SplitFlags {
+    const KdNode* nodes;
+    __device__ uint32_t operator()(uint32_t i) const { return nodes[i].split; }
+};
+
+// (to the left child, to the right child) of an event or a primitive entry
+__device__ inline U2 child_flags(const KdNode& nd, uint32_t prim, const float* bmin, const float* bmax) {
+    if(!nd.split) return U2{0u, 0u};
+    const uint32_t side = side_of(bmin[3ull * prim + nd.axis], bmax[3ull * prim + nd.axis], nd.pos, nd.planar_left);
+    return U2{side != 2u ? 1u : 0u, side != 1u ? 1u : 0u};
 }
 
-__global__ void k_prim_sides(uint32_t n, const uint32_t* pe_prim, const uint32_t* pe_node, const KdNode* nodes,
-                             const float* bmin, const float* bmax, U2* flags) {
-    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const KdNode& nd = nodes[pe_node[i]];
-        U2 f{0u, 0u};
-        if(nd.split) {
-            const uint32_t p = pe_prim[i];
-            const uint32_t side = side_of(bmin[3ull * p + nd.axis], bmax[3ull * p + nd.axis], nd.pos, nd.planar_left);
-            f = U2{side != 2u ? 1u : 0u, side != 1u ? 1u : 0u};
-        }
-        flags[i] = f;
-    }
-}
+struct EventSides {
+    EventArrays ev;
+    const KdNode* nodes;
+    const float* bmin;
+    const float* bmax;
+    __device__ U2 operator()(uint32_t e) const { return child_flags(nodes[ev.node[e]], ev.prim[e], bmin, bmax); }
+};
+
+struct PrimSides {
+    const uint32_t* pe_prim;
+    const uint32_t* pe_node;
+    const KdNode* nodes;
+    const float* bmin;
+    const float* bmax;
+    __device__ U2 operator()(uint32_t i) const { return child_flags(nodes[pe_node[i]], pe_prim[i], bmin, bmax); }
+};
 
 // the two children of every split node, at 2 x (split nodes before it) in the next level
 __global__ void k_children(uint32_t k, const KdNode* nodes, const uint32_t* split_scan, const U2* ev_scan,
@@ -580,10 +641,12 @@ __global__ void k_children(uint32_t k, const KdNode* nodes, const uint32_t* spli
 
 // stable partition of the events into the children's lists (left child's, then right child's, node
 // after node)
-__global__ void k_event_scatter(uint32_t n, EventArrays ev, const KdNode* nodes, const U2* flags, const U2* scan,
-                                const uint32_t* split_scan, EventArrays out) {
+__global__ void k_event_scatter(uint32_t n, EventSides sides, const U2* scan, const uint32_t* split_scan,
+                                EventArrays out) {
+    const EventArrays& ev = sides.ev;
+    const KdNode* nodes = sides.nodes;
     for(uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const U2 f = flags[e];
+        const U2 f = sides(e);
         if(!f.a && !f.b) continue;
         const uint32_t node = ev.node[e];
         const KdNode& nd = nodes[node];
@@ -609,11 +672,13 @@ __global__ void k_event_scatter(uint32_t n, EventArrays ev, const KdNode* nodes,
     }
 }
 
-__global__ void k_prim_scatter(uint32_t n, const uint32_t* pe_prim, const uint32_t* pe_node, const KdNode* nodes,
-                               const U2* flags, const U2* scan, const uint32_t* split_scan, uint32_t* out_prim,
-                               uint32_t* out_node) {
+__global__ void k_prim_scatter(uint32_t n, PrimSides sides, const U2* scan, const uint32_t* split_scan,
+                               uint32_t* out_prim, uint32_t* out_node) {
+    const uint32_t* pe_prim = sides.pe_prim;
+    const uint32_t* pe_node = sides.pe_node;
+    const KdNode* nodes = sides.nodes;
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const U2 f = flags[i];
+        const U2 f = sides(i);
         if(!f.a && !f.b) continue;
         const uint32_t node = pe_node[i];
         const KdNode& nd = nodes[node];
@@ -694,15 +759,22 @@ __global__ void k_write(uint32_t k, const KdRaw* raw, const KdRaw* next, const u
 }
 
 struct LevelStore {
-    DevBuf raw, pool;
+    PBuf raw, pool;
     uint32_t k = 0;
 };
 
 }  // namespace
 
-int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, const std::vector<float>& bmin,
-                         const std::vector<float>& bmax, std::vector<PackedTree>& out, std::string& err) {
+int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, const BigVec<float>& bmin,
+                         const BigVec<float>& bmax, std::vector<PackedTree>& out, std::string& err) {
     cudaStream_t s = ctx->stream;
+    BuildPool build_pool;
+    LRT_CUDA(ctx, build_pool.create(ctx->device, s));
+    struct PoolScope {
+        BuildPool* saved;
+        explicit PoolScope(BuildPool* p) : saved(t_pool) { t_pool = p; }
+        ~PoolScope() { t_pool = saved; }
+    } pool_scope(&build_pool);
     const uint32_t n_meshes = static_cast<uint32_t>(counts.size());
     uint64_t total = 0;
     for(const uint32_t c : counts) {
@@ -757,7 +829,7 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
     const uint32_t mesh_bits = n_meshes > 1 ? 32 - __builtin_clz(n_meshes - 1) : 0;
     const int key_bits = 36 + static_cast<int>(mesh_bits);
 
-    DevBuf d_bmin, d_bmax, d_mesh, d_limits, d_err, keys, vals;
+    PBuf d_bmin, d_bmax, d_mesh, d_limits, d_err, keys, vals;
     LRT_CUDA(ctx, d_bmin.ensure(4 * bmin.size()));
     LRT_CUDA(ctx, d_bmax.ensure(4 * bmax.size()));
     LRT_CUDA(ctx, d_mesh.ensure(4ull * n_prims));
@@ -794,9 +866,8 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
 
     // ---- level by level
     std::vector<std::unique_ptr<LevelStore>> levels;
-    DevBuf nodes_a, nodes_b, pe_node_a, pe_node_b, flags4, scan4, tails, axis_begin, best, plb, split_flag, split_scan,
-        ev_flags, ev_scan, pe_flags, pe_scan;
-    LRT_CUDA(ctx, nodes_a.ensure(sizeof(KdNode) * n_meshes));
+    PBuf nodes_a, nodes_b, pe_node_a, pe_node_b, scan4, tails, axis_begin, best, plb, split_scan, ev_scan, pe_scan;
+    LRT_CUDA(ctx, nodes_a.ensure(sizeof(KdNode) * std::max<size_t>(n_prims / 2 + 1024, n_meshes)));
     LRT_CUDA(ctx, cudaMemcpyAsync(nodes_a.ptr, roots.data(), sizeof(KdNode) * n_meshes, cudaMemcpyHostToDevice, s));
     k_level0_active<<<grid_each(n_meshes), kThreads, 0, s>>>(n_meshes, nodes_a.as<KdNode>(), glimits);
     levels.emplace_back(new LevelStore());
@@ -805,12 +876,29 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
     k_level0_prims<<<grid_of(n_prims), kThreads, 0, s>>>(n_prims, d_mesh.as<uint32_t>(), levels[0]->pool.as<uint32_t>(),
                                                          pe_node_a.as<uint32_t>());
     uint32_t K = n_meshes, E = static_cast<uint32_t>(n_events), P = n_prims;
+    {
+        // the level buffers at once for twice the root's events (references duplicate as the tree
+        // deepens); a level that needs more grows them
+        const size_t e2 = 2 * n_events + 1024, p2 = 2ull * n_prims + 1024;
+        const size_t k2 = std::max<size_t>(n_prims / 2 + 1024, n_meshes);
+        LRT_CUDA(ctx, ev_b.ensure(e2));
+        LRT_CUDA(ctx, pe_node_b.ensure(4 * p2));
+        LRT_CUDA(ctx, scan4.ensure(sizeof(U4) * e2));
+        LRT_CUDA(ctx, ev_scan.ensure(sizeof(U2) * e2));
+        LRT_CUDA(ctx, pe_scan.ensure(sizeof(U2) * p2));
+        LRT_CUDA(ctx, tails.ensure(4 * e2));
+        LRT_CUDA(ctx, plb.ensure(e2));
+        LRT_CUDA(ctx, nodes_b.ensure(sizeof(KdNode) * k2));
+        LRT_CUDA(ctx, axis_begin.ensure(12 * k2));
+        LRT_CUDA(ctx, best.ensure(8 * k2));
+        LRT_CUDA(ctx, split_scan.ensure(4 * k2));
+    }
     EventBufs* ev_cur = &ev_a;
     EventBufs* ev_next = &ev_b;
-    DevBuf* nodes_cur = &nodes_a;
-    DevBuf* nodes_next = &nodes_b;
-    DevBuf* pen_cur = &pe_node_a;
-    DevBuf* pen_next = &pe_node_b;
+    PBuf* nodes_cur = &nodes_a;
+    PBuf* nodes_next = &nodes_b;
+    PBuf* pen_cur = &pe_node_a;
+    PBuf* pen_next = &pe_node_b;
     for(uint32_t level = 0; K > 0; ++level) {
         if(level >= static_cast<uint32_t>(kMaxLevels)) {
             err = "kd-tree build: too many levels";
@@ -819,17 +907,13 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
         LevelStore& L = *levels[level];
         L.k = K;
         LRT_CUDA(ctx, L.raw.ensure(sizeof(KdRaw) * K));
-        LRT_CUDA(ctx, flags4.ensure(sizeof(U4) * (E + 1ull)));
         LRT_CUDA(ctx, scan4.ensure(sizeof(U4) * (E + 1ull)));
         LRT_CUDA(ctx, tails.ensure(4ull * E + 4));
         LRT_CUDA(ctx, axis_begin.ensure(12ull * K));
         LRT_CUDA(ctx, best.ensure(8ull * K));
         LRT_CUDA(ctx, plb.ensure(E + 4ull));
-        LRT_CUDA(ctx, split_flag.ensure(4ull * K));
         LRT_CUDA(ctx, split_scan.ensure(4ull * (K + 1)));
-        LRT_CUDA(ctx, ev_flags.ensure(sizeof(U2) * (E + 1ull)));
         LRT_CUDA(ctx, ev_scan.ensure(sizeof(U2) * (E + 1ull)));
-        LRT_CUDA(ctx, pe_flags.ensure(sizeof(U2) * (P + 1ull)));
         LRT_CUDA(ctx, pe_scan.ensure(sizeof(U2) * (P + 1ull)));
         const EventArrays ev = ev_cur->view();
         KdNode* nodes = nodes_cur->as<KdNode>();
@@ -837,25 +921,21 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
         const uint32_t* pe_node = pen_cur->as<uint32_t>();
 
         LRT_CUDA(ctx, cudaMemsetAsync(best.ptr, 0xff, 8ull * K, s));
+        LRT_CUDA(ctx, scan_exclusive(EventCounts{ev, nodes}, scan4.as<U4>(), E, st, s));
         if(E) {
-            k_event_flags<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, flags4.as<U4>(), axis_begin.as<uint32_t>());
-        }
-        LRT_CUDA(ctx, scan_exclusive(flags4.as<U4>(), scan4.as<U4>(), E, st, s));
-        if(E) {
-            k_group_tails<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, scan4.as<U4>(), tails.as<uint32_t>());
+            k_group_tails<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, scan4.as<U4>(), tails.as<uint32_t>(),
+                                                         axis_begin.as<uint32_t>());
             k_group_costs<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, scan4.as<U4>(), tails.as<uint32_t>(),
                                                          axis_begin.as<uint32_t>(), best.as<unsigned long long>(),
                                                          plb.as<uint8_t>(), gerr);
         }
         k_node_decide<<<grid_each(K), kThreads, 0, s>>>(K, nodes, best.as<unsigned long long>(), ev, plb.as<uint8_t>(),
-                                                      L.raw.as<KdRaw>(), split_flag.as<uint32_t>(), level);
-        LRT_CUDA(ctx, scan_exclusive(split_flag.as<uint32_t>(), split_scan.as<uint32_t>(), K, st, s));
-        if(E) k_event_sides<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, gmin, gmax, ev_flags.as<U2>());
-        LRT_CUDA(ctx, scan_exclusive(ev_flags.as<U2>(), ev_scan.as<U2>(), E, st, s));
-        if(P) {
-            k_prim_sides<<<grid_of(P), kThreads, 0, s>>>(P, pe_prim, pe_node, nodes, gmin, gmax, pe_flags.as<U2>());
-        }
-        LRT_CUDA(ctx, scan_exclusive(pe_flags.as<U2>(), pe_scan.as<U2>(), P, st, s));
+                                                      L.raw.as<KdRaw>(), level);
+        const EventSides ev_sides{ev, nodes, gmin, gmax};
+        const PrimSides pe_sides{pe_prim, pe_node, nodes, gmin, gmax};
+        LRT_CUDA(ctx, scan_exclusive(SplitFlags{nodes}, split_scan.as<uint32_t>(), K, st, s));
+        LRT_CUDA(ctx, scan_exclusive(ev_sides, ev_scan.as<U2>(), E, st, s));
+        LRT_CUDA(ctx, scan_exclusive(pe_sides, pe_scan.as<U2>(), P, st, s));
         LRT_CUDA(ctx, cudaGetLastError());
 
         uint32_t n_split = 0, error = 0;
@@ -890,13 +970,12 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
         k_children<<<grid_each(K), kThreads, 0, s>>>(K, nodes, split_scan.as<uint32_t>(), ev_scan.as<U2>(), pe_scan.as<U2>(),
                                                    L.raw.as<KdRaw>(), nodes_next->as<KdNode>(), glimits);
         if(E) {
-            k_event_scatter<<<grid_of(E), kThreads, 0, s>>>(E, ev, nodes, ev_flags.as<U2>(), ev_scan.as<U2>(),
-                                                            split_scan.as<uint32_t>(), ev_next->view());
+            k_event_scatter<<<grid_of(E), kThreads, 0, s>>>(E, ev_sides, ev_scan.as<U2>(), split_scan.as<uint32_t>(),
+                                                            ev_next->view());
         }
         if(P) {
-            k_prim_scatter<<<grid_of(P), kThreads, 0, s>>>(P, pe_prim, pe_node, nodes, pe_flags.as<U2>(), pe_scan.as<U2>(),
-                                                           split_scan.as<uint32_t>(), N.pool.as<uint32_t>(),
-                                                           pen_next->as<uint32_t>());
+            k_prim_scatter<<<grid_of(P), kThreads, 0, s>>>(P, pe_sides, pe_scan.as<U2>(), split_scan.as<uint32_t>(),
+                                                           N.pool.as<uint32_t>(), pen_next->as<uint32_t>());
         }
         LRT_CUDA(ctx, cudaGetLastError());
         std::swap(ev_cur, ev_next);
@@ -907,8 +986,8 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
         P = static_cast<uint32_t>(P2);
     }
     // free the per-level working set before the tree passes
-    for(DevBuf* b : {&ev_a.node, &ev_a.prim, &ev_a.pos, &ev_a.at, &ev_b.node, &ev_b.prim, &ev_b.pos, &ev_b.at, &flags4,
-                     &scan4, &tails, &ev_flags, &ev_scan, &pe_flags, &pe_scan, &pe_node_a, &pe_node_b}) {
+    for(PBuf* b : {&ev_a.node, &ev_a.prim, &ev_a.pos, &ev_a.at, &ev_b.node, &ev_b.prim, &ev_b.pos, &ev_b.at, &scan4,
+                     &tails, &ev_scan, &pe_scan, &pe_node_a, &pe_node_b}) {
         b->release();
     }
 
@@ -931,7 +1010,7 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
         node_base[m + 1] = node_base[m] + root_raw[m].sub_nodes;
         ref_base[m + 1] = ref_base[m] + root_raw[m].sub_refs;
     }
-    DevBuf d_node_base, d_ref_base, d_prim_base, d_nodes, d_refs, d_depths;
+    PBuf d_node_base, d_ref_base, d_prim_base, d_nodes, d_refs, d_depths;
     LRT_CUDA(ctx, d_node_base.ensure(8ull * n_meshes));
     LRT_CUDA(ctx, d_ref_base.ensure(8ull * n_meshes));
     LRT_CUDA(ctx, d_prim_base.ensure(4ull * n_meshes));
@@ -951,8 +1030,8 @@ int build_kdtrees_device(lrt_context* ctx, const std::vector<uint32_t>& counts, 
                                                           d_refs.as<uint32_t>(), d_depths.as<uint32_t>());
     }
     LRT_CUDA(ctx, cudaGetLastError());
-    std::vector<uint2> all_nodes(node_base[n_meshes]);
-    std::vector<uint32_t> all_refs(ref_base[n_meshes]);
+    BigVec<uint2> all_nodes(node_base[n_meshes]);
+    BigVec<uint32_t> all_refs(ref_base[n_meshes]);
     std::vector<uint32_t> depths(n_meshes);
     LRT_CUDA(ctx, cudaMemcpyAsync(all_nodes.data(), d_nodes.ptr, 8 * all_nodes.size(), cudaMemcpyDeviceToHost, s));
     LRT_CUDA(ctx, cudaMemcpyAsync(all_refs.data(), d_refs.ptr, 4 * all_refs.size(), cudaMemcpyDeviceToHost, s));

@@ -239,8 +239,8 @@ class Context:
         tn, tr = C.c_uint64(0), C.c_uint64(0)
         cap_n, cap_r = max(16, 8 * len(bmin)), max(16, 8 * len(bmin))
         for _ in range(2):
-            nodes = np.zeros((cap_n, 2), dtype=np.uint32)
-            refs = np.zeros(cap_r, dtype=np.uint32)
+            nodes = np.empty((cap_n, 2), dtype=np.uint32)
+            refs = np.empty(cap_r, dtype=np.uint32)
             st = lib().lrt_kdtree_build_device(self.handle, m, ptr(counts, C.c_uint32), ptr(bmin, C.c_float),
                                                ptr(bmax, C.c_float), ptr(nodes, C.c_uint32), cap_n,
                                                ptr(refs, C.c_uint32), cap_r, ptr(nc, C.c_uint32), ptr(rc, C.c_uint32),

@@ -137,12 +137,16 @@ def test_errors(ctx):
     with pytest.raises(lrt.LrtError) as e:
         ctx.kdtree_build_device([soup(10, 1), (np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32))])
     assert e.value.status == -1
+    with pytest.raises(lrt.LrtError) as e:
+        ctx.set_option("kd_build_device", 3)
+    assert e.value.status == -5
     # the context stays usable
     assert_same(ctx.kdtree_build_device([CASES["forty"]])[0], host_tree(*CASES["forty"]), "forty")
 
 
 def test_scene_upload_with_device_trees():
-    """the large scene (256 level-5 spheres, ground quad, four lights): same trees, same hits"""
+    """the large scene (256 level-5 spheres, ground quad, four lights): same trees, same hits, whichever
+    builder the upload uses (0 host cores, 1 GPU; the default picks the GPU at this size)"""
     scene = scenes.large_scene()
     rng = np.random.default_rng(5)
     rays = random_rays(rng, 200_000, [-5.0, 0.0, -5.0], [5.0, 5.0, 5.0])
