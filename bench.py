@@ -615,6 +615,13 @@ def run_large(args):
     t0 = time.perf_counter()
     scene = scenes.large_scene()
     t_gen = time.perf_counter() - t0
+    # the same upload with the kd-trees built on the host cores, for comparison (the default builds them on
+    # the GPU at this size; the trees are identical)
+    with lrt.Context(local, stream.cuda_stream) as ch:
+        ch.set_option("kd_build_device", 0)
+        t0 = time.perf_counter()
+        ch.upload(scene)
+        t_upload_host = time.perf_counter() - t0
     ctx = lrt.Context(local, stream.cuda_stream)
     t0 = time.perf_counter()
     ctx.upload(scene)
@@ -653,6 +660,7 @@ def run_large(args):
             "config": {"workload": "large_grid_8x8x4_level5_photon_1024x1024x%dspp" % spp,
                        "triangles": scene.triangle_count(), "objects": len(scene.objects),
                        "scene_gen_s": t_gen, "upload_s (kd-trees + object hierarchy + copy)": t_upload,
+                       "upload_host_trees_s": t_upload_host,
                        "device_scene_mb": ctx.scene_bytes() / 1e6,
                        "photons": c3["photons"], "photon_particles_shot": shots[0],
                        "photon_preprocess_s (trace + map build)": t_photons, "k": c3["k"],
