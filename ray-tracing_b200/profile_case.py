@@ -14,6 +14,8 @@ eye: the large photon-mapping scene (256 level-5 spheres, 5.24M triangles), `pho
 adjoint: the seven-material scene at size x size x spp per material (7 jobs), one render and one
   path-replay adjoint (k_shade_adj, k_adj_nee, k_adj_suffix).
 batch: 16 seeded jobs of the batched workload with spp scaled down (one graph-replayed wave sequence).
+kdbuild: the SAH kd-trees of the large scene's 257 meshes (5.24M triangle boxes) built on the GPU in one
+  lrt_kdtree_build_device call (radix sort, then 25 levels of scans, costs, decisions and partitions).
 """
 import argparse
 import json
@@ -61,9 +63,26 @@ def batch_case(args):
         print(json.dumps({"jobs": len(jobs), "launches": ctx.stats()["kernel_launches"], "mean": float(np.nanmean(out))}))
 
 
+def kdbuild_case(args):
+    import time
+    import lrt_abi as abi
+    meshes = []
+    for o in scenes.large_scene().objects:
+        if o["kind"] == abi.OBJ_MESH:
+            tri = o["positions"][o["indices"].reshape(-1, 3)]
+            meshes.append((tri.min(axis=1).astype(np.float32), tri.max(axis=1).astype(np.float32)))
+    with lrt.Context(0) as ctx:
+        t0 = time.perf_counter()
+        trees = ctx.kdtree_build_device(meshes)
+        seconds = time.perf_counter() - t0
+        print(json.dumps({"meshes": len(meshes), "boxes": int(sum(len(b) for b, _ in meshes)),
+                          "nodes": int(sum(len(t[0]) for t in trees)), "refs": int(sum(len(t[1]) for t in trees)),
+                          "seconds_with_python": seconds}))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="render", choices=["render", "eye", "adjoint", "batch"])
+    ap.add_argument("--case", default="render", choices=["render", "eye", "adjoint", "batch", "kdbuild"])
     ap.add_argument("--material", default="rough_plastic", choices=scenes.MATERIAL_NAMES)
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--spp", type=int, default=4)
@@ -77,6 +96,8 @@ def main():
         return adjoint_case(args)
     if args.case == "batch":
         return batch_case(args)
+    if args.case == "kdbuild":
+        return kdbuild_case(args)
     with lrt.Context(0) as ctx:
         ctx.upload(scenes.open_box(args.material))
         img = np.zeros((args.size, args.size, 3), np.float32)
