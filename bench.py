@@ -404,7 +404,7 @@ def run_batch(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     tuned = {"launch_config": dict(autotune.DEFAULTS), "autotune": "off"}
     if not args.no_autotune:
-        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), lambda: torch.cuda.synchronize(dev))
+        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr())
         tuned = {"launch_config": cfg, "autotune": "cache hit" if hit else "tuned now", "autotune_key": key}
 
     def batched():

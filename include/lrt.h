@@ -394,6 +394,23 @@ int lrt_render_batch(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs
 int lrt_render_batch_dev(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth,
                          int32_t rr_depth, float* rgb_dev);
 
+/* Launch-shape autotuner of lrt_render_batch: times the jobs (spp scaled to about 150M paths per trial)
+ * over paths per wave {2^19 .. 2^24}, pixel_tile {1, 4, 8, 16} and blocks_per_sm {0, 2, 3}, one knob at a
+ * time from the defaults, and leaves the fastest on the context (the same as lrt_set_option of the
+ * three). With a cache_path (a text file, one line per size class: triangles and paths rounded up to
+ * powers of two, material and emitter counts), a cached class is applied without timing and a timed one
+ * is appended. The knobs change speed only, never images. No reference counterpart. */
+typedef struct lrt_launch_config {
+    uint32_t wave_capacity;
+    uint32_t pixel_tile;
+    uint32_t blocks_per_sm;
+    uint32_t from_cache;  /* 1: read from cache_path; 0: timed by this call */
+    float seconds;        /* the best trial's time */
+    uint32_t trials;      /* configurations timed by this call */
+} lrt_launch_config;
+int lrt_autotune(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_jobs, int32_t max_depth, int32_t rr_depth,
+                 float* rgb_dev, const char* cache_path, lrt_launch_config* out);
+
 /* The plain GPU path tracer, for comparison: one kernel launch per job, one thread per pixel running
  * the reference's render loop (main.cpp:121-136 over path_integrator::li, path_integrator.h:23-166)
  * with the whole path in registers. Same jobs, output layout and images as lrt_render_batch. */

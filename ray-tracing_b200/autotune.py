@@ -8,19 +8,18 @@ Three knobs change only the speed of lrt_render_batch, never its images:
 The traversal stack depth is not a knob: it must hold the deepest kd-tree path (the reference's
 depth limit), and the kernels' block size is fixed at compile time.
 
-tune() runs a coordinate descent over the candidates, timing the caller's jobs with their spp scaled
-down so that one timing covers about `paths_per_trial` paths. Results are cached in a JSON file keyed
-by the scene's size class (triangle count rounded up to a power of two, material and emitter
-counts) and the job mix's size class.
+The timing and the coordinate descent over the candidates are the library's (lrt_autotune: the
+caller's jobs with spp scaled to about 150M paths per trial, one knob at a time from the defaults).
+This module keeps the chosen configurations in a JSON file keyed by the scene's size class (triangle
+count rounded up to a power of two, material and emitter counts) and the job mix's size class, the
+same key the library's own text cache uses.
 """
 from __future__ import annotations
 
 import json
 import math
 import os
-import time
 
-import lrt_abi as abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE_PATH = os.path.join(HERE, "data", "autotune_cache.json")
@@ -58,58 +57,13 @@ def apply(ctx, cfg: dict) -> None:
         ctx.set_option(k, int(cfg.get(k, DEFAULTS[k])))
 
 
-def scaled_jobs(jobs, paths_per_trial: int):
-    """the jobs with spp scaled so that they hold about paths_per_trial paths (at least 1 spp each)"""
-    total = sum(j.width * j.height * j.spp for j in jobs)
-    f = min(1.0, paths_per_trial / max(1, total))
-    out = []
-    for j in jobs:
-        out.append(abi.JobDesc(j.camera, j.width, j.height, max(1, int(round(j.spp * f))), j.sample_offset,
-                               j.override_object, j.override_material, j.output_offset))
-    return out
+def tune(ctx, jobs, max_depth: int, rr_depth: int, out_ptr: int):
+    """lrt_autotune without a cache file: (best configuration, its trial seconds, configurations timed)"""
+    r = ctx.autotune(jobs, max_depth, rr_depth, out_ptr)
+    return {k: r[k] for k in ORDER}, r["seconds"], r["trials"]
 
 
-def coordinate_descent(measure, candidates=CANDIDATES, order=ORDER, start=None, rounds: int = 1):
-    """minimise measure(cfg) -> seconds over one knob at a time; returns (best cfg, best time, trials)"""
-    best = dict(DEFAULTS if start is None else start)
-    best_t = measure(best)
-    trials = [(dict(best), best_t)]
-    for _ in range(rounds):
-        for knob in order:
-            for v in candidates[knob]:
-                if v == best[knob]:
-                    continue
-                cfg = dict(best, **{knob: v})
-                t = measure(cfg)
-                trials.append((dict(cfg), t))
-                if t < best_t:
-                    best, best_t = cfg, t
-    return best, best_t, trials
-
-
-def tune(ctx, jobs, max_depth: int, rr_depth: int, out_ptr: int, sync, paths_per_trial: int = 150_000_000,
-         repeats: int = 2):
-    """times lrt_render_batch_dev on scaled-down jobs; `sync` waits for the device"""
-    trial_jobs = scaled_jobs(jobs, paths_per_trial)
-
-    def measure(cfg):
-        apply(ctx, cfg)
-        ctx.render_batch_dev(trial_jobs, max_depth, rr_depth, out_ptr)  # warm (allocations, graph)
-        sync()
-        times = []
-        for _ in range(repeats):
-            t0 = time.perf_counter()
-            ctx.render_batch_dev(trial_jobs, max_depth, rr_depth, out_ptr)
-            sync()
-            times.append(time.perf_counter() - t0)
-        return min(times)
-
-    best, best_t, trials = coordinate_descent(measure)
-    apply(ctx, best)
-    return best, best_t, trials
-
-
-def tuned(ctx, scene, jobs, max_depth: int, rr_depth: int, out_ptr: int, sync, cache_path: str = CACHE_PATH,
+def tuned(ctx, scene, jobs, max_depth: int, rr_depth: int, out_ptr: int, cache_path: str = CACHE_PATH,
           retune: bool = False):
     """the cached configuration for this scene/job size class, tuned now (and cached) if missing"""
     key = scene_key(scene, jobs)
@@ -118,7 +72,7 @@ def tuned(ctx, scene, jobs, max_depth: int, rr_depth: int, out_ptr: int, sync, c
         cfg = {k: cache[key][k] for k in ORDER}
         apply(ctx, cfg)
         return cfg, key, True
-    best, best_t, trials = tune(ctx, jobs, max_depth, rr_depth, out_ptr, sync)
-    cache[key] = dict(best, seconds=best_t, trials=len(trials))
+    best, best_t, trials = tune(ctx, jobs, max_depth, rr_depth, out_ptr)
+    cache[key] = dict(best, seconds=best_t, trials=trials)
     save_cache(cache, cache_path)
     return best, key, False

@@ -28,7 +28,7 @@ EXPORTS = [
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
-    "lrt_render_plain", "lrt_render_plain_dev", "lrt_load_obj", "lrt_rough_transmittance_eta_slice",
+    "lrt_render_plain", "lrt_render_plain_dev", "lrt_autotune", "lrt_load_obj", "lrt_rough_transmittance_eta_slice",
     "lrt_rough_transmittance_at_alpha", "lrt_scene_update_materials", "lrt_diff_setup", "lrt_render_adjoint",
     "lrt_render_adjoint_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
@@ -85,6 +85,7 @@ def lib():
         L.lrt_render_batch_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
         L.lrt_render_plain.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, P(f32)]
         L.lrt_render_plain_dev.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp]
+        L.lrt_autotune.argtypes = [vp, P(abi.JobDesc), u32, i32, i32, vp, C.c_char_p, P(abi.LaunchConfig)]
         L.lrt_load_obj.argtypes = [C.c_char_p, P(u32), P(u32), P(f32), u32, P(u32), P(f32), u32]
         L.lrt_rough_transmittance_eta_slice.argtypes = [C.c_char_p, f32, P(f32), P(f32), u32, P(u32), P(f32)]
         L.lrt_rough_transmittance_at_alpha.argtypes = [P(f32), P(f32), u32, P(f32), f32, P(f32), P(f32)]
@@ -337,6 +338,15 @@ class Context:
     def render_batch_dev(self, jobs, max_depth: int, rr_depth: int, rgb_ptr: int):
         arr = (abi.JobDesc * len(jobs))(*jobs)
         self._check(lib().lrt_render_batch_dev(self.handle, arr, len(jobs), max_depth, rr_depth, C.c_void_p(rgb_ptr)))
+
+    def autotune(self, jobs, max_depth: int, rr_depth: int, rgb_ptr: int, cache_path: str | None = None) -> dict:
+        """lrt_autotune: times the batch's launch shapes, leaves the fastest on the context and returns it."""
+        arr = (abi.JobDesc * len(jobs))(*jobs)
+        cfg = abi.LaunchConfig()
+        self._check(lib().lrt_autotune(self.handle, arr, len(jobs), max_depth, rr_depth, C.c_void_p(rgb_ptr),
+                                       cache_path.encode() if cache_path else None, C.byref(cfg)))
+        return {"wave_capacity": cfg.wave_capacity, "pixel_tile": cfg.pixel_tile, "blocks_per_sm": cfg.blocks_per_sm,
+                "from_cache": bool(cfg.from_cache), "seconds": cfg.seconds, "trials": cfg.trials}
 
     def render_plain(self, jobs, max_depth: int, rr_depth: int, out: np.ndarray | None = None) -> np.ndarray:
         """The plain one-launch-per-job path tracer over the same jobs and output layout."""

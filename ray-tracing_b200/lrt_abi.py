@@ -132,6 +132,11 @@ class JobDesc(C.Structure):
                 ("output_offset", C.c_uint64)]
 
 
+class LaunchConfig(C.Structure):
+    _fields_ = [("wave_capacity", C.c_uint32), ("pixel_tile", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("from_cache", C.c_uint32), ("seconds", C.c_float), ("trials", C.c_uint32)]
+
+
 class PhotonRenderParams(C.Structure):
     _fields_ = [("global_map", C.c_int32), ("caustic_map", C.c_int32), ("global_radius", C.c_float),
                 ("caustic_radius", C.c_float), ("max_depth", C.c_int32), ("max_specular_depth", C.c_int32),

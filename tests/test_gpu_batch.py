@@ -161,12 +161,21 @@ def test_launch_knobs_keep_images(ctx, library, tmp_path):
         import torch
         out = torch.zeros(ref.size, dtype=torch.float32, device="cuda")
         cache = str(tmp_path / "cache.json")
-        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), torch.cuda.synchronize,
-                                       cache_path=cache)
+        cfg, key, hit = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), cache_path=cache)
         assert not hit and all(cfg[k] in autotune.CANDIDATES[k] for k in autotune.ORDER)
-        cfg2, key2, hit2 = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), torch.cuda.synchronize,
-                                          cache_path=cache)
+        cfg2, key2, hit2 = autotune.tuned(ctx, scene, jobs, DEPTH, RR, out.data_ptr(), cache_path=cache)
         assert hit2 and cfg2 == cfg and key2 == key
+        assert np.array_equal(ctx.render_batch(jobs, DEPTH, RR), ref)
+        # the library's own text cache: timed once (6 + 3 + 2 configurations at most), then read back
+        native = str(tmp_path / "launch_cache.txt")
+        r1 = ctx.autotune(jobs, DEPTH, RR, out.data_ptr(), native)
+        assert not r1["from_cache"] and r1["trials"] == 11 and r1["seconds"] > 0
+        assert all(r1[k] in autotune.CANDIDATES[k] for k in autotune.ORDER)
+        r2 = ctx.autotune(jobs, DEPTH, RR, out.data_ptr(), native)
+        assert r2["from_cache"] and all(r2[k] == r1[k] for k in autotune.ORDER)
+        with open(native) as f:
+            line = f.read().split()
+        assert line[0] == key and [int(x) for x in line[1:4]] == [r1[k] for k in autotune.ORDER]
         assert np.array_equal(ctx.render_batch(jobs, DEPTH, RR), ref)
     finally:
         autotune.apply(ctx, autotune.DEFAULTS)

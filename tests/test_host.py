@@ -2,7 +2,6 @@
 restatements (SAH kd-tree build, ggx.dat slicing, Fdr quadrature, Sobol table) match the reference.
 No GPU work is launched here."""
 import ctypes as C
-import math
 import os
 import re
 
@@ -193,25 +192,22 @@ def test_diff_param_groups():
     assert chan == [0, 1, -1, 2, 2, 0, -1]
 
 
-def test_autotune_coordinate_descent_and_keys():
+def test_autotune_keys_and_cache(tmp_path):
     import autotune
-    # a separable cost with its minimum at capacity 2^20, tile 8, blocks 2
-    target = {"wave_capacity": 1 << 20, "pixel_tile": 8, "blocks_per_sm": 2}
-    calls = []
-
-    def measure(cfg):
-        calls.append(dict(cfg))
-        return sum(abs(math.log2(max(1, cfg[k])) - math.log2(max(1, target[k]))) for k in target) + 1.0
-
-    best, t, trials = autotune.coordinate_descent(measure)
-    assert best == target and t == 1.0 and len(trials) == len(calls)
     scene, sphere, index = scenes.open_box_library(level=1)
     jobs, _ = scenes.batch_jobs(index, sphere, n_jobs=4)
     k1 = autotune.scene_key(scene, jobs)
     assert k1 == autotune.scene_key(scene, jobs) and k1.startswith("tris2^")
-    small = autotune.scaled_jobs(jobs, 1000)
-    assert all(j.spp >= 1 for j in small) and sum(j.width * j.height * j.spp for j in small) < \
-        sum(j.width * j.height * j.spp for j in jobs)
+    tris = scene.triangle_count()
+    paths = sum(j.width * j.height * j.spp for j in jobs)
+    # the library's key: ceil(log2) of the triangle and path counts
+    assert k1 == "tris2^%d_mats%d_emitters%d_paths2^%d" % ((tris - 1).bit_length(), len(scene.materials),
+                                                          len(scene.emitters), (paths - 1).bit_length())
+    path = str(tmp_path / "c.json")
+    autotune.save_cache({k1: dict(autotune.DEFAULTS, seconds=0.5, trials=3)}, path)
+    assert autotune.load_cache(path)[k1]["wave_capacity"] == autotune.DEFAULTS["wave_capacity"]
+    assert autotune.load_cache(str(tmp_path / "missing.json")) == {}
+    assert all(autotune.DEFAULTS[k] in autotune.CANDIDATES[k] for k in autotune.ORDER)
 
 
 OBJ_TEXT = """# a quad, a pentagon fan, negative indices, normals, a degenerate triangle, CRLF lines
