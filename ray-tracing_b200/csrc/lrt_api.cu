@@ -411,10 +411,13 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
 }
 
 // one bounce of shading; kAdj adds the adjoint's derivative records (sampled direction, NEE)
-template <bool kAdj>
+// kKey < 0: every shading key's segment in one launch; kKey >= 0: that key's segment only (0 misses,
+// 1 hits without a BSDF, 2 + t materials of type t), with only that type's BSDF code compiled in
+template <bool kAdj, int kKey = -1>
 __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_t* prefix) {
+    constexpr int kType = kKey >= 2 ? kKey - 2 : -1;
     BounceCounters& bc = a.counters[depth];
-    if(threadIdx.x == 0) {
+    if(kKey < 0 && threadIdx.x == 0) {
         uint32_t acc = 0;
         for(int k = 0; k < kKeys; ++k) {
             prefix[k] = acc;
@@ -422,16 +425,22 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
         }
         prefix[kKeys] = acc;
     }
-    __syncthreads();
-    const uint32_t total = prefix[kKeys];
+    if(kKey < 0) __syncthreads();
+    const uint32_t total = kKey < 0 ? prefix[kKeys] : bc.key_count[kKey < 0 ? 0 : kKey];
     uint32_t* next = (depth & 1) ? a.q0 : a.q1;
     BounceCounters& nc = a.counters[depth + 1];
     const DeviceScene& s = a.s;
     uint32_t shading = 0;
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        int key = 0;
-        while(key + 1 < kKeys && prefix[key + 1] <= i) ++key;
-        const uint32_t pid = a.keyed[static_cast<size_t>(key) * a.capacity + (i - prefix[key])];
+        int key = kKey;
+        uint32_t pid;
+        if(kKey < 0) {
+            key = 0;
+            while(key + 1 < kKeys && prefix[key + 1] <= i) ++key;
+            pid = a.keyed[static_cast<size_t>(key) * a.capacity + (i - prefix[key])];
+        } else {
+            pid = a.keyed[static_cast<size_t>(key) * a.capacity + i];
+        }
         const float4 o4 = a.o[pid], d4 = a.d[pid], tp4 = a.tp[pid], L4 = a.L[pid];
         const float2 misc = a.misc[pid];
         const f3 ro{o4.x, o4.y, o4.z};
@@ -521,9 +530,9 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
                 }
                 if(have_target) {
                     rec.wo = to_local(basis, shadow_dir);
-                    const f3 f_cos = bsdf_eval(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                    const f3 f_cos = bsdf_eval_t<kType>(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
                     if(!is_zero(f_cos)) {
-                        const float bsdf_pdf_v = bsdf_pdf(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                        const float bsdf_pdf_v = bsdf_pdf_t<kType>(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
                         const float light_pdf = pdf_emitter_direction(s, p, shadow_dir);
                         if(light_pdf > 0.0f) {
                             const float w = power_heuristic(light_pdf, bsdf_pdf_v);
@@ -557,7 +566,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
             a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
             continue;
         }
-        const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, rec, bsdf_uv.x, bsdf_uv.y);
+        const f3 weight = bsdf_sample_t<kType>(s.materials, s.tables, mid, ctx, rec, bsdf_uv.x, bsdf_uv.y);
         bool alive = !is_zero(weight);
         f3 new_dir = rd;
         if(alive) {
@@ -606,6 +615,69 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
     __shared__ uint32_t prefix[kKeys + 1];
     shade_wave<false>(a, depth, prefix);
 }
+
+template <int kKey>
+__global__ void __launch_bounds__(kBlock) k_shade_key(WaveArgs a, int depth) {
+    shade_wave<false, kKey>(a, depth, nullptr);
+}
+
+// the shading launches of one bounce: one kernel per key present in the scene, or the all-keys kernel
+struct ShadeLaunch {
+    uint32_t keys = 0;  // bit k: launch k_shade_key<k>; 0: launch k_shade
+    int grid[kKeys + 1] = {};
+};
+
+template <int kKey>
+const void* shade_key_kernel() {
+    return reinterpret_cast<const void*>(&k_shade_key<kKey>);
+}
+const void* shade_kernel_of(int key) {
+    switch(key) {
+    case 0: return shade_key_kernel<0>();
+    case 1: return shade_key_kernel<1>();
+    case 2: return shade_key_kernel<2>();
+    case 3: return shade_key_kernel<3>();
+    case 4: return shade_key_kernel<4>();
+    case 5: return shade_key_kernel<5>();
+    case 6: return shade_key_kernel<6>();
+    case 7: return shade_key_kernel<7>();
+    case 8: return shade_key_kernel<8>();
+    default: return shade_key_kernel<9>();
+    }
+}
+static_assert(kKeys == 10, "one shading kernel per key");
+
+ShadeLaunch shade_launch(lrt_context* ctx) {
+    ShadeLaunch l;
+    if(!ctx->shade_per_key) {
+        l.grid[kKeys] = grid_for(ctx, (const void*)k_shade, kBlock);
+        return l;
+    }
+    l.keys = ctx->shade_keys;
+    for(int k = 0; k < kKeys; ++k) {
+        if(l.keys >> k & 1u) l.grid[k] = grid_for(ctx, shade_kernel_of(k), kBlock);
+    }
+    return l;
+}
+
+void launch_shade(const ShadeLaunch& l, const WaveArgs& a, int depth, cudaStream_t st) {
+    if(!l.keys) {
+        k_shade<<<l.grid[kKeys], kBlock, 0, st>>>(a, depth);
+        return;
+    }
+    if(l.keys & (1u << 0)) k_shade_key<0><<<l.grid[0], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 1)) k_shade_key<1><<<l.grid[1], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 2)) k_shade_key<2><<<l.grid[2], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 3)) k_shade_key<3><<<l.grid[3], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 4)) k_shade_key<4><<<l.grid[4], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 5)) k_shade_key<5><<<l.grid[5], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 6)) k_shade_key<6><<<l.grid[6], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 7)) k_shade_key<7><<<l.grid[7], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 8)) k_shade_key<8><<<l.grid[8], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 9)) k_shade_key<9><<<l.grid[9], kBlock, 0, st>>>(a, depth);
+}
+
+uint32_t shade_launch_count(const ShadeLaunch& l) { return l.keys ? static_cast<uint32_t>(__builtin_popcount(l.keys)) : 1u; }
 
 __global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
     __shared__ uint32_t prefix[kKeys + 1];
@@ -884,7 +956,7 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     const int g_extend =
         grid_for(ctx, cnt ? (const void*)k_extend_persistent<true> : (const void*)k_extend_persistent<false>, kBlock);
     const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const ShadeLaunch shade = shade_launch(ctx);
     const int g_shadow =
         grid_for(ctx, cnt ? (const void*)k_shadow_persistent<true> : (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
@@ -921,7 +993,7 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
                 k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
                 record_stage(ctx, LRT_STAGE_SORT, false);
                 record_stage(ctx, LRT_STAGE_SHADE, true);
-                k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+                launch_shade(shade, a, depth, ctx->stream);
                 record_stage(ctx, LRT_STAGE_SHADE, false);
                 record_stage(ctx, LRT_STAGE_SHADOW, true);
                 if(cnt) {
@@ -930,7 +1002,7 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
                     k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
                 }
                 record_stage(ctx, LRT_STAGE_SHADOW, false);
-                launches += 4;
+                launches += 3 + shade_launch_count(shade);
             }
             record_stage(ctx, LRT_STAGE_ACCUM, true);
             k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
@@ -963,13 +1035,13 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
 
 // The launch sequence of one wave of a batch (also what the CUDA graph holds).
 void launch_batch_wave(lrt_context* ctx, const WaveArgs& a, size_t counters_bytes, int g_raygen, int g_extend,
-                       int g_hitrec, int g_shade, int g_shadow, int g_accum) {
+                       int g_hitrec, const ShadeLaunch& shade, int g_shadow, int g_accum) {
     cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream);
     k_raygen_batch<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
     for(int depth = 0; depth < a.max_depth; ++depth) {
         k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
         k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
-        k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+        launch_shade(shade, a, depth, ctx->stream);
         k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
     }
     k_accumulate_batch<<<g_accum, kBlock, 0, ctx->stream>>>(a);
@@ -1071,13 +1143,13 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
     const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
     const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
     const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const ShadeLaunch shade = shade_launch(ctx);
     const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate_batch, kBlock);
     const unsigned long long waves = (total + a.capacity - 1) / a.capacity;
-    const uint64_t per_wave = 3 + 4ull * max_depth;
+    const uint64_t per_wave = 3 + (3ull + shade_launch_count(shade)) * max_depth;
     const int rst = run_waves(ctx, waves, [&]() {
-        launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, g_shade, g_shadow, g_accum);
+        launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, shade, g_shadow, g_accum);
     });
     if(rst != LRT_OK) return rst;
     ctx->stats.paths += total;
@@ -1396,6 +1468,9 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     ds.tlas = ctx->tlas.as<float4>();
     ds.tlas_objs = ctx->tlas_objs.as<int32_t>();
     ds.n_tlas = ctx->object_bvh ? static_cast<int32_t>(h.tlas.size() / 2) : 0;
+    // shading keys a hit can carry: misses, hits without a BSDF, and 2 + each material type present
+    ctx->shade_keys = 3u;
+    for(const MatRec& m : h.materials) ctx->shade_keys |= 1u << (2 + m.type);
     ctx->scene_bytes = bytes;
     ctx->has_scene = true;
     return LRT_OK;
@@ -1619,6 +1694,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
     } else if(strcmp(name, "photon_eye_kernel") == 0) {
         if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "photon_eye_kernel must be 0, 1 or 2");
         ctx->photon_eye_kernel = static_cast<int>(value);
+    } else if(strcmp(name, "shade_per_key") == 0) {
+        ctx->shade_per_key = value != 0;
     } else if(strcmp(name, "kd_build_device") == 0) {
         if(value < 0 || value > 2) return fail(ctx, LRT_ERR_RANGE, "kd_build_device must be 0, 1 or 2");
         ctx->kd_build_device = static_cast<int>(value);
@@ -1757,7 +1834,7 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
     const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
     const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
     const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const int g_shade = grid_for(ctx, (const void*)k_shade, kBlock);
+    const ShadeLaunch shade = shade_launch(ctx);
     const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
     const uint32_t spp = p->spp;
@@ -1779,11 +1856,11 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
             for(int depth = 0; depth < p->max_depth; ++depth) {
                 k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
                 k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
-                k_shade<<<g_shade, kBlock, 0, ctx->stream>>>(a, depth);
+                launch_shade(shade, a, depth, ctx->stream);
                 k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
             }
             k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
-            launches += 2 + 4ull * p->max_depth;
+            launches += 2 + (3ull + shade_launch_count(shade)) * p->max_depth;
             LRT_CUDA(ctx, cudaGetLastError());
         }
     }

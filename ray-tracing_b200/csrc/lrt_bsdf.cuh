@@ -967,4 +967,78 @@ LRT_HD float bsdf_pdf(const MatRec* mats, const float* tables, int32_t mid, cons
     return base_pdf(m, tables, c, r, meas);
 }
 
+// The same three calls for a material whose type is known at compile time (kType >= 0; -1: the type is
+// read from the record): only that type's code is compiled in, so a kernel specialised per material
+// type holds fewer registers than one that can shade every type.
+template <int kType>
+LRT_HD f3 bsdf_sample_t(const MatRec* mats, const float* tables, int32_t mid, const BsdfCtx& c, BRec& r, float ux,
+                        float uy) {
+    const MatRec& m = mats[mid];
+    if constexpr(kType == LRT_DIFFUSE) {
+        return diffuse_sample(m, c, r, ux, uy);
+    } else if constexpr(kType == LRT_ROUGH_CONDUCTOR) {
+        return conductor_sample(m, c, r, ux, uy);
+    } else if constexpr(kType == LRT_DIELECTRIC) {
+        return dielectric_sample(m, c, r, ux, uy);
+    } else if constexpr(kType == LRT_ROUGH_DIELECTRIC) {
+        return rdiel_sample(m, c, r, ux, uy);
+    } else if constexpr(kType == LRT_PLASTIC) {
+        return plastic_sample(m, c, r, ux, uy);
+    } else if constexpr(kType == LRT_ROUGH_PLASTIC) {
+        return rplastic_sample(m, mat_table(tables, m), c, r, ux, uy);
+    } else if constexpr(kType == LRT_COATING) {
+        return coating_sample(m, mats[m.nested], tables, c, r, ux, uy);
+    } else if constexpr(kType == LRT_ROUGH_COATING) {
+        return rcoat_sample(m, mats[m.nested], tables, c, r, ux, uy);
+    } else {
+        return bsdf_sample(mats, tables, mid, c, r, ux, uy);
+    }
+}
+template <int kType>
+LRT_HD f3 bsdf_eval_t(const MatRec* mats, const float* tables, int32_t mid, const BsdfCtx& c, const BRec& r, int meas) {
+    const MatRec& m = mats[mid];
+    if constexpr(kType == LRT_DIFFUSE) {
+        return diffuse_eval(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_CONDUCTOR) {
+        return conductor_eval(m, c, r, meas);
+    } else if constexpr(kType == LRT_DIELECTRIC) {
+        return dielectric_eval(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_DIELECTRIC) {
+        return rdiel_eval(m, c, r, meas);
+    } else if constexpr(kType == LRT_PLASTIC) {
+        return plastic_eval(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_PLASTIC) {
+        return rplastic_eval(m, mat_table(tables, m), c, r, meas);
+    } else if constexpr(kType == LRT_COATING) {
+        return coating_eval(m, mats[m.nested], tables, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_COATING) {
+        return rcoat_eval(m, mats[m.nested], tables, c, r, meas);
+    } else {
+        return bsdf_eval(mats, tables, mid, c, r, meas);
+    }
+}
+template <int kType>
+LRT_HD float bsdf_pdf_t(const MatRec* mats, const float* tables, int32_t mid, const BsdfCtx& c, const BRec& r, int meas) {
+    const MatRec& m = mats[mid];
+    if constexpr(kType == LRT_DIFFUSE) {
+        return diffuse_pdf(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_CONDUCTOR) {
+        return conductor_pdf(m, c, r, meas);
+    } else if constexpr(kType == LRT_DIELECTRIC) {
+        return dielectric_pdf(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_DIELECTRIC) {
+        return rdiel_pdf(m, c, r, meas);
+    } else if constexpr(kType == LRT_PLASTIC) {
+        return plastic_pdf(m, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_PLASTIC) {
+        return rplastic_pdf(m, mat_table(tables, m), c, r, meas);
+    } else if constexpr(kType == LRT_COATING) {
+        return coating_pdf(m, mats[m.nested], tables, c, r, meas);
+    } else if constexpr(kType == LRT_ROUGH_COATING) {
+        return rcoat_pdf(m, mats[m.nested], tables, c, r, meas);
+    } else {
+        return bsdf_pdf(mats, tables, mid, c, r, meas);
+    }
+}
+
 }  // namespace lrt

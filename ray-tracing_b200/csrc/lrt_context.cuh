@@ -118,6 +118,8 @@ struct lrt_context {
     std::vector<int> event_stage;
     // photons
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
+    bool shade_per_key = true;  // one shading kernel per material type present (false: one for all)
+    uint32_t shade_keys = 3u;    // bit k: shading key k can occur in the uploaded scene
     int kd_build_device = 2;  // lrt_scene_upload's kd-trees: 0 host cores, 1 GPU, 2 GPU from 2^15 triangles
     int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
     lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L;
