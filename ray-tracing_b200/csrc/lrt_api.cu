@@ -616,9 +616,14 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs a, int depth) {
     shade_wave<false>(a, depth, prefix);
 }
 
-template <int kKey>
+__global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
+    __shared__ uint32_t prefix[kKeys + 1];
+    shade_wave<true>(a, depth, prefix);
+}
+
+template <int kKey, bool kAdj = false>
 __global__ void __launch_bounds__(kBlock) k_shade_key(WaveArgs a, int depth) {
-    shade_wave<false, kKey>(a, depth, nullptr);
+    shade_wave<kAdj, kKey>(a, depth, nullptr);
 }
 
 // the shading launches of one bounce: one kernel per key present in the scene, or the all-keys kernel
@@ -627,62 +632,60 @@ struct ShadeLaunch {
     int grid[kKeys + 1] = {};
 };
 
-template <int kKey>
-const void* shade_key_kernel() {
-    return reinterpret_cast<const void*>(&k_shade_key<kKey>);
-}
+template <bool kAdj>
 const void* shade_kernel_of(int key) {
     switch(key) {
-    case 0: return shade_key_kernel<0>();
-    case 1: return shade_key_kernel<1>();
-    case 2: return shade_key_kernel<2>();
-    case 3: return shade_key_kernel<3>();
-    case 4: return shade_key_kernel<4>();
-    case 5: return shade_key_kernel<5>();
-    case 6: return shade_key_kernel<6>();
-    case 7: return shade_key_kernel<7>();
-    case 8: return shade_key_kernel<8>();
-    default: return shade_key_kernel<9>();
+    case 0: return reinterpret_cast<const void*>(&k_shade_key<0, kAdj>);
+    case 1: return reinterpret_cast<const void*>(&k_shade_key<1, kAdj>);
+    case 2: return reinterpret_cast<const void*>(&k_shade_key<2, kAdj>);
+    case 3: return reinterpret_cast<const void*>(&k_shade_key<3, kAdj>);
+    case 4: return reinterpret_cast<const void*>(&k_shade_key<4, kAdj>);
+    case 5: return reinterpret_cast<const void*>(&k_shade_key<5, kAdj>);
+    case 6: return reinterpret_cast<const void*>(&k_shade_key<6, kAdj>);
+    case 7: return reinterpret_cast<const void*>(&k_shade_key<7, kAdj>);
+    case 8: return reinterpret_cast<const void*>(&k_shade_key<8, kAdj>);
+    default: return reinterpret_cast<const void*>(&k_shade_key<9, kAdj>);
     }
 }
 static_assert(kKeys == 10, "one shading kernel per key");
 
+template <bool kAdj = false>
 ShadeLaunch shade_launch(lrt_context* ctx) {
     ShadeLaunch l;
     if(!ctx->shade_per_key) {
-        l.grid[kKeys] = grid_for(ctx, (const void*)k_shade, kBlock);
+        l.grid[kKeys] = grid_for(ctx, kAdj ? (const void*)k_shade_adj : (const void*)k_shade, kBlock);
         return l;
     }
     l.keys = ctx->shade_keys;
     for(int k = 0; k < kKeys; ++k) {
-        if(l.keys >> k & 1u) l.grid[k] = grid_for(ctx, shade_kernel_of(k), kBlock);
+        if(l.keys >> k & 1u) l.grid[k] = grid_for(ctx, shade_kernel_of<kAdj>(k), kBlock);
     }
     return l;
 }
 
+template <bool kAdj = false>
 void launch_shade(const ShadeLaunch& l, const WaveArgs& a, int depth, cudaStream_t st) {
     if(!l.keys) {
-        k_shade<<<l.grid[kKeys], kBlock, 0, st>>>(a, depth);
+        if(kAdj) {
+            k_shade_adj<<<l.grid[kKeys], kBlock, 0, st>>>(a, depth);
+        } else {
+            k_shade<<<l.grid[kKeys], kBlock, 0, st>>>(a, depth);
+        }
         return;
     }
-    if(l.keys & (1u << 0)) k_shade_key<0><<<l.grid[0], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 1)) k_shade_key<1><<<l.grid[1], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 2)) k_shade_key<2><<<l.grid[2], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 3)) k_shade_key<3><<<l.grid[3], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 4)) k_shade_key<4><<<l.grid[4], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 5)) k_shade_key<5><<<l.grid[5], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 6)) k_shade_key<6><<<l.grid[6], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 7)) k_shade_key<7><<<l.grid[7], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 8)) k_shade_key<8><<<l.grid[8], kBlock, 0, st>>>(a, depth);
-    if(l.keys & (1u << 9)) k_shade_key<9><<<l.grid[9], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 0)) k_shade_key<0, kAdj><<<l.grid[0], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 1)) k_shade_key<1, kAdj><<<l.grid[1], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 2)) k_shade_key<2, kAdj><<<l.grid[2], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 3)) k_shade_key<3, kAdj><<<l.grid[3], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 4)) k_shade_key<4, kAdj><<<l.grid[4], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 5)) k_shade_key<5, kAdj><<<l.grid[5], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 6)) k_shade_key<6, kAdj><<<l.grid[6], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 7)) k_shade_key<7, kAdj><<<l.grid[7], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 8)) k_shade_key<8, kAdj><<<l.grid[8], kBlock, 0, st>>>(a, depth);
+    if(l.keys & (1u << 9)) k_shade_key<9, kAdj><<<l.grid[9], kBlock, 0, st>>>(a, depth);
 }
 
 uint32_t shade_launch_count(const ShadeLaunch& l) { return l.keys ? static_cast<uint32_t>(__builtin_popcount(l.keys)) : 1u; }
-
-__global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
-    __shared__ uint32_t prefix[kKeys + 1];
-    shade_wave<true>(a, depth, prefix);
-}
 
 // adjoint: the NEE derivatives of the shadow rays of one depth that reached their light
 __global__ void __launch_bounds__(kBlock) k_adj_nee(WaveArgs a, int depth) {
@@ -1191,7 +1194,7 @@ int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigne
     const int g_raygen = grid_for(ctx, (const void*)k_raygen_batch, kBlock);
     const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
     const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const int g_shade = grid_for(ctx, (const void*)k_shade_adj, kBlock);
+    const ShadeLaunch shade = shade_launch<true>(ctx);
     const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false, true>, kBlock);
     const int g_nee = grid_for(ctx, (const void*)k_adj_nee, kBlock);
     const int g_suffix = grid_for(ctx, (const void*)k_adj_suffix, kBlock);
@@ -1204,7 +1207,7 @@ int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigne
         for(int depth = 0; depth < max_depth; ++depth) {
             k_extend_persistent<false><<<g_extend, kBlock, 0, sm>>>(a, depth);
             k_hitrec<<<g_hitrec, kBlock, 0, sm>>>(a, depth);
-            k_shade_adj<<<g_shade, kBlock, 0, sm>>>(a, depth);
+            launch_shade<true>(shade, a, depth, sm);
             k_shadow_persistent<false, true><<<g_shadow, kBlock, 0, sm>>>(a, depth);
             k_adj_nee<<<g_nee, kBlock, 0, sm>>>(a, depth);
         }
@@ -1213,7 +1216,7 @@ int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigne
     });
     if(rst != LRT_OK) return rst;
     ctx->stats.paths += total;
-    ctx->stats.kernel_launches += waves * (3 + 5ull * max_depth);
+    ctx->stats.kernel_launches += waves * (3 + (4ull + shade_launch_count(shade)) * max_depth);
     return LRT_OK;
 }
 
