@@ -5,7 +5,9 @@
 render (default): `frames` frames of one open-box scene (the benchmark geometry), then the last frame
   again with work counting on, printing the extension rays of every bounce of that frame, so that DRAM
   bytes an ncu capture reports for one k_extend launch can be divided by the rays it traced. One frame
-  at 512x512x4 spp is one wave of 1M paths: max_depth x 3 + 2 launches, about 0.5 GB of device memory.
+  at 512x512x4 spp is one wave of 1M paths: raygen and accumulate, and per bounce extend, hit records,
+  shadow and one shading kernel per shading key present (three here: misses, the diffuse walls, the
+  sphere's material); about 0.5 GB of device memory.
   With the defaults, k_extend launch number 9 (0-based, `ncu -k regex:k_extend -s 9 -c 1`) is bounce 1
   of the last frame.
 eye: the large photon-mapping scene (256 level-5 spheres, 5.24M triangles), `photons` photons, one
