@@ -1,6 +1,6 @@
 """Small, fixed cases for profiler captures (ncu) of the library's kernels.
 
-    python ray-tracing_b200/profile_case.py [--case render|eye|adjoint|batch] [options]
+    python ray-tracing_b200/profile_case.py [--case render|eye|adjoint|batch|kdbuild] [options]
 
 render (default): `frames` frames of one open-box scene (the benchmark geometry), then the last frame
   again with work counting on, printing the extension rays of every bounce of that frame, so that DRAM
