@@ -1363,6 +1363,11 @@ int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t*
                             uint64_t* total_nodes, uint64_t* total_refs) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     if((n_meshes && !counts) || !total_nodes || !total_refs) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null argument");
+    if(n_meshes == 0) {  // nothing to build, nothing written
+        *total_nodes = 0;
+        *total_refs = 0;
+        return LRT_OK;
+    }
     LRT_CUDA(ctx, cudaSetDevice(ctx->device));
     uint64_t n = 0;
     for(uint32_t m = 0; m < n_meshes; ++m) {
