@@ -31,6 +31,16 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, name), name
 
 
+def test_null_context_is_rejected_without_cuda():
+    """entry points that take a context check it before any CUDA call (no GPU needed here)"""
+    L = lrt.lib()
+    tn, tr = C.c_uint64(7), C.c_uint64(7)
+    assert L.lrt_kdtree_build_device(None, 0, None, None, None, None, 0, None, 0, None, None, None,
+                                     C.byref(tn), C.byref(tr)) == -1
+    cfg = abi.LaunchConfig()
+    assert L.lrt_autotune(None, None, 0, 8, 3, None, None, C.byref(cfg)) == -1
+
+
 def test_status_strings():
     L = lrt.lib()
     L.lrt_status_string.restype = C.c_char_p
