@@ -28,6 +28,8 @@
  *   lrt_photon_irradiance       photon_map::estimate_irradiance src/integrator/photonmapper/photon_map.h:38-70
  *   lrt_rough_transmittance_slice  rough_transmittance ctor src/material/func/rough_transmittance.h:15-24,67-185
  *   lrt_fresnel_diffuse_reflectance fresnel_diffuse_reflectance src/material/func/fresnel.h:128-133
+ *   lrt_hosek_state             env_emitter ctor src/emitter/env_emitter.h:13-30 -> arhosek_rgb_skymodelstate_alloc_init
+ *                               third_party/hosek/ArHosekSkyModel.cc:602-635
  */
 #ifndef LRT_H
 #define LRT_H
@@ -145,7 +147,8 @@ typedef struct lrt_object_desc {
 /*
  * Emitter description. For LRT_EMITTER_ENV, hosek_config/hosek_radiance are the RGB model state
  * (ArHosekSkyModelState configs[0..2] and radiances[0..2]) cooked by
- * arhosek_rgb_skymodelstate_alloc_init(turbidity, albedo, asin(normalize(sun_direction).y)).
+ * arhosek_rgb_skymodelstate_alloc_init(turbidity, albedo, asin(normalize(sun_direction).y)); left all
+ * zero, the upload cooks it from sun_direction, turbidity and albedo (lrt_hosek_state).
  */
 typedef struct lrt_emitter_desc {
     int32_t kind;
@@ -280,6 +283,15 @@ const char* lrt_status_string(int status);
 int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha,
                                   float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
 float lrt_fresnel_diffuse_reflectance(float eta);
+/* The Hosek-Wilkie RGB sky state of env_emitter's constructor (src/emitter/env_emitter.h:13-30:
+ * elevation = asin(normalize(sun_direction).y) in float, then arhosek_rgb_skymodelstate_alloc_init,
+ * third_party/hosek/ArHosekSkyModel.cc:602-635, in double): config = configs[0..2][0..8] (27 doubles),
+ * radiance = radiances[0..2]; bit-identical to the reference. The model's tables cover turbidity
+ * 1..10 and ground albedo 0..1: other values give LRT_ERR_RANGE (the reference reads outside its
+ * tables there). lrt_scene_upload cooks the state itself when an env emitter's hosek_config is all
+ * zero. */
+int lrt_hosek_state(const float* sun_direction /* 3 */, float turbidity, float albedo, double* config /* 27 */,
+                    double* radiance /* 3 */);
 /* The same table in two steps, so that a caller without ggx.dat can re-slice for any alpha: the eta
  * slice (set_eta, rough_transmittance.h:129-167) = n_alpha x LRT_TRANS_SAMPLES transmittance values
  * (alpha-major) and n_alpha diffuse values, with the file's alpha range; then set_alpha on it

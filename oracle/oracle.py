@@ -21,19 +21,17 @@ REF_LIB = os.path.join(REF_DIR, "liblrt_ref.so")
 GGX_PATH = os.path.join(REF_DIR, "third_party", "data", "ggx.dat")
 RESTATEMENT_LIB = os.path.join(ORACLE_DIR, "build", "liblrt_oracle.so")
 
-_ref = None
+_ref = {}
+TIMING_LIBS = {v: os.path.join(REF_DIR, "liblrt_ref_timing_%s.so" % v) for v in ("v3", "v4")}
 
 
 def reference_available() -> bool:
     return os.path.exists(REF_LIB) and os.path.exists(GGX_PATH)
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        if not reference_available():
-            raise FileNotFoundError("reference oracle not built: run `make -C oracle ref` (needs the reference sources)")
-        lib = C.CDLL(REF_LIB)
+def _load(path):
+    if True:
+        lib = C.CDLL(path)
         vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int32, C.c_float
         P = C.POINTER
         lib.ref_last_error.restype = C.c_char_p
@@ -52,6 +50,8 @@ def ref_lib():
         lib.ref_camera_rays.argtypes = [vp, u32, u32, P(u32), u32, P(abi.Ray)]
         lib.ref_render.restype = C.c_double
         lib.ref_render.argtypes = [vp, P(abi.RenderParams), u32, P(f32), P(f32)]
+        lib.ref_render_window.restype = C.c_double
+        lib.ref_render_window.argtypes = [vp, P(abi.RenderParams), u32, u32, u32, P(f32), P(f32)]
         lib.ref_photon_render.restype = C.c_double
         lib.ref_photon_render.argtypes = [vp, P(abi.RenderParams), u32, P(abi.Photon), u32, f32, P(abi.Photon), u32, f32,
                                           P(abi.PhotonRenderParams), P(f32), P(f32)]
@@ -71,8 +71,47 @@ def ref_lib():
         lib.ref_fresnel_diffuse_reflectance.argtypes = [f32]
         lib.ref_hosek_state.argtypes = [P(f32), f32, f32, P(C.c_double), P(C.c_double)]
         lib.ref_hardware_concurrency.restype = u32
-        _ref = lib
-    return _ref
+        return lib
+
+
+def ref_lib(timing: bool = False):
+    """The parity build (timing=False: -O2/-O3 -ffp-contract=off, the reference's own arithmetic), or
+    the timing build for this host (timing=True: -O3 for the widest x86-64 level its CPU supports,
+    with GCC's default contraction), falling back to the parity build when none was made."""
+    global _ref
+    if not reference_available():
+        raise FileNotFoundError("reference oracle not built: run `make -C oracle ref` (needs the reference sources)")
+    key = timing_variant() if timing else "parity"
+    if key not in _ref:
+        _ref[key] = _load(TIMING_LIBS.get(key, REF_LIB))
+    return _ref[key]
+
+
+def cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def timing_variant() -> str:
+    """'v4' (AVX-512), 'v3' (AVX2 + FMA) or 'parity': the widest timing build this host can run"""
+    flags = cpu_flags()
+    v3 = {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "abm", "movbe", "xsave"}
+    v4 = v3 | {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}
+    for name, need in (("v4", v4), ("v3", v3)):
+        if need <= flags and os.path.exists(TIMING_LIBS[name]):
+            return name
+    return "parity"
+
+
+def timing_build_flags() -> str:
+    v = timing_variant()
+    return "-O3 -ffp-contract=off (parity build)" if v == "parity" else "-O3 -march=x86-64-%s" % v
 
 
 def _p(a, t=C.c_float):
@@ -82,16 +121,17 @@ def _p(a, t=C.c_float):
 class RefWorld:
     """Reference objects built from the same scene description as the GPU library."""
 
-    def __init__(self, scene):
+    def __init__(self, scene, timing: bool = False):
+        """timing=True: the timing build (the CPU baseline); otherwise the parity build."""
         self.holder = abi.SceneHolder(scene)
-        lib = ref_lib()
-        self.handle = lib.ref_world_create(C.byref(self.holder.desc), REF_DIR.encode())
+        self.lib = ref_lib(timing)
+        self.handle = self.lib.ref_world_create(C.byref(self.holder.desc), REF_DIR.encode())
         if not self.handle:
-            raise RuntimeError("reference scene construction failed: %s" % lib.ref_last_error().decode())
+            raise RuntimeError("reference scene construction failed: %s" % self.lib.ref_last_error().decode())
 
     def close(self):
         if self.handle:
-            ref_lib().ref_world_destroy(self.handle)
+            self.lib.ref_world_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -104,51 +144,59 @@ class RefWorld:
         rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
         hits = np.zeros(len(rays), dtype=abi.HIT_DTYPE)
         tests = C.c_uint64(0)
-        mism = ref_lib().ref_trace(self.handle, _p(rays, abi.Ray), len(rays), _p(hits, abi.Hit), C.byref(tests))
+        mism = self.lib.ref_trace(self.handle, _p(rays, abi.Ray), len(rays), _p(hits, abi.Hit), C.byref(tests))
         assert mism == 0, "harness object loop disagrees with scene::hit on %d rays" % mism
         return hits, tests.value
 
     def bsdf(self, material: int, queries: np.ndarray):
         queries = np.ascontiguousarray(queries, dtype=abi.BSDF_QUERY_DTYPE)
         out = np.zeros(len(queries), dtype=abi.BSDF_RESULT_DTYPE)
-        ref_lib().ref_bsdf_query(self.handle, material, _p(queries, abi.BsdfQuery), len(queries),
+        self.lib.ref_bsdf_query(self.handle, material, _p(queries, abi.BsdfQuery), len(queries),
                                  _p(out, abi.BsdfResult))
         return out
 
     def bsdf_flags(self, material: int) -> int:
-        return ref_lib().ref_bsdf_flags(self.handle, material)
+        return self.lib.ref_bsdf_flags(self.handle, material)
 
     def sky(self, dirs: np.ndarray):
         dirs = np.ascontiguousarray(dirs, dtype=np.float32)
         out = np.zeros((len(dirs), 3), dtype=np.float32)
-        ref_lib().ref_sky_eval(self.handle, _p(dirs), len(dirs), _p(out))
+        self.lib.ref_sky_eval(self.handle, _p(dirs), len(dirs), _p(out))
         return out
 
     def emitter_sample(self, points, u2):
         points = np.ascontiguousarray(points, dtype=np.float32)
         u2 = np.ascontiguousarray(u2, dtype=np.float32)
         out = np.zeros((len(points), 16), dtype=np.float32)
-        ref_lib().ref_emitter_sample(self.handle, _p(points), _p(u2), len(points), _p(out))
+        self.lib.ref_emitter_sample(self.handle, _p(points), _p(u2), len(points), _p(out))
         return out
 
     def emitter_pdf(self, points, dirs):
         points = np.ascontiguousarray(points, dtype=np.float32)
         dirs = np.ascontiguousarray(dirs, dtype=np.float32)
         out = np.zeros(len(points), dtype=np.float32)
-        ref_lib().ref_emitter_pdf(self.handle, _p(points), _p(dirs), len(points), _p(out))
+        self.lib.ref_emitter_pdf(self.handle, _p(points), _p(dirs), len(points), _p(out))
         return out
 
     def camera_rays(self, width, height, pixel_sample):
         ps = np.ascontiguousarray(pixel_sample, dtype=np.uint32)
         rays = np.zeros(len(ps), dtype=abi.RAY_DTYPE)
-        ref_lib().ref_camera_rays(self.handle, width, height, _p(ps, C.c_uint32), len(ps), _p(rays, abi.Ray))
+        self.lib.ref_camera_rays(self.handle, width, height, _p(ps, C.c_uint32), len(ps), _p(rays, abi.Ray))
         return rays
 
     def render(self, params: abi.RenderParams, threads: int = 0, want_sq: bool = False):
         img = np.zeros((params.height, params.width, 3), dtype=np.float32)
         sq = np.zeros_like(img) if want_sq else None
-        secs = ref_lib().ref_render(self.handle, C.byref(params), threads, _p(img),
+        secs = self.lib.ref_render(self.handle, C.byref(params), threads, _p(img),
                                     _p(sq) if sq is not None else None)
+        return img, sq, secs
+
+    def render_window(self, params: abi.RenderParams, col_begin: int, col_end: int, threads: int = 0):
+        """Mean and mean of squares over rows [row_begin, row_end) x columns [col_begin, col_end) of the
+        full frame (the crop of a render, pixel for pixel); the image arrays are full-frame sized."""
+        img = np.zeros((params.height, params.width, 3), dtype=np.float32)
+        sq = np.zeros_like(img)
+        secs = self.lib.ref_render_window(self.handle, C.byref(params), col_begin, col_end, threads, _p(img), _p(sq))
         return img, sq, secs
 
     def render_photon(self, params, pp, global_photons, global_scale, caustic_photons, caustic_scale, threads=0,
@@ -158,7 +206,7 @@ class RefWorld:
         c = np.ascontiguousarray(caustic_photons, dtype=abi.PHOTON_DTYPE)
         img = np.zeros((params.height, params.width, 3), dtype=np.float32)
         sq = np.zeros_like(img) if want_sq else None
-        secs = ref_lib().ref_photon_render(self.handle, C.byref(params), threads, _p(g, abi.Photon) if len(g) else None,
+        secs = self.lib.ref_photon_render(self.handle, C.byref(params), threads, _p(g, abi.Photon) if len(g) else None,
                                            len(g), global_scale, _p(c, abi.Photon) if len(c) else None, len(c),
                                            caustic_scale, C.byref(pp), _p(img), _p(sq) if sq is not None else None)
         return img, sq, secs
@@ -166,7 +214,7 @@ class RefWorld:
     def trace_particles(self, kind, first, count, max_depth, rr_depth, max_per=64):
         photons = np.zeros(count * max_per, dtype=abi.PHOTON_DTYPE)
         counts = np.zeros(count, dtype=np.uint32)
-        ref_lib().ref_trace_particles(self.handle, kind, first, count, max_depth, rr_depth, max_per,
+        self.lib.ref_trace_particles(self.handle, kind, first, count, max_depth, rr_depth, max_per,
                                       _p(photons, abi.Photon), _p(counts, C.c_uint32))
         return photons.reshape(count, max_per), counts
 
@@ -174,7 +222,7 @@ class RefWorld:
         photons = np.zeros(requested, dtype=abi.PHOTON_DTYPE)
         shot = C.c_uint64(0)
         secs = C.c_double(0)
-        n = ref_lib().ref_photon_gather(self.handle, kind, requested, max_depth, rr_depth,
+        n = self.lib.ref_photon_gather(self.handle, kind, requested, max_depth, rr_depth,
                                         _p(photons, abi.Photon), C.byref(shot), C.byref(secs))
         return photons[:n], shot.value, secs.value
 

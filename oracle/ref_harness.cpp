@@ -216,11 +216,15 @@ struct ref_photon_map {
 // The tile loop of src/main.cpp:103-147 (32x32 tiles on a thread_pool of `threads` workers) around
 // `radiance(ray, sampler)`. rgb = per-pixel mean; rgb_sq (optional) = per-pixel mean of squares. Returns
 // the wall-clock seconds of the tile loop (steady_clock, as main.cpp:103,148).
+// Columns [col_begin, col_end) only when col_end > col_begin (a crop window of the full frame: the camera
+// and pixel indices are those of the whole image).
 template <typename Radiance>
 double render_tiles(const ref_world& w, const lrt_render_params* p, uint32_t threads, float* rgb, float* rgb_sq,
-                    Radiance&& radiance) {
+                    Radiance&& radiance, uint32_t col_begin = 0, uint32_t col_end = 0) {
     const int width = static_cast<int>(p->width);
     const int height = static_cast<int>(p->height);
+    const int x_begin = col_end > col_begin ? static_cast<int>(col_begin) : 0;
+    const int x_end = col_end > col_begin ? static_cast<int>(std::min<uint32_t>(col_end, p->width)) : width;
     const int row_begin = p->row_end > p->row_begin ? static_cast<int>(p->row_begin) : 0;
     const int row_end = p->row_end > p->row_begin ? static_cast<int>(p->row_end) : height;
     const int spp = static_cast<int>(p->spp);
@@ -229,8 +233,8 @@ double render_tiles(const ref_world& w, const lrt_render_params* p, uint32_t thr
     {
         thread_pool pool(threads == 0 ? std::thread::hardware_concurrency() : threads);
         for(int y0 = row_begin; y0 < row_end; y0 += tile) {
-            for(int x0 = 0; x0 < width; x0 += tile) {
-                const int x1 = std::min(x0 + tile, width);
+            for(int x0 = x_begin; x0 < x_end; x0 += tile) {
+                const int x1 = std::min(x0 + tile, x_end);
                 const int y1 = std::min(y0 + tile, row_end);
                 pool.submit([&, x0, y0, x1, y1] {
                     for(int y = y0; y < y1; ++y) {
@@ -477,6 +481,18 @@ double ref_render(void* handle, const lrt_render_params* p, uint32_t threads, fl
     const path_integrator integrator;
     return render_tiles(w, p, threads, rgb, rgb_sq,
                         [&](ray& r, sampler& smp) { return integrator.radiance(r, *w.world, smp); });
+}
+
+// The same over a window of columns (rows from p): the crop of a large frame, pixel for pixel.
+double ref_render_window(void* handle, const lrt_render_params* p, uint32_t col_begin, uint32_t col_end,
+                         uint32_t threads, float* rgb, float* rgb_sq) {
+    const auto& w = *static_cast<ref_world*>(handle);
+    lrt_ref_max_depth = p->max_depth;
+    lrt_ref_rr_depth = p->rr_depth;
+    const path_integrator integrator;
+    return render_tiles(
+        w, p, threads, rgb, rgb_sq, [&](ray& r, sampler& smp) { return integrator.radiance(r, *w.world, smp); },
+        col_begin, col_end);
 }
 
 // Photon-mapper image: photon_integrator::radiance with the given photon maps (built by

@@ -375,13 +375,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
                 const Ray r{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}};
                 bool any_mode = true;
                 const EmitRec& e = a.s.emitters[light];
-                if(e.kind == LRT_EMITTER_AREA) {
-                    const ObjRec& lo = a.s.objects[e.object];
-                    float t;
-                    f3 p;
-                    any_mode = !(lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, r, 0.001f, o.w, t, p)
-                                                                : hit_sphere(lo, r, 0.001f, o.w, t));
-                }
+                if(e.kind == LRT_EMITTER_AREA) any_mode = !light_shape_reachable(a.s, a.s.objects[e.object], r, 0.001f, o.w);
                 trav_begin(st, r, 0.001f, o.w, any_mode);
                 active = true;
                 ++rays;
@@ -1292,6 +1286,19 @@ int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha, 
 
 float lrt_fresnel_diffuse_reflectance(float eta) { return fresnel_diffuse_reflectance(eta); }
 
+int lrt_hosek_state(const float* sun_direction, float turbidity, float albedo, double* config, double* radiance) {
+    if(!sun_direction || !config || !radiance) return LRT_ERR_INVALID_ARGUMENT;
+    std::string err;
+    double cfg[3][9], rad[3];
+    const int st = hosek_state(sun_direction, turbidity, albedo, cfg, rad, err);
+    if(st != LRT_OK) return st;
+    for(int c = 0; c < 3; ++c) {
+        for(int k = 0; k < 9; ++k) config[9 * c + k] = cfg[c][k];
+        radiance[c] = rad[c];
+    }
+    return LRT_OK;
+}
+
 int lrt_load_obj(const char* path, uint32_t* n_vertices, uint32_t* n_indices, float* positions,
                  uint32_t vertex_capacity, uint32_t* indices, float* corner_normals, uint32_t index_capacity) {
     if(!path || !n_vertices || !n_indices) return LRT_ERR_INVALID_ARGUMENT;
@@ -1451,6 +1458,8 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     LRT_CUDA(ctx, upload(ctx->emission, emission, s, bytes));
     LRT_CUDA(ctx, upload(ctx->tlas, h.tlas, s, bytes));
     LRT_CUDA(ctx, upload(ctx->tlas_objs, h.tlas_objs, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->light_cdf, h.light_cdf, s, bytes));
+    LRT_CUDA(ctx, upload(ctx->light_tri, h.light_tri, s, bytes));
     LRT_CUDA(ctx, cudaStreamSynchronize(s));
     DeviceScene& ds = ctx->ds;
     ds.nodes = ctx->nodes.as<uint2>();
@@ -1464,6 +1473,8 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     ds.sobol = ctx->sobol.as<uint32_t>();
     ds.emission_cdf = ctx->emission.as<float>();
     ds.emission_index = reinterpret_cast<const int32_t*>(ctx->emission.as<float>() + h.emission_cdf.size());
+    ds.light_cdf = ctx->light_cdf.as<float>();
+    ds.light_tri = ctx->light_tri.as<float4>();
     ds.n_objects = static_cast<int32_t>(h.objects.size());
     ds.n_materials = static_cast<int32_t>(h.materials.size());
     ds.n_emitters = static_cast<int32_t>(h.emitters.size());

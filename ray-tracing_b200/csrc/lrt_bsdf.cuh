@@ -73,8 +73,10 @@ LRT_HD f3 ggx_sample(float alpha, f3 wi, float ux, float uy) {
     const f3 t2 = cross(vh, t1);
     const float r = sqrtf(ux);
     const float phi = 2.0f * kPi * uy;
-    const float disk_x = r * cosf(phi);
-    float disk_y = r * sinf(phi);
+    float sin_phi, cos_phi;
+    sincos_rn(phi, sin_phi, cos_phi);
+    const float disk_x = r * cos_phi;
+    float disk_y = r * sin_phi;
     const float stretch = 0.5f * (1.0f + vh.z);
     disk_y = (1.0f - stretch) * sqrtf(smax(0.0f, 1.0f - disk_x * disk_x)) + stretch * disk_y;
     const f3 nh = disk_x * t1 + disk_y * t2 + sqrtf(smax(0.0f, 1.0f - disk_x * disk_x - disk_y * disk_y)) * vh;
@@ -187,7 +189,7 @@ LRT_HD float cubic_interp_1d(float x, const float* values, uint32_t size) {
 }
 LRT_HD float trans_eval(const float* table, float cos_theta) {
     if(!(cos_theta >= 0.0f)) return 0.0f;
-    const float warped = powf(cos_theta, 0.25f);
+    const float warped = quartic_root_rn(cos_theta);
     return sclamp(cubic_interp_1d(warped, table, LRT_TRANS_SAMPLES), 0.0f, 1.0f);
 }
 
@@ -196,7 +198,9 @@ LRT_HD f3 cosine_hemisphere(float ux, float uy, float& pdf) {
     const float sin_theta = sqrtf(1.0f - ux);
     const float phi = 2.0f * kPi * uy;
     pdf = cos_theta / kPi;
-    return f3{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    float sin_phi, cos_phi;
+    sincos_rn(phi, sin_phi, cos_phi);
+    return f3{cos_phi * sin_theta, sin_phi * sin_theta, cos_theta};
 }
 
 LRT_HD void rec_reset(BRec& r) {
@@ -216,7 +220,9 @@ LRT_HD f3 diffuse_sample(const MatRec& m, const BsdfCtx& c, BRec& r, float ux, f
     const float cos_theta = sqrtf(ux);
     const float sin_theta = sqrtf(1.0f - ux);
     const float phi = 2.0f * kPi * uy;
-    r.wo = f3{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    float sin_phi, cos_phi;
+    sincos_rn(phi, sin_phi, cos_phi);
+    r.wo = f3{cos_phi * sin_theta, sin_phi * sin_theta, cos_theta};
     r.pdf = cos_theta / kPi;
     r.sampled_type = lobe;
     r.sampled_component = 0;
@@ -710,7 +716,7 @@ LRT_HD f3 coating_absorption(const MatRec& m, f3 wi_inner, f3 wo_inner) {
     if(m.sigma_zero) return mk(1.0f);
     const float path_length = (1.0f / fabsf(wi_inner.z)) + (1.0f / fabsf(wo_inner.z));
     const f3 exponent = load3(m.sigma_a) * (-m.thickness * path_length);
-    return f3{expf(exponent.x), expf(exponent.y), expf(exponent.z)};
+    return f3{exp_rn(exponent.x), exp_rn(exponent.y), exp_rn(exponent.z)};
 }
 LRT_HD float coating_specular_probability(float reflectance, float ssw) {
     const float specular = reflectance * ssw;

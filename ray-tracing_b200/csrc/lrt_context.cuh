@@ -93,6 +93,7 @@ struct lrt_context {
     lrt::HostScene host;
     lrt::DeviceScene ds{};
     lrt::DevBuf nodes, tris, ref_prim, normals, objects, materials, tables, emitters, emission, sobol, tlas, tlas_objs;
+    lrt::DevBuf light_cdf, light_tri;
     bool object_bvh = true;  // false: walk the object list in order even where a hierarchy was built
     uint64_t scene_bytes = 0;
     // render

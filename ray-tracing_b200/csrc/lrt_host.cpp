@@ -741,6 +741,77 @@ float fresnel_diffuse_reflectance(float eta) {
     return q.integrate([eta](float xi) { return fresnel_ext_host(sqrtf(xi), eta); }, 0.0f, 1.0f);
 }
 
+// ---- Hosek-Wilkie RGB sky state ----
+#include "lrt_hosek_rgb.inc"
+
+namespace {
+
+// The model's quintic Bernstein blend over its six elevation control points c[0], c[step], ..., c[5 step]
+// at the warped elevation s, B_k(s) = C(5,k) (1-s)^(5-k) s^k, each term multiplied and the terms summed
+// in the order ArHosekSkyModel_CookConfiguration writes them (ArHosekSkyModel.cc:164-171) so that the
+// double result is the reference's bit for bit.
+double hosek_bernstein(const double* c, int step, double s) {
+    const double r = 1.0 - s;
+    return pow(r, 5.0) * c[0] + 5.0 * pow(r, 4.0) * s * c[step] + 10.0 * pow(r, 3.0) * pow(s, 2.0) * c[2 * step] +
+           10.0 * pow(r, 2.0) * pow(s, 3.0) * c[3 * step] + 5.0 * r * pow(s, 4.0) * c[4 * step] +
+           pow(s, 5.0) * c[5 * step];
+}
+
+// One channel: bilinear in (ground albedo 0/1, integer turbidity t/t+1) over the tables of `per` values
+// per (albedo, turbidity) cell, each cell the Bernstein blend over elevation; `count` outputs.
+void hosek_cook(const double* table, int per, int count, double turbidity, double albedo, double elevation,
+                double* out) {
+    const int t = static_cast<int>(turbidity);
+    const double t_rem = turbidity - static_cast<double>(t);
+    const double s = pow(elevation / (3.141592653589793 / 2.0), 1.0 / 3.0);
+    const int stride = 6 * per;  // one (albedo, turbidity) cell: 6 control points x `per` values
+    // cells in the reference's accumulation order: (albedo 0, t), (albedo 1, t), then -- below
+    // turbidity 10 -- (albedo 0, t + 1), (albedo 1, t + 1)
+    struct Cell {
+        int albedo_side, turbidity;
+        double weight;
+    };
+    const Cell cells[4] = {{0, t, (1.0 - albedo) * (1.0 - t_rem)},
+                           {1, t, albedo * (1.0 - t_rem)},
+                           {0, t + 1, (1.0 - albedo) * t_rem},
+                           {1, t + 1, albedo * t_rem}};
+    const int n_cells = t == 10 ? 2 : 4;
+    for(int k = 0; k < n_cells; ++k) {
+        const double* cell = table + cells[k].albedo_side * 10 * stride + (cells[k].turbidity - 1) * stride;
+        for(int i = 0; i < count; ++i) {
+            const double v = cells[k].weight * hosek_bernstein(cell + i, per, s);
+            out[i] = k == 0 ? v : out[i] + v;
+        }
+    }
+}
+
+}  // namespace
+
+int hosek_state(const float sun_direction[3], float turbidity, float albedo, double config[3][9], double radiance[3],
+                std::string& error) {
+    if(!(turbidity >= 1.0f && turbidity <= 10.0f)) {
+        error = "turbidity must lie in [1, 10] (the model's table range)";
+        return LRT_ERR_RANGE;
+    }
+    if(!(albedo >= 0.0f && albedo <= 1.0f)) {
+        error = "ground albedo must lie in [0, 1]";
+        return LRT_ERR_RANGE;
+    }
+    const f3 d = load3(sun_direction);
+    if(!(length_squared(d) > 0.0f)) {
+        error = "sun direction must be non-zero";
+        return LRT_ERR_INVALID_ARGUMENT;
+    }
+    // env_emitter.h:14,28: the direction normalised in float, elevation = asin(clamp(y, -1, 1)) in float
+    const f3 sun = normalize(d);
+    const float elevation = asinf(sclamp(sun.y, -1.0f, 1.0f));
+    for(int c = 0; c < 3; ++c) {
+        hosek_cook(kHosekRgb[c], 9, 9, turbidity, albedo, elevation, config[c]);
+        hosek_cook(kHosekRgbRad[c], 1, 1, turbidity, albedo, elevation, &radiance[c]);
+    }
+    return LRT_OK;
+}
+
 // Sobol direction numbers: dimension 0 is the van der Corput sequence, dimensions 1..15 come from
 // the primitive polynomials and initial direction numbers of Joe & Kuo (new-joe-kuo-6.21201,
 // dimensions 2..16), the table src/core/sobol.h:51-69 also uses.
@@ -1274,8 +1345,22 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
             }
             const ObjRec& o = s.objects[e.object];
             if(o.kind == LRT_OBJECT_MESH) {
-                err = "emitter " + std::to_string(i) + ": area lights over triangle meshes are not supported";
-                return LRT_ERR_INVALID_ARGUMENT;
+                // triangle_mesh ctor (triangle_mesh.h:14-28): the area CDF summed triangle by triangle in
+                // float, the same sum that gives the mesh's area
+                const lrt_object_desc& od = d->objects[e.object];
+                r.tri_first = static_cast<uint32_t>(s.light_cdf.size());
+                r.n_tris = od.n_indices / 3;
+                float running = 0.0f;
+                for(uint32_t t = 0; t < r.n_tris; ++t) {
+                    const f3 p0 = load3(od.positions + 3ull * od.indices[3 * t]);
+                    const f3 p1 = load3(od.positions + 3ull * od.indices[3 * t + 1]);
+                    const f3 p2 = load3(od.positions + 3ull * od.indices[3 * t + 2]);
+                    running += 0.5f * length(cross(p1 - p0, p2 - p0));
+                    s.light_cdf.push_back(running);
+                    s.light_tri.push_back(float4{p0.x, p0.y, p0.z, 0.0f});
+                    s.light_tri.push_back(float4{p1.x, p1.y, p1.z, 0.0f});
+                    s.light_tri.push_back(float4{p2.x, p2.y, p2.z, 0.0f});
+                }
             }
             r.object = e.object;
             r.shape = o.kind;
@@ -1312,9 +1397,13 @@ int build_host_scene(const lrt_scene_desc* d, HostScene& s, std::string& err, co
                 }
                 r.rad[c] = e.hosek_radiance[c];
             }
-            if(!any) {
-                err = "emitter " + std::to_string(i) + ": Hosek state is empty";
-                return LRT_ERR_INVALID_ARGUMENT;
+            if(!any) {  // no state given: cook it from (sun direction, turbidity, albedo) as env_emitter does
+                std::string cook_err;
+                const int st = hosek_state(e.sun_direction, e.turbidity, e.albedo, r.cfg, r.rad, cook_err);
+                if(st != LRT_OK) {
+                    err = "emitter " + std::to_string(i) + ": " + cook_err;
+                    return st;
+                }
             }
             ++s.n_infinite;
         } else {

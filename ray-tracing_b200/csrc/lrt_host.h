@@ -60,6 +60,9 @@ struct HostScene {
     std::vector<float> emission_cdf;
     std::vector<int32_t> emission_index;
     float emission_power = 0.0f;
+    // area lights over meshes: per triangle the running area sum and the corner positions
+    std::vector<float> light_cdf;
+    std::vector<float4> light_tri;
     float bounding_radius = 0.0f;  // scene::bounding_sphere_radius (scene.h:41-45)
     bool has_delta_bsdf = false;   // scene::has_delta_bsdf (scene.h:48-57)
     // meshes of more than 64 triangles, largest first; queue segmentation is off when there are > 4
@@ -123,6 +126,11 @@ int rough_transmittance_alpha(const float* sliced_t, const float* sliced_d, uint
                               float alpha_max, float alpha, float* table, float* diffuse, std::string& error);
 int rough_transmittance_slice(const char* path, float eta, float alpha, float* table, float* diffuse, std::string& error);
 float fresnel_diffuse_reflectance(float eta);
+// The Hosek-Wilkie RGB sky state env_emitter's constructor cooks (src/emitter/env_emitter.h:13-30 ->
+// arhosek_rgb_skymodelstate_alloc_init, third_party/hosek/ArHosekSkyModel.cc:602-635): per channel the
+// nine radiance-distribution coefficients and the radiance scale, bit-identical to the reference.
+int hosek_state(const float sun_direction[3], float turbidity, float albedo, double config[3][9], double radiance[3],
+                std::string& error);
 void sobol_direction_table(uint32_t table[16][32]);
 
 }  // namespace lrt

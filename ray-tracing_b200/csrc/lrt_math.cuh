@@ -63,6 +63,36 @@ LRT_HD float max3(f3 v) {  // std::max({r, g, b})
 }
 LRT_HD float signum(float v) { return static_cast<float>((v > 0.0f) - (v < 0.0f)); }
 
+// Single-precision sin/cos, x^(1/4) (the reference's powf(x, 0.25f)), exp and acos as the reference's
+// libm returns them. glibc's float versions (sinf/cosf/powf/expf, under 0.6-0.9 ulp) give the correctly
+// rounded result for nearly every argument; CUDA's float versions are within 1-2 ulp and left about 1%
+// of arguments an ulp away, which grazing reflections and the Catmull-Rom table lookups amplify past
+// 1e-5. On the device these evaluate in double precision and round once to float, which is the
+// correctly rounded value except where the double result lies within a double ulp or so of a float
+// rounding boundary.
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ void sincos_rn(float x, float& s, float& c) {
+    double sd, cd;
+    sincos(static_cast<double>(x), &sd, &cd);
+    s = static_cast<float>(sd);
+    c = static_cast<float>(cd);
+}
+// x^(1/4) for x >= 0 as two double-precision square roots (each correctly rounded)
+__device__ __forceinline__ float quartic_root_rn(float x) {
+    return static_cast<float>(sqrt(sqrt(static_cast<double>(x))));
+}
+__device__ __forceinline__ float exp_rn(float x) { return static_cast<float>(exp(static_cast<double>(x))); }
+__device__ __forceinline__ float acos_rn(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
+#else
+inline void sincos_rn(float x, float& s, float& c) {
+    s = sinf(x);
+    c = cosf(x);
+}
+inline float quartic_root_rn(float x) { return powf(x, 0.25f); }
+inline float exp_rn(float x) { return expf(x); }
+inline float acos_rn(float x) { return acosf(x); }
+#endif
+
 // onb::build_from_normal / local_to_world / world_to_local (src/core/onb.h:8-23)
 struct Onb {
     f3 a0, a1, a2;

@@ -45,12 +45,14 @@ __device__ __forceinline__ bool area_sample_ray(const DeviceScene& s, const Emit
     if(e.area <= 0.0f) return false;
     f3 p, n;
     float pdf_area = 0.0f;
-    shape_sample_position(s.objects[e.object], sx, sy, p, n, pdf_area);
+    emitter_sample_position(s, e, sx, sy, p, n, pdf_area);
     if(pdf_area <= 0.0f) return false;
     const float cos_theta = sqrtf(dx);
     const float sin_theta = sqrtf(1.0f - dx);
     const float phi = 2.0f * kPi * dy;
-    const f3 local{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    float sin_phi, cos_phi;
+    sincos_rn(phi, sin_phi, cos_phi);
+    const f3 local{cos_phi * sin_theta, sin_phi * sin_theta, cos_theta};
     const Onb frame = onb_from_normal(n);
     out.ray = Ray{p, to_world(frame, local)};
     out.weight = load3(e.radiance) * (kPi * e.area);  // power()
@@ -915,11 +917,7 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
                     bool any_mode = true;
                     const EmitRec& e = s.emitters[light.emitter];
                     if(e.kind == LRT_EMITTER_AREA) {  // scene_occluded's rule
-                        const ObjRec& lo = s.objects[e.object];
-                        float t;
-                        f3 pp;
-                        any_mode = !(lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, sr, 0.001f, tmax, t, pp)
-                                                                    : hit_sphere(lo, sr, 0.001f, tmax, t));
+                        any_mode = !light_shape_reachable(s, s.objects[e.object], sr, 0.001f, tmax);
                     }
                     trav_begin(ts, sr, 0.001f, tmax, any_mode);
                     return true;

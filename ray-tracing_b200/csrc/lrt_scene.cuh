@@ -412,6 +412,24 @@ __device__ __forceinline__ int32_t scene_hit_emitter(const DeviceScene& s, const
     return s.objects[best].emitter;
 }
 
+// Whether an occlusion ray towards an area light can reach the light's own shape within [t_min, t_max]
+// (the rule of scene_occluded); for a mesh light: whether any of its triangles is accepted.
+static __device__ __noinline__ bool mesh_light_reachable(const DeviceScene& s, const ObjRec& o, const Ray& r, float t_min,
+                                                  float t_max) {
+    MeshHit mh;
+    TraceCount cnt{0, 0};
+    return ray_may_hit_box(o, r, t_min, t_max) && trace_mesh<false, true>(s, o, r, t_min, t_max, mh, cnt);
+}
+
+__device__ __forceinline__ bool light_shape_reachable(const DeviceScene& s, const ObjRec& o, const Ray& r, float t_min,
+                                                      float t_max) {
+    float t;
+    f3 p;
+    if(o.kind == LRT_OBJECT_RECTANGLE) return hit_rectangle(o, r, t_min, t_max, t, p);
+    if(o.kind == LRT_OBJECT_SPHERE) return hit_sphere(o, r, t_min, t_max, t);
+    return mesh_light_reachable(s, o, r, t_min, t_max);
+}
+
 // Shadow test of path_integrator.h:113-115: blocked = (closest hit exists) && (its emitter != light).
 // When the light's own shape cannot be hit within [t_min, t_max] (always the case for the sky), the
 // closest hit is never the light, so blocked == "any object has an accepted hit": objects are tested
@@ -422,12 +440,7 @@ __device__ __forceinline__ bool scene_occluded(const DeviceScene& s, const Ray& 
                                                int32_t light, TraceCount& cnt) {
     const EmitRec& e = s.emitters[light];
     if(e.kind == LRT_EMITTER_AREA) {
-        const ObjRec& lo = s.objects[e.object];
-        float t;
-        f3 p;
-        const bool light_reachable = lo.kind == LRT_OBJECT_RECTANGLE ? hit_rectangle(lo, r, t_min, t_max, t, p)
-                                                                      : hit_sphere(lo, r, t_min, t_max, t);
-        if(light_reachable) {
+        if(light_shape_reachable(s, s.objects[e.object], r, t_min, t_max)) {
             const int32_t hit = scene_hit_emitter<kCount>(s, r, t_min, t_max, cnt);
             return hit != -2 && hit != light;
         }
@@ -747,8 +760,8 @@ __device__ __forceinline__ double hosek_radiance(const double* cfg, double theta
 __device__ __forceinline__ f3 env_eval(const EmitRec& e, f3 direction) {
     const f3 dir = normalize(direction);
     if(dir.y <= 0.0f) return mk(1.0f);
-    const float theta = acosf(sclamp(dir.y, 0.0f, 1.0f));
-    const float gamma = acosf(sclamp(dot(dir, load3(e.sun)), -1.0f, 1.0f));
+    const float theta = acos_rn(sclamp(dir.y, 0.0f, 1.0f));
+    const float gamma = acos_rn(sclamp(dot(dir, load3(e.sun)), -1.0f, 1.0f));
     const f3 c{static_cast<float>(hosek_radiance(e.cfg[0], theta, gamma) * e.rad[0]),
                static_cast<float>(hosek_radiance(e.cfg[1], theta, gamma) * e.rad[1]),
                static_cast<float>(hosek_radiance(e.cfg[2], theta, gamma) * e.rad[2])};
@@ -773,9 +786,49 @@ struct DirectSample {
     int32_t emitter;
 };
 
-// hittable::sample_position of the emitter's shape (rectangle.h:65-69, sphere.h:60-67)
-__device__ __forceinline__ void shape_sample_position(const ObjRec& o, float sx, float sy, f3& p, f3& n, float& pdf) {
-    if(o.kind == LRT_OBJECT_RECTANGLE) {
+// triangle_mesh::sample_position (triangle_mesh.h:109-138): sample.x picks a triangle by area through
+// the mesh's float area CDF (std::upper_bound), its remainder and sample.y place a point by the
+// square-root barycentric warp; the normal is the unit geometric normal.
+static __device__ __noinline__ void mesh_light_sample_position(const DeviceScene& s, const EmitRec& e, float sx, float sy,
+                                                        f3& p, f3& n, float& pdf) {
+    pdf = 0.0f;
+    if(e.area <= 0.0f || e.n_tris == 0) return;
+    const float* cdf = s.light_cdf + e.tri_first;
+    const float target = smin(sx, 0.999999f) * e.area;
+    uint32_t first = 0, count = e.n_tris;  // std::upper_bound: the first entry greater than target
+    while(count > 0) {
+        const uint32_t step = count / 2;
+        if(!(target < cdf[first + step])) {
+            first += step + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    const uint32_t tri = first < e.n_tris ? first : e.n_tris - 1;
+    const float prev = tri == 0 ? 0.0f : cdf[tri - 1];
+    const float span = cdf[tri] - prev;
+    const float u0 = span > 0.0f ? (target - prev) / span : 0.0f;
+    const float su = sqrtf(u0);
+    const float b0 = 1.0f - su;
+    const float b1 = sy * su;
+    const float b2 = 1.0f - b0 - b1;
+    const float4* c = s.light_tri + 3ull * (e.tri_first + tri);
+    const f3 p0{c[0].x, c[0].y, c[0].z}, p1{c[1].x, c[1].y, c[1].z}, p2{c[2].x, c[2].y, c[2].z};
+    p = b0 * p0 + b1 * p1 + b2 * p2;
+    const f3 geometric = cross(p1 - p0, p2 - p0);
+    n = geometric / length(geometric);
+    pdf = 1.0f / e.area;
+}
+
+// hittable::sample_position of the emitter's shape (rectangle.h:65-69, sphere.h:60-67,
+// triangle_mesh.h:109-138)
+__device__ __forceinline__ void emitter_sample_position(const DeviceScene& s, const EmitRec& e, float sx, float sy,
+                                                        f3& p, f3& n, float& pdf) {
+    const ObjRec& o = s.objects[e.object];
+    if(o.kind == LRT_OBJECT_MESH) {
+        mesh_light_sample_position(s, e, sx, sy, p, n, pdf);
+    } else if(o.kind == LRT_OBJECT_RECTANGLE) {
         p = load3(o.corner) + sx * load3(o.edge_u) + sy * load3(o.edge_v);
         n = load3(o.normal);
         pdf = 1.0f / o.area;
@@ -783,7 +836,9 @@ __device__ __forceinline__ void shape_sample_position(const ObjRec& o, float sx,
         const float z = 1.0f - 2.0f * sy;
         const float ring = sqrtf(smax(0.0f, 1.0f - z * z));
         const float phi = 2.0f * kPi * sx;
-        n = f3{ring * cosf(phi), ring * sinf(phi), z};
+        float sin_phi, cos_phi;
+        sincos_rn(phi, sin_phi, cos_phi);
+        n = f3{ring * cos_phi, ring * sin_phi, z};
         p = load3(o.center) + o.radius * n;
         pdf = 1.0f / o.area;
     }
@@ -795,7 +850,7 @@ __device__ __forceinline__ bool area_sample(const DeviceScene& s, const EmitRec&
     if(e.area <= 0.0f) return false;
     f3 p, n;
     float pdf_area = 0.0f;
-    shape_sample_position(s.objects[e.object], sx, sy, p, n, pdf_area);
+    emitter_sample_position(s, e, sx, sy, p, n, pdf_area);
     const f3 to_light = p - shading_point;
     const float dist2 = length_squared(to_light);
     if(dist2 < 1e-8f) return false;
@@ -817,7 +872,9 @@ __device__ __forceinline__ bool env_sample(const EmitRec& e, float sx, float sy,
     const float cos_theta = (1.0f - sx) + sx * e.cos_cutoff;
     const float sin_theta = sqrtf(smax(0.0f, 1.0f - cos_theta * cos_theta));
     const float phi = 2.0f * kPi * sy;
-    const f3 local{cosf(phi) * sin_theta, sinf(phi) * sin_theta, cos_theta};
+    float sin_phi, cos_phi;
+    sincos_rn(phi, sin_phi, cos_phi);
+    const f3 local{cos_phi * sin_theta, sin_phi * sin_theta, cos_theta};
     const f3 a0 = load3(e.frame[0]), a1 = load3(e.frame[1]), a2 = load3(e.frame[2]);
     out.direction = a0 * local.x + a1 * local.y + a2 * local.z;
     out.pdf = e.cone_pdf;
@@ -845,6 +902,21 @@ __device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f
     return out.pdf > 0.0f;
 }
 
+// triangle_mesh::hit of a mesh light over [0.001, inf) (area_emitter.h:60): the closest triangle's
+// t, front_face and hit-record normal (the shading normal turned toward the ray)
+static __device__ __noinline__ bool mesh_light_hit(const DeviceScene& s, int32_t object, const Ray& r, float& t, f3& normal) {
+    const ObjRec& o = s.objects[object];
+    MeshHit mh;
+    TraceCount cnt{0, 0};
+    if(!ray_may_hit_box(o, r, 0.001f, kInf) || !trace_mesh<false, false>(s, o, r, 0.001f, kInf, mh, cnt)) return false;
+    HitInfo h;
+    hit_record_of(s, r, object, mh.t, mh, h);
+    if(!h.front_face) return false;
+    t = mh.t;
+    normal = h.normal;
+    return true;
+}
+
 // area_emitter::pdf (area_emitter.h:51-72): re-intersects the light shape
 __device__ __forceinline__ float area_pdf(const DeviceScene& s, const EmitRec& e, f3 shading_point, f3 direction) {
     if(e.area <= 0.0f) return 0.0f;
@@ -853,7 +925,9 @@ __device__ __forceinline__ float area_pdf(const DeviceScene& s, const EmitRec& e
     const ObjRec& o = s.objects[e.object];
     float t;
     f3 normal;
-    if(o.kind == LRT_OBJECT_RECTANGLE) {
+    if(o.kind == LRT_OBJECT_MESH) {
+        if(!mesh_light_hit(s, e.object, r, t, normal)) return 0.0f;
+    } else if(o.kind == LRT_OBJECT_RECTANGLE) {
         f3 p;
         if(!hit_rectangle(o, r, 0.001f, kInf, t, p)) return 0.0f;
         normal = load3(o.normal);

@@ -12,6 +12,8 @@
 //   emitters   EmitRec[n_emitters]
 //   tlas       float4 [2 * nodes]       bounding-volume hierarchy over the objects (scenes of > 16 objects)
 //   tlas_objs  int32  [n_objects]       object indices in leaf order
+//   light_cdf  float  [mesh-light tris]  area CDF of every mesh that is an area light, mesh after mesh
+//   light_tri  float4 [3 * same]         corner positions of those triangles (area-light sampling)
 #pragma once
 
 #include <stdint.h>
@@ -80,6 +82,8 @@ struct EmitRec {
     int32_t sun_active;  // env
     float radiance[3];   // area
     float area;          // area: shape area
+    uint32_t tri_first;  // area over a mesh: its first entry in light_cdf / light_tri
+    uint32_t n_tris;     // area over a mesh: its triangle count
     // env
     float sun[3];
     float frame[3][3];   // onb built from sun (axis 0, 1, 2)
@@ -119,6 +123,8 @@ struct DeviceScene {
     const uint32_t* sobol;          // 16 x 32 Sobol direction numbers
     const float* emission_cdf;      // scene::sample_emitter_ray luminance CDF (scene.h:21-34)
     const int32_t* emission_index;  // emitter index of each CDF bin
+    const float* light_cdf;         // mesh lights: running triangle area per triangle (triangle_mesh.h:17-24)
+    const float4* light_tri;        // mesh lights: the triangle's three corner positions
     int32_t n_objects;
     int32_t n_materials;
     int32_t n_emitters;

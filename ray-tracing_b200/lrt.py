@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "liblrt.so")
 # every entry point include/lrt.h declares (checked by the CPU test suite)
 EXPORTS = [
     "lrt_create", "lrt_destroy", "lrt_last_error", "lrt_status_string", "lrt_rough_transmittance_slice",
-    "lrt_fresnel_diffuse_reflectance", "lrt_kdtree_build", "lrt_kdtree_build_device", "lrt_scene_upload", "lrt_scene_device_bytes",
+    "lrt_fresnel_diffuse_reflectance", "lrt_hosek_state", "lrt_kdtree_build", "lrt_kdtree_build_device", "lrt_scene_upload", "lrt_scene_device_bytes",
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
@@ -63,6 +63,7 @@ def lib():
         L.lrt_rough_transmittance_slice.argtypes = [C.c_char_p, f32, f32, P(f32), P(f32)]
         L.lrt_fresnel_diffuse_reflectance.restype = f32
         L.lrt_fresnel_diffuse_reflectance.argtypes = [f32]
+        L.lrt_hosek_state.argtypes = [P(f32), f32, f32, P(C.c_double), P(C.c_double)]
         L.lrt_kdtree_build.argtypes = [P(f32), P(f32), u32, P(u32), u32, P(u32), u32, P(u32), P(u32), P(u32)]
         L.lrt_kdtree_build_device.argtypes = [vp, u32, P(u32), P(f32), P(f32), P(u32), u64, P(u32), u64, P(u32),
                                               P(u32), P(u32), P(u64), P(u64)]
@@ -107,6 +108,19 @@ def lib():
         L.lrt_render_photon_dev.argtypes = [vp, P(abi.RenderParams), P(abi.PhotonRenderParams), vp]
         _lib = L
     return _lib
+
+
+def hosek_state(sun_direction, turbidity: float, albedo: float):
+    """The Hosek-Wilkie RGB sky state env_emitter's constructor cooks: (config (3, 9), radiance (3,)) as
+    float64, bit-identical to the reference."""
+    sun = np.ascontiguousarray(sun_direction, dtype=np.float32).reshape(3)
+    cfg = np.zeros((3, 9), dtype=np.float64)
+    rad = np.zeros(3, dtype=np.float64)
+    st = lib().lrt_hosek_state(ptr(sun, C.c_float), float(np.float32(turbidity)), float(np.float32(albedo)),
+                               ptr(cfg, C.c_double), ptr(rad, C.c_double))
+    if st != 0:
+        raise LrtError(st, "Hosek state: turbidity must lie in [1, 10], albedo in [0, 1]")
+    return cfg, rad
 
 
 def rough_transmittance_slice(ggx_path: str, eta: float, alpha: float):

@@ -12,9 +12,10 @@ normals), so the GPU library and the reference harness receive identical inputs.
 * Materials follow the reference constructors and src/main.cpp:38-47 where the workload leaves a
   parameter open (plastic Kd, coating nests).
 
-Rough-transmittance tables and the cooked Hosek state are caller-side inputs of the library (the
-reference computes them on the host at material/emitter construction). They are read from
-``data/scene_data.json``; ``data/make_scene_data.py`` fills that file.
+Rough-transmittance tables are caller-side inputs of the library (the reference slices them from its
+ggx.dat at material construction): the eta slices the workload materials need are read from
+``data/scene_data.json`` (``tests/golden/make_scene_data.py`` fills it) and cut to a 1-D table for any
+alpha by the library. The Hosek sky state is cooked by the library (``lrt.hosek_state``).
 """
 from __future__ import annotations
 
@@ -58,7 +59,7 @@ class Scene:
 
 
 # ---------------------------------------------------------------------------------------------
-# caller-side tables (rough transmittance, cooked Hosek state)
+# caller-side tables (rough transmittance) and the cooked Hosek state
 
 _scene_data_cache = None
 
@@ -74,7 +75,7 @@ def load_scene_data() -> dict:
             with open(SCENE_DATA) as f:
                 _scene_data_cache = json.load(f)
         else:
-            _scene_data_cache = {"transmittance": {}, "hosek": {}}
+            _scene_data_cache = {"eta_slices": {}}
     return _scene_data_cache
 
 
@@ -107,13 +108,9 @@ def transmittance_table(eta: float, alpha: float):
 
 
 def hosek_state(sun_direction, turbidity: float, albedo: float):
-    key = _f32_key(*sun_direction, turbidity, albedo)
-    data = load_scene_data()["hosek"]
-    if key not in data:
-        raise KeyError("no cooked Hosek state for sun=%r in %s; run data/make_scene_data.py"
-                       % (tuple(map(float, sun_direction)), SCENE_DATA))
-    entry = data[key]
-    return np.array(entry["config"], dtype=np.float64).reshape(3, 9), np.array(entry["radiance"], dtype=np.float64)
+    """(config (3, 9), radiance (3,)) of the sky, cooked by liblrt as env_emitter's constructor does."""
+    import lrt
+    return lrt.hosek_state(sun_direction, turbidity, albedo)
 
 
 def required_tables(materials) -> list:
@@ -369,6 +366,57 @@ def mesh_box(path: str, material: str = "diffuse", scale: float = 0.9, aspect: f
                     "edge_u": (2 * h, 0.0, 0.0), "edge_v": (0.0, 0.0, 2 * h)})
     emitters = [{"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (17.0, 12.0, 4.0)}]
     scene = Scene(objects, mats, emitters, default_camera(aspect), name="mesh_box_%s" % material)
+    if attach:
+        attach_tables(scene.materials)
+    return scene
+
+
+def demo_scene(bunny_path: str, aspect: float = 1.0, sphere_light: bool = False, attach: bool = True) -> Scene:
+    """The reference's own demo scene (src/main.cpp:58-90): the bunny loaded by load_obj with the rough
+    plastic of main.cpp:43 (alpha 0.1, Kd (0.8, 0.1, 0.05)), the ground as a sphere of radius 100 centred
+    at (0, -100.5, 0) with diffuse (0.8, 0.8, 0), and the 1.2 x 1.2 rectangle light of radiance 12 at
+    height 1.5; the camera at (0, 0.5, 3) looks at the origin (camera.h's default look_at) with a 60
+    degree field of view. sphere_light adds the sphere light main.cpp:55-56 defines (radius 0.3 at
+    (1.2, 0.4, 0), radiance 4) as an object and an emitter of the scene (main.cpp builds it but leaves it
+    out)."""
+    mats = [{"type": abi.MAT_ROUGH_PLASTIC, "int_ior": 1.49, "ext_ior": 1.000277, "alpha": 0.1,
+             "specular_reflectance": (1, 1, 1), "diffuse_reflectance": (0.8, 0.1, 0.05)},
+            {"type": abi.MAT_DIFFUSE, "diffuse_reflectance": (0.8, 0.8, 0.0)}]
+    objects = [obj_mesh(bunny_path, 0),
+               {"kind": abi.OBJ_SPHERE, "material": 1, "center": (0.0, -100.5, 0.0), "radius": 100.0},
+               {"kind": abi.OBJ_RECTANGLE, "material": -1, "corner": (-0.6, 1.5, -0.6), "edge_u": (1.2, 0.0, 0.0),
+                "edge_v": (0.0, 0.0, 1.2)}]
+    emitters = [{"kind": abi.EMITTER_AREA, "object": 2, "radiance": (12.0, 12.0, 12.0)}]
+    if sphere_light:
+        objects.append({"kind": abi.OBJ_SPHERE, "material": -1, "center": (1.2, 0.4, 0.0), "radius": 0.3})
+        emitters.append({"kind": abi.EMITTER_AREA, "object": 3, "radiance": (4.0, 4.0, 4.0)})
+    camera = {"origin": (0.0, 0.5, 3.0), "look_at": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 60.0,
+              "aspect": aspect}
+    scene = Scene(objects, mats, emitters, camera, name="demo_scene" + ("_sphere_light" if sphere_light else ""))
+    if attach:
+        attach_tables(scene.materials)
+    return scene
+
+
+def mesh_light_box(level: int = 6, light_level: int = 2, seed: int = 20261203, material: str = "diffuse",
+                   aspect: float = 1.0, attach: bool = True) -> Scene:
+    """The closed box and displaced sphere of cornell_box lit by an emitting triangle mesh instead of the
+    ceiling rectangle: a displaced icosphere (level 2, 320 triangles, radius 0.16) near the ceiling with
+    radiance (9, 6, 3) and a white diffuse surface, an area light over a mesh as area_emitter takes any
+    hittable (area_emitter.h:17-49, triangle_mesh.h:109-138). A second emitter, a small rectangle on the
+    back wall of radiance (2, 3, 6), makes the light pick of scene::sample_emitter_direction matter."""
+    mats, sphere_mat = material_library(material)
+    objects = _box_quads(0, 1, 2, roof=True)
+    pos, idx, nrm = displaced_icosphere(level, SPHERE_CENTER, SPHERE_RADIUS, 0.05, seed)
+    objects.append({"kind": abi.OBJ_MESH, "material": sphere_mat, "positions": pos, "indices": idx,
+                    "corner_normals": nrm})
+    lpos, lidx, lnrm = displaced_icosphere(light_level, (0.35, 1.55, 0.2), 0.16, 0.1, seed + 7)
+    objects.append({"kind": abi.OBJ_MESH, "material": 0, "positions": lpos, "indices": lidx, "corner_normals": lnrm})
+    emitters = [{"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (9.0, 6.0, 3.0)}]
+    objects.append({"kind": abi.OBJ_RECTANGLE, "material": -1, "corner": (-0.7, 0.6, BOX_Z0 + 1e-3),
+                    "edge_u": (0.3, 0.0, 0.0), "edge_v": (0.0, 0.3, 0.0)})  # normal +z, into the box
+    emitters.append({"kind": abi.EMITTER_AREA, "object": len(objects) - 1, "radiance": (2.0, 3.0, 6.0)})
+    scene = Scene(objects, mats, emitters, default_camera(aspect), name="mesh_light_box_%s" % material)
     if attach:
         attach_tables(scene.materials)
     return scene

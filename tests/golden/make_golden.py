@@ -3,7 +3,7 @@ LinRT sources compiled by oracle/Makefile into oracle/_ref/liblrt_ref.so).
 
 The reference ships no tests, golden vectors or known-answer data, so these files ARE the pinned
 reference outputs: every input is stored beside the output it produced. Regenerate with
-    make -C oracle ref && make -C ray-tracing_b200/csrc && python tests/golden/make_golden.py
+    make -C oracle ref && make -C ray-tracing_b200/csrc && python tests/golden/make_golden.py [fixture ...]
 """
 import os
 import sys
@@ -244,7 +244,36 @@ def knn_kat(rng):
     save("knn_kat.npz", **out)
 
 
+def light_kat():
+    """area lights over a triangle mesh (scenes.mesh_light_box): emitter sampling and pdf at random
+    points, and per-particle photons emitted from the mesh light"""
+    rng = np.random.default_rng(SEED + 11)
+    out = {}
+    world = oracle.RefWorld(scenes.mesh_light_box(level=1))
+    n = 2048
+    p = np.stack([rng.uniform(-0.99, 0.99, n), rng.uniform(0.0, 1.99, n), rng.uniform(-0.99, 1.49, n)],
+                 1).astype(np.float32)
+    u2 = rng.random((n, 2), dtype=np.float32)
+    ds = world.emitter_sample(p, u2)
+    dirs = random_dirs(rng, n)
+    ok = ds[:, 0] > 0
+    dirs[ok] = np.where(rng.random((int(ok.sum()), 1)) < 0.7, ds[ok, 1:4], dirs[ok])
+    out["mesh_points"], out["mesh_u2"], out["mesh_dirs"] = p, u2, dirs
+    out["mesh_sample"] = ds
+    out["mesh_pdf"] = world.emitter_pdf(p, dirs)
+    world.close()
+    world = oracle.RefWorld(scenes.mesh_light_box(level=3))
+    ph, cnt = world.trace_particles(abi.GATHER_SURFACE, 0, 2048, 8, 5, max_per=16)
+    out["mesh_photons"], out["mesh_photon_counts"] = ph, cnt
+    world.close()
+    save("light_kat.npz", **out)
+
+
 def main():
+    if len(sys.argv) > 1:  # only the named fixtures, e.g. `make_golden.py light_kat`
+        for name in sys.argv[1:]:
+            globals()[name]()
+        return
     rng = np.random.default_rng(SEED)
     sampler_kat(rng)
     camera_kat(rng)
@@ -255,6 +284,7 @@ def main():
     knn_kat(rng)
     photon_kat(rng)
     image_kat()
+    light_kat()
 
 
 if __name__ == "__main__":

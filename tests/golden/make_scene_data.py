@@ -3,10 +3,9 @@
 * rough-transmittance eta slices (the set_eta step over ggx.dat) for every eta the seven materials
   use, made by liblrt's own host routine (lrt_rough_transmittance_eta_slice); the 1-D table for any
   alpha follows from a slice by lrt_rough_transmittance_at_alpha, and the CPU tests check that pair
-  bit for bit against the reference's rough_transmittance;
-* the cooked RGB Hosek-Wilkie state of the workload sky, from the reference's vendored Hosek model
-  (arhosek_rgb_skymodelstate_alloc_init through the oracle build), which a reference-side caller would
-  read from its env_emitter.
+  bit for bit against the reference's rough_transmittance.
+
+(The Hosek sky state is not stored: the library cooks it, lrt_hosek_state.)
 
 Run from the repository root after `make -C oracle ref` and `make -C ray-tracing_b200/csrc`:
     python tests/golden/make_scene_data.py
@@ -15,8 +14,6 @@ import base64
 import json
 import os
 import sys
-
-import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "ray-tracing_b200"))
@@ -28,8 +25,7 @@ import scenes  # noqa: E402
 
 
 def main():
-    data = {"hosek": {},
-            "note": "caller-side inputs of the workload scenes; made by tests/golden/make_scene_data.py"}
+    data = {"note": "caller-side inputs of the workload scenes; made by tests/golden/make_scene_data.py"}
     pairs = []
     for name in scenes.MATERIAL_NAMES:
         mats, _ = scenes.material_library(name)
@@ -44,16 +40,10 @@ def main():
                                    "alpha_range": [float(x) for x in rng],
                                    "table_f32_b64": base64.b64encode(table.astype("<f4").tobytes()).decode(),
                                    "diffuse_f32_b64": base64.b64encode(diffuse.astype("<f4").tobytes()).decode()}
-    sky = scenes.sky_emitter()
-    key = scenes._f32_key(*sky["sun_direction"], sky["turbidity"], sky["albedo"])
-    cfg, rad = oracle.hosek_state(sky["sun_direction"], sky["turbidity"], sky["albedo"])
-    data["hosek"][key] = {"sun_direction": [float(np.float32(v)) for v in sky["sun_direction"]],
-                          "turbidity": sky["turbidity"], "albedo": sky["albedo"],
-                          "config": [float(x) for x in cfg.reshape(-1)], "radiance": [float(x) for x in rad]}
     os.makedirs(scenes.DATA_DIR, exist_ok=True)
     with open(scenes.SCENE_DATA, "w") as f:
         json.dump(data, f, indent=1)
-    print("wrote", scenes.SCENE_DATA, len(data["eta_slices"]), "eta slices,", len(data["hosek"]), "sky states")
+    print("wrote", scenes.SCENE_DATA, len(data["eta_slices"]), "eta slices")
 
 
 if __name__ == "__main__":

@@ -3,9 +3,8 @@ by the unmodified reference, tests/golden/make_golden.py) and, where the oracle 
 live reference on fresh random inputs.
 
 Bars: the sampler, camera rays and kd-tree traversal (object, triangle, t, hit point, normal) are
-bit-exact; BSDF sample/eval/pdf, sky radiance and emitter sampling agree within 1e-5 relative (FP32),
-with exact agreement on every discrete outcome (sampled lobe, component) except samples that land
-within rounding of a lobe-selection threshold."""
+bit-exact; BSDF eval/pdf, sky radiance and emitter sampling agree within 1e-5 relative (FP32) on every
+query; BSDF sampling agrees within 1e-5 on all but a measured, bounded handful (_compare_bsdf)."""
 import numpy as np
 import pytest
 
@@ -104,32 +103,46 @@ def test_trace_edge_cases(ctx):
         _check_hits(hits, ref)
 
 
-def _compare_bsdf(res, ref, q, material, allow_discrete=0.004):
-    # discrete outcomes
+def _max_rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-30)
+    d[(a == b) | (np.isnan(a) & np.isnan(b))] = 0.0
+    return float(d.max()) if d.size else 0.0
+
+
+def _compare_bsdf(res, ref, q, material):
+    """BSDF parity bars, with the sizes measured on B200 against the reference built with glibc:
+
+    * eval and pdf: every query within 1e-5 relative (+1e-7 absolute); measured worst 5.5e-7.
+    * the sampled lobe and component: identical for all but 1 in 10,000 queries (measured: none differ
+      in 13 x 20,768 queries).
+    * the sampled weight, pdf, eta and direction: within 1e-5 for all but 1 in 5,000 queries, and those
+      within 1e-3 (measured: at most 2 of 20,000 per material, worst 1.4e-4). The sampled directions
+      pass through sin/cos, which the library evaluates in double and rounds once (the correctly
+      rounded float), glibc's sinf/cosf being under 0.56 ulp but not always correctly rounded; a grazing
+      reflection amplifies that last-bit difference.
+    """
+    n = len(q)
     type_ok = (res["sampled_type"] == ref["sampled_type"]) & (res["sampled_component"] == ref["sampled_component"])
-    frac_bad = 1.0 - type_ok.mean()
-    assert frac_bad <= allow_discrete, "material %d: %.4f of samples chose another lobe" % (material, frac_bad)
-    ok = type_ok
+    assert (~type_ok).sum() <= n // 10000, "material %d: %d samples chose another lobe" % (material, (~type_ok).sum())
+    e_ok = rel_close(res["eval"], ref["eval"]).all(axis=1) & rel_close(res["pdf"], ref["pdf"])
+    assert e_ok.all(), "material %d: %d eval/pdf beyond 1e-5 (worst %.3g / %.3g): %s vs %s" % (
+        material, (~e_ok).sum(), _max_rel(res["eval"], ref["eval"]), _max_rel(res["pdf"], ref["pdf"]),
+        res[~e_ok][:2], ref[~e_ok][:2])
     w_ok = rel_close(res["sample_weight"], ref["sample_weight"]).all(axis=1)
     pdf_ok = rel_close(res["sample_pdf"], ref["sample_pdf"])
     eta_ok = res["sample_eta"] == ref["sample_eta"]
     nonzero = np.any(ref["sample_weight"] != 0, axis=1)
     wo_ok = rel_close(res["sample_wo"], ref["sample_wo"], rtol=1e-5, atol=1e-6).all(axis=1) | ~nonzero
-    bad = ok & ~(w_ok & pdf_ok & eta_ok & wo_ok)
-    # Sampled directions go through sinf/cosf; CUDA's and glibc's differ by an ulp for ~1% of arguments
-    # (neither is correctly rounded). Where the reflection cancels (grazing wo) that ulp grows to ~1e-3
-    # relative (most for peaky lobes, e.g. a coating over alpha = 0.05 glass). Such ill-conditioned
-    # samples may be up to 0.6% of the queries, each within 1e-2.
-    assert bad.sum() <= max(5, int(0.006 * len(q))), "material %d: %d sample mismatches, e.g. %s vs %s" % (
+    bad = type_ok & ~(w_ok & pdf_ok & eta_ok & wo_ok)
+    assert bad.sum() <= max(1, n // 5000), "material %d: %d sample mismatches, e.g. %s vs %s" % (
         material, bad.sum(), res[bad][:2], ref[bad][:2])
-    loose = (rel_close(res["sample_weight"], ref["sample_weight"], 1e-2, 1e-6).all(axis=1)
-             & rel_close(res["sample_pdf"], ref["sample_pdf"], 1e-2, 1e-6)
-             & rel_close(res["sample_wo"], ref["sample_wo"], 1e-2, 1e-4).all(axis=1))
-    assert loose[bad].all(), "material %d: a sample differs by more than 1e-2: %s vs %s" % (
+    loose = (rel_close(res["sample_weight"], ref["sample_weight"], 1e-3, 1e-6).all(axis=1)
+             & rel_close(res["sample_pdf"], ref["sample_pdf"], 1e-3, 1e-6)
+             & rel_close(res["sample_wo"], ref["sample_wo"], 1e-3, 1e-5).all(axis=1) & eta_ok)
+    assert loose[bad].all(), "material %d: a sample differs by more than 1e-3: %s vs %s" % (
         material, res[bad & ~loose][:2], ref[bad & ~loose][:2])
-    e_ok = rel_close(res["eval"], ref["eval"]).all(axis=1) & rel_close(res["pdf"], ref["pdf"])
-    assert (~e_ok).sum() <= max(1, int(0.002 * len(q))), "material %d: eval/pdf mismatches %s vs %s" % (
-        material, res[~e_ok][:2], ref[~e_ok][:2])
 
 
 def _zoo():
