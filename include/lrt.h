@@ -269,6 +269,11 @@ typedef struct lrt_render_stats {
     float stage_ms[LRT_STAGE_COUNT];
     uint32_t stage_launches[LRT_STAGE_COUNT];
     uint64_t rays_at_depth[LRT_MAX_STAT_DEPTH];  /* extension rays per bounce (option count_work) */
+    /* k-nearest-photon queries of lrt_photon_irradiance(_dev) with option count_work */
+    uint64_t knn_queries;
+    uint64_t knn_nodes_visited;   /* photon-map nodes read */
+    uint64_t knn_photons_tested;  /* photon positions whose distance was computed */
+    uint64_t knn_photons_found;   /* photons returned (<= k per query) and read by the estimate */
 } lrt_render_stats;
 
 /* ---- context ---- */
@@ -497,6 +502,10 @@ int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photon
  * reference pops its max-heap. */
 int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t n, float r2,
                    uint32_t k, uint32_t* idx_out, float* d2_out, uint32_t* count_out);
+/* The same with caller-owned device buffers (points, normals: 3 floats each; rgb_dev: 3 floats per
+ * query), ordered on the context's stream, no synchronisation. */
+int lrt_photon_irradiance_dev(lrt_context* ctx, int32_t map, const float* points_dev, const float* normals_dev,
+                              uint32_t n, float radius, int32_t max_depth, uint32_t k, float* rgb_dev);
 int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, const float* normals,
                           uint32_t n, float radius, int32_t max_depth, uint32_t k, float* rgb_out);
 

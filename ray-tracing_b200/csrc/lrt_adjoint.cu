@@ -177,10 +177,12 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(AdjArgs a) {
             if(depth == a.max_depth - 1) break;
             const f3 weight = bsdf_sample(s.materials, s.tables, mid, bctx, rec, bsdf_uv.x, bsdf_uv.y);
             if(is_zero(weight)) break;
-            if(measure_of(rec.sampled_type) == kSolidAngle && an > 0) {
-                const f3 e0 = bsdf_eval(s.materials, s.tables, mid, bctx, rec, kSolidAngle);
+            if(an > 0) {
+                const int meas = measure_of(rec.sampled_type);
+                const BsdfCtx ectx = sampled_value_ctx(bctx, rec);
+                const f3 e0 = bsdf_eval(s.materials, s.tables, mid, ectx, rec, meas);
                 for(int32_t k = 0; k < an; ++k) {
-                    const f3 de = group_d_eval(a.d, mid, bctx, rec, a.d.aff_list[ab + k]);
+                    const f3 de = group_d_eval(a.d, mid, ectx, rec, a.d.aff_list[ab + k], meas);
                     vd[depth][k] = f3{safe_ratio(de.x, e0.x), safe_ratio(de.y, e0.y), safe_ratio(de.z, e0.z)};
                 }
                 vn[depth] = an;

@@ -40,18 +40,29 @@ int adjoint_wavefront(lrt_context* ctx, const std::vector<JobRec>& recs, unsigne
                       int32_t rr_depth, const float* adjoint_dev, double* grad_dev);
 
 #ifdef __CUDACC__
-// d(f cos)/d(group) at rec: the central difference of the group's packed records (kept out of line, one
-// copy of the BSDF dispatch for every call site)
+// d(f cos)/d(group) at rec in measure `meas`: the central difference of the group's packed records (kept
+// out of line, one copy of the BSDF dispatch for every call site)
 static __device__ __noinline__ f3 d_eval(const MatRec* plus, const MatRec* minus, const float* tables, float inv2step,
-                                  int32_t mid, const BsdfCtx& c, const BRec& rec) {
-    const f3 ep = bsdf_eval(plus, tables, mid, c, rec, kSolidAngle);
-    const f3 em = bsdf_eval(minus, tables, mid, c, rec, kSolidAngle);
+                                  int32_t mid, const BsdfCtx& c, const BRec& rec, int meas) {
+    const f3 ep = bsdf_eval(plus, tables, mid, c, rec, meas);
+    const f3 em = bsdf_eval(minus, tables, mid, c, rec, meas);
     return (ep - em) * inv2step;
 }
 
-__device__ __forceinline__ f3 group_d_eval(const DiffDev& d, int32_t mid, const BsdfCtx& c, const BRec& rec, int32_t grp) {
+__device__ __forceinline__ f3 group_d_eval(const DiffDev& d, int32_t mid, const BsdfCtx& c, const BRec& rec, int32_t grp,
+                                           int meas = kSolidAngle) {
     const MatRec* plus = d.pert + static_cast<size_t>(2 * grp) * d.n_materials;
-    return d_eval(plus, plus + d.n_materials, d.pert_tables, d.inv2step[grp], mid, c, rec);
+    return d_eval(plus, plus + d.n_materials, d.pert_tables, d.inv2step[grp], mid, c, rec, meas);
+}
+
+// The BSDF value a sampled direction's path weight carries (weight = value / sampling probability): in
+// solid angle, the whole BSDF at wo; for a delta lobe, the discrete value of the sampled component alone
+// (the evaluation context restricted to it), since several delta components can share a direction (a
+// coating's mirror reflection and its nested material's refracted mirror reflection).
+__device__ __forceinline__ BsdfCtx sampled_value_ctx(const BsdfCtx& c, const BRec& rec) {
+    BsdfCtx e = c;
+    if(measure_of(rec.sampled_type) == kDiscrete) e.component = rec.sampled_component;
+    return e;
 }
 
 __device__ __forceinline__ float rgb_channel(f3 v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }

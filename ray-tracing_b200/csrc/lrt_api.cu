@@ -585,14 +585,17 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
             a.misc[pid] = make_float2(rec.pdf, have ? 1.0f : 0.0f);
             const int seg = heavy_key(s, Ray{p, new_dir}, 0.001f, kInf);
             next[static_cast<size_t>(seg) * a.capacity + warp_append_keyed(nc.active, seg)] = pid;
-            if(kAdj && !is_zero(delta) && measure_of(rec.sampled_type) == kSolidAngle) {
-                // dE/E of the sampled direction per group; its suffix is known at the end of the wave
+            if(kAdj && !is_zero(delta)) {
+                // dE/E of the sampled direction per group (E in the sampled lobe's measure); its suffix is
+                // known at the end of the wave
                 const int32_t ab = a.diff.aff_begin[mid];
                 const int32_t an = a.diff.aff_begin[mid + 1] - ab;
                 if(an > 0) {
-                    const f3 e0 = bsdf_eval(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
+                    const int meas = measure_of(rec.sampled_type);
+                    const BsdfCtx ectx = sampled_value_ctx(ctx, rec);
+                    const f3 e0 = bsdf_eval(s.materials, s.tables, mid, ectx, rec, meas);
                     for(int32_t k = 0; k < an; ++k) {
-                        const f3 de = group_d_eval(a.diff, mid, ctx, rec, a.diff.aff_list[ab + k]);
+                        const f3 de = group_d_eval(a.diff, mid, ectx, rec, a.diff.aff_list[ab + k], meas);
                         a.adj_dlog[(static_cast<size_t>(depth) * a.adj_kmax + k) * a.capacity + pid] =
                             make_float4(safe_ratio(de.x, e0.x), safe_ratio(de.y, e0.y), safe_ratio(de.z, e0.z), 0.0f);
                     }

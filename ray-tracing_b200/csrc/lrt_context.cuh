@@ -124,6 +124,7 @@ struct lrt_context {
     int kd_build_device = 2;  // lrt_scene_upload's kd-trees: 0 host cores, 1 GPU, 2 GPU from 2^15 triangles
     int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
     lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L;
+    lrt::DevBuf knn_work;  // k-NN counters (option count_work): queries, nodes, photons tested, found
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
     lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye;
 };

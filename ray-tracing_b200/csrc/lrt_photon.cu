@@ -430,7 +430,15 @@ struct KnnHeap {
     }
 };
 
-__device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2, uint32_t k, KnnHeap& heap) {
+// per-query work of a k-NN search (algorithmic-bytes accounting); compiled out unless requested
+struct KnnCount {
+    uint32_t nodes;
+    uint32_t tested;
+};
+
+template <bool kCount = false>
+__device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2, uint32_t k, KnnHeap& heap,
+                                           KnnCount* cnt = nullptr) {
     heap.size = 0;
     if(m.n == 0 || k == 0) return;
     int32_t stack[64];
@@ -438,11 +446,13 @@ __device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2,
     stack[top++] = 0;
     while(top > 0) {
         const PhotonNode nd = m.nodes[stack[--top]];
+        if(kCount) ++cnt->nodes;
         float limit = r2;
         if(heap.size == k) limit = smin(limit, heap.d[0]);
         if(nd.axis == 3) {
             for(int32_t j = 0; j < nd.b; ++j) {
                 const uint32_t pi = static_cast<uint32_t>(nd.a + j);
+                if(kCount) ++cnt->tested;
                 const float4 p4 = __ldg(m.pos + pi);
                 const float distance = length_squared(f3{p4.x, p4.y, p4.z} - point);
                 if(distance > limit) continue;
@@ -476,12 +486,15 @@ __global__ void __launch_bounds__(kBlock) k_knn(MapView m, const float* points, 
 }
 
 // photon_map::estimate_irradiance (photon_map.h:38-70), neighbours in heap pop order
+template <bool kCount = false>
 __device__ __forceinline__ f3 estimate_irradiance(const MapView& m, f3 point, f3 normal, float radius, int32_t max_depth,
-                                                 uint32_t k, KnnHeap& heap) {
+                                                 uint32_t k, KnnHeap& heap, KnnCount* cnt = nullptr,
+                                                 uint32_t* found = nullptr) {
     f3 sum = mk(0.0f);
     if(m.n == 0 || radius <= 0.0f || k == 0) return sum;
     const float squared_radius = radius * radius;
-    knn_search(m, point, squared_radius, k, heap);
+    knn_search<kCount>(m, point, squared_radius, k, heap, cnt);
+    if(kCount) *found += heap.size;
     const float inverse_squared_radius = 1.0f / squared_radius;
     while(heap.size > 0) {
         const uint32_t pi = heap.i[0];
@@ -505,12 +518,24 @@ __device__ __forceinline__ f3 estimate_irradiance(const MapView& m, f3 point, f3
     return sum * (m.scale * 3.0f * (1.0f / kPi) * inverse_squared_radius);
 }
 
+// one query per thread; kCount adds the queries' nodes, photons tested and photons found to work[0..3]
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_irradiance(MapView m, const float* points, const float* normals, uint32_t n,
-                                                       float radius, int32_t max_depth, uint32_t k, float* rgb) {
+                                                       float radius, int32_t max_depth, uint32_t k, float* rgb,
+                                                       unsigned long long* work) {
+    KnnCount cnt{0, 0};
+    uint32_t found = 0, queries = 0;
     for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         KnnHeap heap;
-        store3(rgb + 3ull * q, estimate_irradiance(m, load3(points + 3ull * q), load3(normals + 3ull * q), radius,
-                                                   max_depth, k, heap));
+        store3(rgb + 3ull * q, estimate_irradiance<kCount>(m, load3(points + 3ull * q), load3(normals + 3ull * q),
+                                                           radius, max_depth, k, heap, &cnt, &found));
+        ++queries;
+    }
+    if(kCount) {
+        add_count(&work[0], queries);
+        add_count(&work[1], cnt.nodes);
+        add_count(&work[2], cnt.tested);
+        add_count(&work[3], found);
     }
 }
 
@@ -1474,22 +1499,75 @@ int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t 
     return LRT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// the irradiance queries on device buffers; with count_work their k-NN work goes into the stats
+int irradiance_launch(lrt_context* ctx, int32_t map, const float* points, const float* normals, uint32_t n,
+                      float radius, int32_t max_depth, uint32_t k, float* rgb) {
+    const MapView view = view_of(ctx->maps[map]);
+    if(!ctx->count_work) {
+        const int grid = grid_for(ctx, (const void*)k_irradiance<false>, kBlock);
+        k_irradiance<false><<<grid, kBlock, 0, ctx->stream>>>(view, points, normals, n, radius, max_depth, k, rgb,
+                                                              nullptr);
+        LRT_CUDA(ctx, cudaGetLastError());
+        ctx->stats.kernel_launches += 1;
+        return LRT_OK;
+    }
+    LRT_CUDA(ctx, ctx->knn_work.ensure(4 * sizeof(unsigned long long)));
+    unsigned long long* work = ctx->knn_work.as<unsigned long long>();
+    LRT_CUDA(ctx, cudaMemsetAsync(work, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    const int grid = grid_for(ctx, (const void*)k_irradiance<true>, kBlock);
+    k_irradiance<true><<<grid, kBlock, 0, ctx->stream>>>(view, points, normals, n, radius, max_depth, k, rgb, work);
+    LRT_CUDA(ctx, cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+    unsigned long long h[4];
+    LRT_CUDA(ctx, cudaMemcpyAsync(h, work, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stats.knn_queries += h[0];
+    ctx->stats.knn_nodes_visited += h[1];
+    ctx->stats.knn_photons_tested += h[2];
+    ctx->stats.knn_photons_found += h[3];
+    return LRT_OK;
+}
+
+int irradiance_check(lrt_context* ctx, int32_t map, uint32_t k) {
+    if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
+    if(k > kMaxKnn) return fail(ctx, LRT_ERR_RANGE, "k must be at most %u", kMaxKnn);
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_photon_irradiance_dev(lrt_context* ctx, int32_t map, const float* points_dev, const float* normals_dev,
+                              uint32_t n, float radius, int32_t max_depth, uint32_t k, float* rgb_dev) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    const int st = irradiance_check(ctx, map, k);
+    if(st != LRT_OK) return st;
+    if(n == 0) return LRT_OK;
+    if(!points_dev || !normals_dev || !rgb_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    return irradiance_launch(ctx, map, points_dev, normals_dev, n, radius, max_depth, k, rgb_dev);
+}
+
 int lrt_photon_irradiance(lrt_context* ctx, int32_t map, const float* points, const float* normals, uint32_t n,
                           float radius, int32_t max_depth, uint32_t k, float* rgb_out) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
-    if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
-    if(k > kMaxKnn) return fail(ctx, LRT_ERR_RANGE, "k must be at most %u", kMaxKnn);
+    const int st = irradiance_check(ctx, map, k);
+    if(st != LRT_OK) return st;
     if(n == 0) return LRT_OK;
     if(!points || !normals || !rgb_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null buffer");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
     const size_t pb = 12ull * n;
     LRT_CUDA(ctx, ctx->scratch_a.ensure(3 * pb));
     float* base = ctx->scratch_a.as<float>();
     LRT_CUDA(ctx, cudaMemcpyAsync(base, points, pb, cudaMemcpyHostToDevice, ctx->stream));
     LRT_CUDA(ctx, cudaMemcpyAsync(base + 3ull * n, normals, pb, cudaMemcpyHostToDevice, ctx->stream));
-    const int grid = grid_for(ctx, (const void*)k_irradiance, kBlock);
-    k_irradiance<<<grid, kBlock, 0, ctx->stream>>>(view_of(ctx->maps[map]), base, base + 3ull * n, n, radius, max_depth, k,
-                                                   base + 6ull * n);
-    LRT_CUDA(ctx, cudaGetLastError());
+    const int r = irradiance_launch(ctx, map, base, base + 3ull * n, n, radius, max_depth, k, base + 6ull * n);
+    if(r != LRT_OK) return r;
     LRT_CUDA(ctx, cudaMemcpyAsync(rgb_out, base + 6ull * n, pb, cudaMemcpyDeviceToHost, ctx->stream));
     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return LRT_OK;

@@ -1,7 +1,10 @@
 """Material parameters of a scene as a flat vector, and the caller side of liblrt's path-replay adjoint.
 
 A parameter is one scalar of one material: an albedo channel (diffuse_reflectance of diffuse, plastic
-and rough plastic), a roughness (alpha of the rough materials) or a conductor eta / k channel. The
+and rough plastic; the coat tint specular_reflectance of the smooth and rough coatings), a roughness
+(alpha of the rough materials) or a conductor eta / k channel. On the seven-material differentiation
+workload (the three wall albedos, the seven sphere materials and the coatings' nested plastic and rough
+glass) that is 38 scalars: 5 roughnesses, 9 RGB albedos and the conductor's eta and k. The
 channels of one field form a group, moved together, since channel c of a BSDF value moves only with
 channel c of the field; a roughness is a group of its own. For each group the library receives the
 scene's material list moved by +step and by -step (with the rough-transmittance tables re-sliced
@@ -21,11 +24,13 @@ import scenes
 
 ALBEDO_TYPES = (abi.MAT_DIFFUSE, abi.MAT_PLASTIC, abi.MAT_ROUGH_PLASTIC)
 ROUGH_TYPES = (abi.MAT_ROUGH_DIELECTRIC, abi.MAT_ROUGH_CONDUCTOR, abi.MAT_ROUGH_PLASTIC, abi.MAT_ROUGH_COATING)
+COATING_TYPES = (abi.MAT_COATING, abi.MAT_ROUGH_COATING)
 
 
 def scene_params(materials, only=None):
     """[(material, field, channel)] of every differentiable scalar, in material order: alpha first, then
-    diffuse_reflectance, eta, k channels. `only`: restrict to these material indices."""
+    diffuse_reflectance (coatings: specular_reflectance), eta, k channels. `only`: restrict to these
+    material indices."""
     out = []
     for i, m in enumerate(materials):
         if only is not None and i not in only:
@@ -35,6 +40,8 @@ def scene_params(materials, only=None):
             out.append((i, "alpha", None))
         if t in ALBEDO_TYPES:
             out += [(i, "diffuse_reflectance", c) for c in range(3)]
+        if t in COATING_TYPES:
+            out += [(i, "specular_reflectance", c) for c in range(3)]
         if t == abi.MAT_ROUGH_CONDUCTOR:
             out += [(i, "eta", c) for c in range(3)] + [(i, "k", c) for c in range(3)]
     return out
@@ -45,9 +52,14 @@ def param_name(materials, p) -> str:
     return "m%d.%s%s" % (i, field, "" if c is None else "[%d]" % c)
 
 
+# the values lrt_abi.material_descs gives a field a material dict leaves out
+FIELD_DEFAULTS = {"specular_reflectance": (1.0, 1.0, 1.0), "diffuse_reflectance": (0.5, 0.5, 0.5),
+                  "eta": (0.0, 0.0, 0.0), "k": (0.0, 0.0, 0.0), "alpha": 0.0}
+
+
 def get_value(materials, p) -> float:
     i, field, c = p
-    v = materials[i][field]
+    v = materials[i].get(field, FIELD_DEFAULTS[field])
     return float(v if c is None else v[c])
 
 
@@ -56,7 +68,7 @@ def set_value(materials, p, value) -> None:
     if c is None:
         materials[i][field] = float(value)
     else:
-        v = [float(x) for x in materials[i][field]]
+        v = [float(x) for x in materials[i].get(field, FIELD_DEFAULTS[field])]
         v[c] = float(value)
         materials[i][field] = tuple(v)
 

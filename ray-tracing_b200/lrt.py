@@ -33,6 +33,7 @@ EXPORTS = [
     "lrt_render_adjoint_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
     "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
+    "lrt_photon_irradiance_dev",
     "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
 ]
 
@@ -103,6 +104,7 @@ def lib():
         L.lrt_photon_map_build.argtypes = [vp, i32, P(abi.Photon), u32, f32]
         L.lrt_photon_knn.argtypes = [vp, i32, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
         L.lrt_photon_irradiance.argtypes = [vp, i32, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
+        L.lrt_photon_irradiance_dev.argtypes = [vp, i32, vp, vp, u32, f32, i32, u32, vp]
         L.lrt_photon_preprocess.argtypes = [vp, u32, u32, i32, i32, f32, P(abi.PhotonRenderParams), P(u64)]
         L.lrt_render_photon.argtypes = [vp, P(abi.RenderParams), P(abi.PhotonRenderParams), P(f32)]
         L.lrt_render_photon_dev.argtypes = [vp, P(abi.RenderParams), P(abi.PhotonRenderParams), vp]
@@ -390,6 +392,8 @@ class Context:
             "stage_ms": {abi.STAGE_NAMES[i]: s.stage_ms[i] for i in range(6)},
             "stage_launches": {abi.STAGE_NAMES[i]: s.stage_launches[i] for i in range(6)},
             "rays_at_depth": [int(s.rays_at_depth[i]) for i in range(16)],
+            "knn_queries": s.knn_queries, "knn_nodes_visited": s.knn_nodes_visited,
+            "knn_photons_tested": s.knn_photons_tested, "knn_photons_found": s.knn_photons_found,
         }
 
     def reset_stats(self):
@@ -442,6 +446,12 @@ class Context:
 
     def render_photon_dev(self, params: abi.RenderParams, pp: abi.PhotonRenderParams, rgb_ptr: int):
         self._check(lib().lrt_render_photon_dev(self.handle, C.byref(params), C.byref(pp), C.c_void_p(rgb_ptr)))
+
+    def photon_irradiance_dev(self, map_id: int, points_ptr: int, normals_ptr: int, n: int, radius: float,
+                              max_depth: int, k: int, rgb_ptr: int):
+        self._check(lib().lrt_photon_irradiance_dev(self.handle, map_id, C.c_void_p(points_ptr),
+                                                    C.c_void_p(normals_ptr), n, radius, max_depth, k,
+                                                    C.c_void_p(rgb_ptr)))
 
     def photon_irradiance(self, map_id: int, points, normals, radius: float, max_depth: int, k: int):
         points = np.ascontiguousarray(points, dtype=np.float32)

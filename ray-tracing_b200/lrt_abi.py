@@ -154,7 +154,8 @@ class RenderStats(C.Structure):
                 ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64),
                 ("shading_events", C.c_uint64),
                 ("kernel_launches", C.c_uint64), ("stage_ms", C.c_float * 6), ("stage_launches", C.c_uint32 * 6),
-                ("rays_at_depth", C.c_uint64 * 16)]
+                ("rays_at_depth", C.c_uint64 * 16), ("knn_queries", C.c_uint64), ("knn_nodes_visited", C.c_uint64),
+                ("knn_photons_tested", C.c_uint64), ("knn_photons_found", C.c_uint64)]
 
 
 # numpy views of the record arrays

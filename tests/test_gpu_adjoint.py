@@ -1,18 +1,21 @@
 """Path-replay adjoint of the path tracer (lrt_render_adjoint) against finite differences.
 
 * Linear functional F = sum_pixels <w, image> with fixed weights w: the adjoint (detached sampling)
-  and the central difference of F with common random numbers (the same samples at +h and -h) are
-  unbiased estimates of the same dE[F]/dparam, so over independent sample ranges their paired
-  difference has mean zero. For parameters that no sampling decision depends on (diffuse albedos,
-  conductor eta / k) the two agree path by path up to O(h^2): h = 1e-3, |mean| <= 4 standard errors +
-  0.1%. Where a sampling decision depends on the parameter (GGX directions on alpha, the plastic lobe
-  choice on the albedo's luminance), the difference quotient with common random numbers moves by rare,
-  large jumps where a decision flips between +h and -h; its mean is right but its spread needs many
-  seeds: all 32 parameters, h = 1e-2, 48 seeds, 4 standard errors + 2%.
-  Both run without Russian roulette, whose survival probability follows the throughput and would add
-  such jumps to every parameter.
+  and the central difference of F at h = 1e-3 with common random numbers (the same samples at +h and
+  -h) are estimates of the same dE[F]/dparam. Over independent sample ranges (seeds):
+  - every parameter: the two means agree within 3 Monte Carlo standard errors (of the two estimates,
+    from their spread over the seeds), with no other allowance;
+  - parameters that no sampling decision depends on (diffuse albedos, conductor eta / k, the coat tints)
+    also agree path by path: their paired difference is float32 rounding of the images and the
+    adjoint's sums, so its mean is within 3 of its own (much smaller) standard errors plus 2e-5 of the
+    gradient (measured: at most 1.1e-5).
+  Where a sampling decision depends on the parameter (GGX directions on alpha, the plastic lobe choice
+  on the albedo's luminance), the difference quotient moves by rare, large jumps where a decision flips
+  between +h and -h: its mean is right but its spread needs many seeds. 16 seeds for the path-by-path
+  set, 96 for all 38 parameters of the differentiation workload. Both run without Russian roulette,
+  whose survival probability follows the throughput and would add such jumps to every parameter.
 * The same against central differences of the reference CPU renderer (oracle/_ref) on the rough
-  conductor scene.
+  conductor, rough plastic and rough coating scenes, their roughness among the parameters.
 * Materials moved by lrt_scene_update_materials render exactly as a fresh upload of the moved scene.
 * An L2 image loss optimised with Adam through the autograd wrapper decreases and moves the
   roughness toward the target.
@@ -42,15 +45,27 @@ def fd_jobs(scene, sphere, index, w, h, spp, seeds):
     return jobs, off
 
 
-def assert_paired(adj, fd, names, k_se=4.0, rel=0.02):
-    """adj, fd: [seeds, params] estimates on the same samples; paired mean difference within k_se SE"""
+PATH_BY_PATH_REL = 2e-5
+
+
+def assert_agree(adj, fd, names, sharp=()):
+    """adj, fd: [seeds, params] estimates on the same samples. Every parameter's means within 3 Monte Carlo
+    standard errors; the columns in `sharp` also path by path (paired mean difference within 3 of its
+    standard errors + PATH_BY_PATH_REL of the gradient)."""
+    n = adj.shape[0]
+    diff_mean = adj.mean(axis=0) - fd.mean(axis=0)
+    se_mc = np.sqrt(adj.var(axis=0, ddof=1) / n + fd.var(axis=0, ddof=1) / n)
     d = adj - fd
-    mean = d.mean(axis=0)
-    se = d.std(axis=0, ddof=1) / np.sqrt(d.shape[0])
-    scale = np.abs(fd.mean(axis=0)) + np.abs(adj.mean(axis=0))
-    bad = np.abs(mean) > k_se * se + rel * scale + 1e-7
-    assert not bad.any(), "\n".join("%s adj %.6g fd %.6g se %.3g" % (names[j], adj[:, j].mean(), fd[:, j].mean(), se[j])
-                                    for j in np.nonzero(bad)[0])
+    se_d = d.std(axis=0, ddof=1) / np.sqrt(n)
+    msgs = []
+    for j in range(adj.shape[1]):
+        if abs(diff_mean[j]) > 3.0 * se_mc[j]:
+            msgs.append("%s: adj %.6g fd %.6g, %.2f Monte Carlo SE" % (
+                names[j], adj[:, j].mean(), fd[:, j].mean(), abs(diff_mean[j]) / max(se_mc[j], 1e-300)))
+        if j in sharp and abs(diff_mean[j]) > 3.0 * se_d[j] + PATH_BY_PATH_REL * abs(fd[:, j].mean()):
+            msgs.append("%s: path by path adj %.8g fd %.8g (relative %.2e, paired SE %.2e)" % (
+                names[j], adj[:, j].mean(), fd[:, j].mean(), diff_mean[j] / abs(fd[:, j].mean()), se_d[j]))
+    assert not msgs, "\n".join(msgs)
 
 
 def central_differences(ctx, dm, jobs, floats, seeds, weights, step, params):
@@ -80,33 +95,39 @@ def library3():
     return scenes.open_box_library(level=3)
 
 
+def sharp_params(scene, params):
+    """parameters no sampling decision depends on: diffuse albedos, conductor eta / k, coat tints"""
+    return [j for j, (m, field, c) in enumerate(params)
+            if field in ("eta", "k", "specular_reflectance") or scene.materials[m]["type"] == diff.abi.MAT_DIFFUSE]
+
+
 def test_adjoint_matches_central_differences_path_by_path(ctx, library3):
     scene, sphere, index = library3
     ctx.upload(scene)
     dm = diff.Differentiable(ctx, scene)
-    assert len(dm.params) == 32
-    sharp = [j for j, (m, field, c) in enumerate(dm.params)
-             if field in ("eta", "k") or scene.materials[m]["type"] == diff.abi.MAT_DIFFUSE]
-    assert len(sharp) == 18
-    seeds = 12
+    assert len(dm.params) == 38
+    sharp = sharp_params(scene, dm.params)
+    assert len(sharp) == 24
+    seeds = 16
     jobs, floats = fd_jobs(scene, sphere, index, 20, 20, 4, seeds)
     weights = np.random.default_rng(7).uniform(0.5, 1.5, floats).astype(np.float32)
     adj = adjoint_per_seed(dm, jobs, seeds, weights)[:, sharp]
     fd = central_differences(ctx, dm, jobs, floats, seeds, weights, 1e-3, sharp)
     assert np.abs(adj).min() > 0
-    assert_paired(adj, fd, [dm.names()[j] for j in sharp], rel=1e-3)
+    assert_agree(adj, fd, [dm.names()[j] for j in sharp], sharp=range(len(sharp)))
 
 
 def test_adjoint_matches_central_differences_all(ctx, library3):
     scene, sphere, index = library3
     ctx.upload(scene)
     dm = diff.Differentiable(ctx, scene)
-    seeds = 48
+    seeds = 96
     jobs, floats = fd_jobs(scene, sphere, index, 20, 20, 4, seeds)
     weights = np.random.default_rng(7).uniform(0.5, 1.5, floats).astype(np.float32)
     adj = adjoint_per_seed(dm, jobs, seeds, weights)
-    fd = central_differences(ctx, dm, jobs, floats, seeds, weights, 1e-2, list(range(len(dm.params))))
-    assert_paired(adj, fd, dm.names())
+    fd = central_differences(ctx, dm, jobs, floats, seeds, weights, 1e-3, list(range(len(dm.params))))
+    assert np.all(np.abs(adj).max(axis=0) > 0), "a parameter without any derivative"
+    assert_agree(adj, fd, dm.names(), sharp=sharp_params(scene, dm.params))
 
 
 def test_adjoint_zero_and_linear(ctx):
@@ -137,38 +158,46 @@ def test_update_materials_equals_fresh_upload(ctx):
 
 
 @pytest.mark.skipif(not oracle.reference_available(), reason="reference build (oracle/_ref) missing")
-def test_adjoint_matches_reference_differences(ctx):
-    """central differences (h = 1e-2, same samples at +h and -h) of the reference CPU renderer on the
-    rough conductor scene: sphere alpha, eta[0], k[2] and the white wall's albedo[0]"""
-    scene = scenes.open_box("rough_conductor", level=3)
+@pytest.mark.parametrize("material", ["rough_conductor", "rough_plastic", "rough_coating"])
+def test_adjoint_matches_reference_differences(ctx, material):
+    """central differences of the reference CPU renderer (same samples at +h and -h, h = 1e-3) on the open
+    box with the sphere in `material`: the sphere's roughness (for the rough coating also its nested
+    rough glass), its other parameters, and the white wall's albedo[0]; within 3 Monte Carlo standard
+    errors (the GPU and CPU renders are not bit-identical, so no path-by-path bar)"""
+    scene = scenes.open_box(material, level=3)
     ctx.upload(scene)
-    params = [(3, "alpha", None), (3, "eta", 0), (3, "k", 2), (0, "diffuse_reflectance", 0)]
+    sphere_params = [p for p in diff.scene_params(scene.materials) if p[0] >= 3]
+    params = sphere_params + [(0, "diffuse_reflectance", 0)]
+    if material == "rough_conductor":
+        params = [p for p in params if p[1] in ("alpha", "diffuse_reflectance") or p[2] in (0, 2)]
     dm = diff.Differentiable(ctx, scene, params)
-    seeds, w, h, spp = 16, 12, 12, 4
+    seeds, w, h, spp = 32, 12, 12, 4
     weights = np.random.default_rng(5).uniform(0.5, 1.5, (h, w, 3)).astype(np.float32)
     base = dm.values()
     adj = np.zeros((seeds, len(params)))
-    fd = np.zeros((seeds, len(params)))
-    step = 1e-2
+    fd = {1e-3: np.zeros((seeds, len(params)))}
     worlds = {}
     for j in range(len(params)):
-        for sign in (1.0, -1.0):
-            v = base.copy()
-            v[j] += sign * step
-            moved = scenes.Scene(scene.objects, diff.with_values(scene.materials, params, v), scene.emitters,
-                                 scene.camera, scene.name)
-            worlds[(j, sign)] = oracle.RefWorld(moved)
+        for step in fd:
+            for sign in (1.0, -1.0):
+                v = base.copy()
+                v[j] += sign * step
+                moved = scenes.Scene(scene.objects, diff.with_values(scene.materials, params, v), scene.emitters,
+                                     scene.camera, scene.name)
+                worlds[(j, step, sign)] = oracle.RefWorld(moved)
     for k in range(seeds):
         job = scenes.job_desc(scene.camera, w, h, spp, k * spp)
         adj[k] = dm.adjoint([job], DEPTH, NO_RR, weights)
         p = scenes.render_params(w, h, spp, DEPTH, NO_RR, sample_offset=k * spp)
         for j in range(len(params)):
-            fp = float((worlds[(j, 1.0)].render(p)[0] * weights).astype(np.float64).sum())
-            fm = float((worlds[(j, -1.0)].render(p)[0] * weights).astype(np.float64).sum())
-            fd[k, j] = (fp - fm) / (2 * step)
+            for step, arr in fd.items():
+                fp = float((worlds[(j, step, 1.0)].render(p)[0] * weights).astype(np.float64).sum())
+                fm = float((worlds[(j, step, -1.0)].render(p)[0] * weights).astype(np.float64).sum())
+                arr[k, j] = (fp - fm) / (2 * step)
     for wld in worlds.values():
         wld.close()
-    assert_paired(adj, fd, dm.names())
+    assert any(p[1] == "alpha" for p in params)
+    assert_agree(adj, fd[1e-3], dm.names())
 
 
 def test_adam_moves_roughness_to_target(ctx):
