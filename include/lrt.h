@@ -28,6 +28,7 @@
  *   lrt_photon_irradiance       photon_map::estimate_irradiance src/integrator/photonmapper/photon_map.h:38-70
  *   lrt_rough_transmittance_slice  rough_transmittance ctor src/material/func/rough_transmittance.h:15-24,67-185
  *   lrt_fresnel_diffuse_reflectance fresnel_diffuse_reflectance src/material/func/fresnel.h:128-133
+ *   lrt_tonemap                 to_byte + the flip of ImageWriter::save src/io/image_write.cpp:10-20,60-69
  *   lrt_hosek_state             env_emitter ctor src/emitter/env_emitter.h:13-30 -> arhosek_rgb_skymodelstate_alloc_init
  *                               third_party/hosek/ArHosekSkyModel.cc:602-635
  */
@@ -49,10 +50,8 @@ extern "C" {
 #define LRT_ERR_IO               (-4)
 #define LRT_ERR_RANGE            (-5)
 #define LRT_ERR_NO_SCENE         (-6)
-#define LRT_ERR_QUEUE_OVERFLOW   (-7)
-#define LRT_ERR_TIMEOUT          (-8)
+/* -7, -8 and -10 are not used: no kernel of the library waits on a queue or a flag */
 #define LRT_ERR_NO_DEVICE        (-9)
-#define LRT_ERR_DEVICE_CHECK     (-10)
 
 /* ---- BSDF flags (src/material/bsdf.h:18-28) ---- */
 #define LRT_BSDF_NONE        0u
@@ -119,6 +118,9 @@ typedef struct lrt_material_desc {
     float sigma_a[3];
     float trans_table[LRT_TRANS_SAMPLES];
     float trans_internal_diffuse;
+    /* coatings: {eta, 1/eta} exactly as a constructed coating_bsdf holds them (coating.h keeps the
+     * ratio and its reciprocal, not the two indices); eta_pair[0] > 0 overrides int_ior/ext_ior */
+    float eta_pair[2];
 } lrt_material_desc;
 
 /* objects of the linear object list (src/core/hittable_list.h); order is significant */
@@ -284,6 +286,19 @@ int lrt_destroy(lrt_context* ctx);
 const char* lrt_last_error(const lrt_context* ctx);
 const char* lrt_status_string(int status);
 
+/* the float-to-byte conversion of the image writer (src/io/image_write.cpp:10-20: NaN -> 0,
+ * value^(1/2.2), clamp to [0, 0.999], truncate value*256) applied to width*height RGB pixels, with the
+ * writer's optional vertical flip (image_write.cpp:60-69) when flip != 0; bytes holds 3 per pixel.
+ * The bytes are those of the reference's to_byte with the host's powf (see lrt_tonemap_table). */
+int lrt_tonemap(lrt_context* ctx, const float* rgb, uint32_t width, uint32_t height, int flip, uint8_t* bytes);
+int lrt_tonemap_dev(lrt_context* ctx, const float* rgb_dev, uint32_t width, uint32_t height, int flip,
+                    uint8_t* bytes_dev);
+/* the 256 byte thresholds these use (host only, no device work): thresholds[k] for k = 1..255 is the
+ * smallest float whose byte is >= k under the reference's to_byte evaluated with this process's C
+ * library powf, thresholds[0] = 0; a finite value v >= 0 converts to the number of k >= 1 with
+ * thresholds[k] <= v. LRT_ERR_RANGE if the host powf made the steps non-monotonic. */
+int lrt_tonemap_table(float* thresholds /* 256 */);
+
 /* host-side utilities (no device work) */
 int lrt_rough_transmittance_slice(const char* ggx_path, float eta, float alpha,
                                   float* table_out /* LRT_TRANS_SAMPLES */, float* diffuse_out);
@@ -345,6 +360,11 @@ int lrt_kdtree_build_device(lrt_context* ctx, uint32_t n_meshes, const uint32_t*
 int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc);
 /* bytes the last upload copied host->device */
 uint64_t lrt_scene_device_bytes(const lrt_context* ctx);
+/* replaces the uploaded scene's camera by a constructed camera's own frame (camera.h:20-44 keeps
+ * origin, lower_left_corner, horizontal and vertical; the render reads only these), so a caller
+ * holding a built camera renders with its exact vectors; LRT_ERR_NO_SCENE before an upload */
+int lrt_scene_set_camera_frame(lrt_context* ctx, const float* origin, const float* lower_left_corner,
+                               const float* horizontal, const float* vertical);
 /* kd-tree of one mesh object: node count, leaf-list length, maximum depth */
 int lrt_mesh_tree_info(const lrt_context* ctx, uint32_t object, uint32_t* nodes, uint32_t* refs,
                        uint32_t* depth);
@@ -384,8 +404,14 @@ int lrt_render_dev(lrt_context* ctx, const lrt_render_params* params, float* rgb
  * 32 MiB file-scope device array that every GPU loading the library holds until exit; the caller
  * passes the output buffer and has uploaded the scene. Limits: max_depth <= 64 (LRT_ERR_RANGE beyond).
  * Its first call on a device looks the array up (cudaGetSymbolAddress) and should come before any
- * stream capture. Calls share the array: calls that overlap on the GPU race. */
+ * stream capture; later calls outside a capture look it up again (a device reset between calls gets the
+ * new address). Calls share the array: calls that overlap on the GPU race. The render statistics count
+ * its paths and launches, but the options count_work and stage_timing are not honoured here (their
+ * counters and events would need buffers of their own). */
 int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params* params, float* rgb_dev);
+/* Device allocations (cudaMalloc, pool allocations) the library has made in this process so far, for
+ * callers that check a call allocated nothing (no counterpart in the reference). */
+uint64_t lrt_device_allocations(void);
 
 /* One render job of a batch: its own pinhole camera, resolution, samples and (optionally) the material
  * of one object replaced, rendered over the uploaded scene exactly as lrt_render would render it with

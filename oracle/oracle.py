@@ -71,6 +71,7 @@ def _load(path):
         lib.ref_fresnel_diffuse_reflectance.argtypes = [f32]
         lib.ref_hosek_state.argtypes = [P(f32), f32, f32, P(C.c_double), P(C.c_double)]
         lib.ref_hardware_concurrency.restype = u32
+        lib.ref_to_bytes.argtypes = [P(f32), C.c_int, C.c_int, C.c_int, P(C.c_uint8)]
         return lib
 
 
@@ -315,6 +316,15 @@ def hosek_state(sun_direction, turbidity, albedo):
     rad = np.zeros(3, dtype=np.float64)
     ref_lib().ref_hosek_state(_p(sd), turbidity, albedo, _p(cfg, C.c_double), _p(rad, C.c_double))
     return cfg.reshape(3, 9), rad
+
+
+def to_bytes(rgb, flip=False):
+    """The reference image writer's 8-bit RGB of a (height, width, 3) float image (image_write.cpp)."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+    h, w = rgb.shape[0], rgb.shape[1]
+    out = np.empty((h, w, 3), dtype=np.uint8)
+    ref_lib().ref_to_bytes(_p(rgb), w, h, int(bool(flip)), _p(out, C.c_uint8))
+    return out
 
 
 def hardware_concurrency() -> int:

@@ -268,6 +268,12 @@ double render_tiles(const ref_world& w, const lrt_render_params* p, uint32_t thr
 
 }  // namespace
 
+// the image writer's float-to-byte conversion (io/image_write.cpp:10-20); it has external linkage in
+// the reference but no declaration in image_write.h
+namespace LinRT {
+unsigned char to_byte(global_precision value);
+}
+
 extern "C" {
 
 const char* ref_last_error() { return g_error.c_str(); }
@@ -676,6 +682,20 @@ int32_t ref_kdtree_packed(const float* bmin, const float* bmax, uint32_t n, uint
     std::copy(nodes.begin(), nodes.end(), nodes_out);
     std::copy(refs.begin(), refs.end(), refs_out);
     return 0;
+}
+
+// ImageWriter::save's byte conversion and vertical flip (image_write.cpp:53-69) of width*height RGB
+// pixels into out (3 bytes per pixel)
+void ref_to_bytes(const float* rgb, int width, int height, int flip, unsigned char* out) {
+    const size_t n = static_cast<size_t>(width) * static_cast<size_t>(height);
+    for(size_t i = 0; i < 3 * n; ++i) out[i] = LinRT::to_byte(rgb[i]);
+    if(flip) {
+        for(int y = 0; y < height / 2; ++y) {
+            unsigned char* a = out + 3ull * static_cast<size_t>(y) * width;
+            unsigned char* b = out + 3ull * static_cast<size_t>(height - 1 - y) * width;
+            std::swap_ranges(a, a + 3ull * width, b);
+        }
+    }
 }
 
 }  // extern "C"

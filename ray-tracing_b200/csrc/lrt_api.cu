@@ -410,6 +410,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
 template <bool kAdj, int kKey = -1>
 __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_t* prefix) {
     constexpr int kType = kKey >= 2 ? kKey - 2 : -1;
+    constexpr bool kMeshLights = kKey < 0;  // the per-key kernels run only on scenes without mesh lights
     BounceCounters& bc = a.counters[depth];
     if(kKey < 0 && threadIdx.x == 0) {
         uint32_t acc = 0;
@@ -456,7 +457,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
             if(!have_pdf) {
                 result += throughput * Le;
             } else {
-                const float light_pdf = pdf_emitter_direction(s, mk(0.0f), rd);
+                const float light_pdf = pdf_emitter_direction<kMeshLights>(s, mk(0.0f), rd);
                 const float w = power_heuristic(sa_pdf, light_pdf);
                 result += throughput * w * Le;
             }
@@ -475,7 +476,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
                 if(!have_pdf) {
                     result += throughput * Le;
                 } else {
-                    const float light_pdf = pdf_emitter_direction(s, ro, rd);
+                    const float light_pdf = pdf_emitter_direction<kMeshLights>(s, ro, rd);
                     const float w = power_heuristic(sa_pdf, light_pdf);
                     result += throughput * w * Le;
                 }
@@ -507,7 +508,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
         if((mat.flags & (kDiffuse | kGlossy)) != 0) {  // NEE (path_integrator.h:86-128)
             DirectSample light{};
             light.distance = kInf;
-            if(sample_emitter_direction(s, p, light_uv.x, light_uv.y, light)) {
+            if(sample_emitter_direction<kMeshLights>(s, p, light_uv.x, light_uv.y, light)) {
                 const f3 shadow_origin = p + normal * 1e-4f;
                 f3 shadow_dir = light.direction;
                 float tmax = kInf;
@@ -527,7 +528,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
                     const f3 f_cos = bsdf_eval_t<kType>(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
                     if(!is_zero(f_cos)) {
                         const float bsdf_pdf_v = bsdf_pdf_t<kType>(s.materials, s.tables, mid, ctx, rec, kSolidAngle);
-                        const float light_pdf = pdf_emitter_direction(s, p, shadow_dir);
+                        const float light_pdf = pdf_emitter_direction<kMeshLights>(s, p, shadow_dir);
                         if(light_pdf > 0.0f) {
                             const float w = power_heuristic(light_pdf, bsdf_pdf_v);
                             const f3 contrib = throughput * f_cos * light.radiance * (w / light_pdf);
@@ -649,7 +650,7 @@ static_assert(kKeys == 10, "one shading kernel per key");
 template <bool kAdj = false>
 ShadeLaunch shade_launch(lrt_context* ctx) {
     ShadeLaunch l;
-    if(!ctx->shade_per_key) {
+    if(!ctx->shade_per_key || ctx->has_mesh_lights) {
         l.grid[kKeys] = grid_for(ctx, kAdj ? (const void*)k_shade_adj : (const void*)k_shade, kBlock);
         return l;
     }
@@ -1231,10 +1232,7 @@ const char* lrt_status_string(int status) {
     case LRT_ERR_IO: return "LRT_ERR_IO";
     case LRT_ERR_RANGE: return "LRT_ERR_RANGE";
     case LRT_ERR_NO_SCENE: return "LRT_ERR_NO_SCENE";
-    case LRT_ERR_QUEUE_OVERFLOW: return "LRT_ERR_QUEUE_OVERFLOW";
-    case LRT_ERR_TIMEOUT: return "LRT_ERR_TIMEOUT";
     case LRT_ERR_NO_DEVICE: return "LRT_ERR_NO_DEVICE";
-    case LRT_ERR_DEVICE_CHECK: return "LRT_ERR_DEVICE_CHECK";
     default: return "LRT_ERR_UNKNOWN";
     }
 }
@@ -1493,12 +1491,37 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     // shading keys a hit can carry: misses, hits without a BSDF, and 2 + each material type present
     ctx->shade_keys = 3u;
     for(const MatRec& m : h.materials) ctx->shade_keys |= 1u << (2 + m.type);
+    ctx->has_mesh_lights = false;
+    for(const EmitRec& e : h.emitters) {
+        ctx->has_mesh_lights |= e.kind == LRT_EMITTER_AREA && e.shape == LRT_OBJECT_MESH;
+    }
     ctx->scene_bytes = bytes;
     ctx->has_scene = true;
     return LRT_OK;
 }
 
 uint64_t lrt_scene_device_bytes(const lrt_context* ctx) { return ctx ? ctx->scene_bytes : 0; }
+
+uint64_t lrt_device_allocations(void) { return g_device_allocations.load(); }
+
+int lrt_scene_set_camera_frame(lrt_context* ctx, const float* origin, const float* lower_left_corner,
+                               const float* horizontal, const float* vertical) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(!origin || !lower_left_corner || !horizontal || !vertical) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "camera frame: null vector");
+    }
+    if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
+    CamRec cam{};
+    for(int i = 0; i < 3; ++i) {
+        cam.origin[i] = origin[i];
+        cam.llc[i] = lower_left_corner[i];
+        cam.horizontal[i] = horizontal[i];
+        cam.vertical[i] = vertical[i];
+    }
+    ctx->host.cam = cam;
+    ctx->ds.cam = cam;
+    return LRT_OK;
+}
 
 int lrt_mesh_tree_info(const lrt_context* ctx, uint32_t object, uint32_t* nodes, uint32_t* refs, uint32_t* depth) {
     if(!ctx || !ctx->has_scene || object >= ctx->host.mesh_info.size()) return LRT_ERR_INVALID_ARGUMENT;
@@ -1783,7 +1806,12 @@ int noalloc_scratch(lrt_context* ctx, unsigned char** base) {
     if(ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) {
         return fail(ctx, LRT_ERR_RANGE, "allocation-free render supports device ordinals below %d", kNoAllocMaxDevices);
     }
-    if(!g_noalloc_base[ctx->device]) {
+    // The address is looked up again on every call outside stream capture (cheap, host side), so that a
+    // device reset that recreated the primary context between calls cannot leave a stale address; inside
+    // a capture the address of the last call outside one is used.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if(cudaStreamIsCapturing(ctx->stream, &capture) != cudaSuccess) capture = cudaStreamCaptureStatusNone;
+    if(!g_noalloc_base[ctx->device] || capture == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if(e != cudaSuccess || !p) {

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -15,6 +17,9 @@
 #include "lrt_types.h"
 
 namespace lrt {
+
+// device allocations the library has made in this process (lrt_device_allocations)
+inline std::atomic<uint64_t> g_device_allocations{0};
 
 struct DevBuf {
     void* ptr = nullptr;
@@ -32,7 +37,10 @@ struct DevBuf {
         if(n <= bytes) return cudaSuccess;
         release();
         cudaError_t e = cudaMalloc(&ptr, n);
-        if(e == cudaSuccess) bytes = n;
+        if(e == cudaSuccess) {
+            bytes = n;
+            ++g_device_allocations;
+        }
         return e;
     }
     template <typename T>
@@ -121,12 +129,13 @@ struct lrt_context {
     bool photon_tree_device = false;  // false: reference-identical tree built on the host
     bool shade_per_key = true;  // one shading kernel per material type present (false: one for all)
     uint32_t shade_keys = 3u;    // bit k: shading key k can occur in the uploaded scene
+    bool has_mesh_lights = false;  // a mesh is an area light: the one all-keys shading kernel runs
     int kd_build_device = 2;  // lrt_scene_upload's kd-trees: 0 host cores, 1 GPU, 2 GPU from 2^15 triangles
     int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
-    lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L;
+    lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L, eye_queries;
     lrt::DevBuf knn_work;  // k-NN counters (option count_work): queries, nodes, photons tested, found
     lrt::PhotonMap maps[lrt::kMaxPhotonMaps];
-    lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye;
+    lrt::DevBuf ph_counts, ph_offsets, ph_out, ph_tmp, ph_keys, ph_vals, ph_cub, ph_seg, ph_eye, ph_stage;
 };
 
 namespace lrt {
@@ -141,10 +150,13 @@ inline int fail(lrt_context* ctx, int code, const char* fmt, ...) {
     return code;
 }
 
+// A failed runtime call also sets the thread's last-error state; it is cleared here so that the next
+// launch check (cudaGetLastError) of a later call does not report this failure again.
 #define LRT_CUDA(ctx, call)                                                                                   \
     do {                                                                                                      \
         cudaError_t e_ = (call);                                                                              \
         if(e_ != cudaSuccess) {                                                                               \
+            (void)cudaGetLastError();                                                                         \
             return ::lrt::fail(ctx, e_ == cudaErrorMemoryAllocation ? LRT_ERR_OUT_OF_MEMORY : LRT_ERR_CUDA,   \
                                "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);          \
         }                                                                                                     \

@@ -1048,6 +1048,10 @@ int pack_materials(const lrt_material_desc* mats, uint32_t n, std::vector<MatRec
         if(m.type == LRT_COATING || m.type == LRT_ROUGH_COATING) {
             r.eta = m.int_ior / m.ext_ior;
             r.inv_eta = m.ext_ior / m.int_ior;
+            if(m.eta_pair[0] > 0.0f) {
+                r.eta = m.eta_pair[0];
+                r.inv_eta = m.eta_pair[1];
+            }
             const f3 optical = load3(m.sigma_a) * (-2.0f * m.thickness);
             const float avg = (expf(optical.x) + expf(optical.y) + expf(optical.z)) / 3.0f;
             r.specular_sampling_weight = 1.0f / (avg + 1.0f);

@@ -87,6 +87,7 @@ struct PBuf {
         release();
         n += n / 4;
         const cudaError_t e = cudaMallocFromPoolAsync(&ptr, n, t_pool->pool, t_pool->stream);
+        if(e == cudaSuccess) ++g_device_allocations;
         if(e == cudaSuccess) bytes = n;
         return e;
     }

@@ -157,22 +157,40 @@ __global__ void k_particles_slots(DeviceScene s, int kind, uint32_t first, uint3
     }
 }
 
-// counting pass
-__global__ void k_particles_count(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
-                                  uint32_t* counts) {
+// The gather traces each particle once: its first kStagedPhotons photons go to a staging slot of its own
+// and its photon count beside them; once the host has walked the counts in particle order (the work
+// items' cut and `shot`), the staged photons are copied to their places. A particle that stored more
+// photons than its slot holds is traced again, straight into its place (k_particles_store_list).
+constexpr uint32_t kStagedPhotons = 4;
+
+__global__ void k_particles_trace(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
+                                  lrt_photon* staging, uint32_t* counts) {
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        PhotonOut o{nullptr, 0, 0, 0};
+        PhotonOut o{staging, static_cast<uint64_t>(i) * kStagedPhotons, static_cast<uint64_t>(i + 1) * kStagedPhotons, 0};
         trace_particle(s, kind, first + i, max_depth, rr_depth, o);
         counts[i] = o.count;
     }
 }
 
-// storing pass: particle i writes at offsets[i] (absolute photon index), dropping indices >= limit
-__global__ void k_particles_store(DeviceScene s, int kind, uint32_t first, uint32_t count, int max_depth, int rr_depth,
-                                  const uint64_t* offsets, uint64_t limit, lrt_photon* out) {
+// staged photons of particles [0, count) to out[offsets[i] ..], dropping indices >= limit; one warp per
+// particle run of 32 photons would not pay: a particle has a handful
+__global__ void k_particles_place(const lrt_photon* staging, const uint32_t* counts, const uint64_t* offsets,
+                                  uint32_t count, uint64_t limit, lrt_photon* out) {
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t c = counts[i];
+        if(c > kStagedPhotons) continue;  // traced again
+        const uint64_t o = offsets[i];
+        for(uint32_t k = 0; k < c && o + k < limit; ++k) out[o + k] = staging[static_cast<uint64_t>(i) * kStagedPhotons + k];
+    }
+}
+
+// the listed particles traced again, writing at their offsets (absolute photon index), dropping indices >= limit
+__global__ void k_particles_store_list(DeviceScene s, int kind, uint32_t first, const uint32_t* list, uint32_t n,
+                                       int max_depth, int rr_depth, const uint64_t* offsets, uint64_t limit,
+                                       lrt_photon* out) {
+    for(uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t i = list[j];
         PhotonOut o{out, offsets[i], limit, 0};
-        if(offsets[i] >= limit) continue;
         trace_particle(s, kind, first + i, max_depth, rr_depth, o);
     }
 }
@@ -797,7 +815,33 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye(DeviceScene s, EyeParams 
 // (trav_step, the persistent traversal of the path tracer), and a lane whose ray is done resumes its
 // walk with the result; a lane whose camera sample is done takes the next one. Samples, sampler
 // draws, rays and additions to L are those of eye_sample, in the same order.
-enum EyeQuery : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, kQueryBsdf = 3 };
+enum EyeQueryKind : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, kQueryBsdf = 3 };
+
+// A ray query of the wavefront eye pass, in device memory with its result. A lane's walk issues the
+// shadow rays of a frame's emitter samples, and the rays of its BSDF samples when they do not recurse,
+// as one batch of up to kEyeBatch queries: their sampler draws happen in order when they are issued,
+// none depends on another's result, and the results are applied in issue order, so the radiance sums
+// are those of one query at a time. A frame's own ray and a BSDF sample that recurses go alone.
+constexpr uint32_t kEyeBatch = 16;
+
+struct EyeQuery {
+    float4 o;          // origin, t_min
+    float4 d;          // direction, t_max
+    float4 a;          // shadow: what L gains when the light is visible; BSDF sample: weight (xyz), pdf (w)
+    int32_t kind;      // EyeQueryKind
+    int32_t light;     // shadow: the light
+    int32_t any_mode;
+    int32_t best;      // result: the traversal's best object (-1 none), closest t, the hit's u, v, reference
+    float closest;
+    float u, v;
+    uint32_t ref;
+};
+
+// where eye_advance puts its queries: q == nullptr -- one query at a time, into the lane and `ts`
+struct EyeBatch {
+    EyeQuery* q;
+    uint32_t n;
+};
 
 struct EyeLane {
     Sampler smp;
@@ -824,17 +868,40 @@ __device__ __forceinline__ EyeFlags eye_flags(const DeviceScene& s, const EyePar
     return f;
 }
 
-// Advances the lane's walk until it issues a ray query (true; ts holds the ray) or finishes its sample.
+// Issues a query: without a batch, into the lane and ts (the walk then stops); with one, appended to it.
+// Returns true when the walk must stop here: always without a batch; with one, when the query must go
+// alone (its result decides what the walk does next) or the batch is full.
+__device__ __forceinline__ bool eye_issue(EyeLane& ln, TravState& ts, EyeBatch& b, uint8_t kind, const Ray& r,
+                                          float t_max, bool any_mode, f3 qa, float qpdf, int32_t qlight, bool alone) {
+    if(!b.q) {
+        ln.query = kind;
+        ln.qa = qa;
+        ln.qpdf = qpdf;
+        ln.qlight = qlight;
+        trav_begin(ts, r, 0.001f, t_max, any_mode);
+        return true;
+    }
+    EyeQuery& Q = b.q[b.n++];
+    Q.o = make_float4(r.o.x, r.o.y, r.o.z, 0.001f);
+    Q.d = make_float4(r.d.x, r.d.y, r.d.z, t_max);
+    Q.a = make_float4(qa.x, qa.y, qa.z, qpdf);
+    Q.kind = kind;
+    Q.light = qlight;
+    Q.any_mode = any_mode ? 1 : 0;
+    return alone || b.n == kEyeBatch;
+}
+
+// Advances the lane's walk until it issues a ray query (true; ts holds the ray, or the batch its queries)
+// or finishes its sample.
 __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st, KnnHeap& heap,
-                            int* overflow, TravState& ts, int frame_limit) {
+                            int* overflow, TravState& ts, int frame_limit, EyeBatch& batch) {
     const uint32_t(*table)[32] = sobol_table(s);
     constexpr uint32_t kSmooth = kDiffuse | kGlossy;
     while(ln.top >= 0) {
         EyeFrame& F = st[ln.top];
         if(F.stage == kEyeStart) {
             if(!F.evaluated) {
-                ln.query = kQueryHit;
-                trav_begin(ts, Ray{F.ro, F.rd}, 0.001f, kInf, false);
+                eye_issue(ln, ts, batch, kQueryHit, Ray{F.ro, F.rd}, kInf, false, mk(0.0f), 0.0f, -1, true);
                 return true;
             }
             if(F.obj < 0) {
@@ -935,18 +1002,18 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
                     if(light_pdf <= 0.0f) continue;
                     const float weight = power_heuristic(light_pdf * static_cast<float>(counts.emitter),
                                                          bsdf_pdf_v * static_cast<float>(counts.bsdf)) * counts.emitter_weight;
-                    ln.qa = F.tp * (value * light.radiance * (weight / light_pdf));
-                    ln.qlight = light.emitter;
-                    ln.query = kQueryShadow;
                     const Ray sr{shadow_origin, shadow_dir};
                     bool any_mode = true;
                     const EmitRec& e = s.emitters[light.emitter];
                     if(e.kind == LRT_EMITTER_AREA) {  // scene_occluded's rule
                         any_mode = !light_shape_reachable(s, s.objects[e.object], sr, 0.001f, tmax);
                     }
-                    trav_begin(ts, sr, 0.001f, tmax, any_mode);
-                    return true;
+                    if(eye_issue(ln, ts, batch, kQueryShadow, sr, tmax, any_mode,
+                                 F.tp * (value * light.radiance * (weight / light_pdf)), 0.0f, light.emitter, false)) {
+                        return true;
+                    }
                 }
+                if(batch.n > 0) return true;
             }
             F.stage = kEyeBsdf;
             F.iter = 0;
@@ -965,12 +1032,12 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
                 const F2 u = sampler_next_2d(table, ln.smp);
                 const f3 weight = bsdf_sample(s.materials, s.tables, mid, ctx, r, u.x, u.y);
                 if(is_zero(weight) || r.pdf <= 0.0f) continue;
-                ln.qa = weight;
-                ln.qpdf = r.pdf;
-                ln.query = kQueryBsdf;
-                trav_begin(ts, Ray{F.p, to_world(basis, r.wo)}, 0.001f, kInf, false);
-                return true;
+                if(eye_issue(ln, ts, batch, kQueryBsdf, Ray{F.p, to_world(basis, r.wo)}, kInf, false, weight, r.pdf,
+                             -1, sample_indirect)) {
+                    return true;
+                }
             }
+            if(batch.n > 0) return true;
         }
         --ln.top;
     }
@@ -1075,7 +1142,8 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye_persistent(DeviceScene s,
                 ln.query = kQueryNone;
                 have = true;
             }
-            if(eye_advance(s, ep, ln, frames, heap, overflow, ts, kEyeFrames)) {
+            EyeBatch one{nullptr, 0};
+            if(eye_advance(s, ep, ln, frames, heap, overflow, ts, kEyeFrames, one)) {
                 tracing = true;
             } else {
                 L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
@@ -1102,19 +1170,15 @@ enum EyeSlotState : uint32_t { kSlotIdle = 0, kSlotTracing = 1, kSlotDone = 2 };
 
 struct EyeSlot {
     EyeLane ln;
-    float4 qo;  // query ray origin, t_min
-    float4 qd;  // query ray direction, t_max
-    int32_t any_mode;
-    int32_t best;
-    float closest;
     uint32_t state;
-    MeshHit best_mesh;
+    uint32_t nq;  // queries of the slot's batch in flight
 };
 
 struct EyeWave {
     EyeSlot* slots;
     EyeFrame* frames;      // frame_limit frames per slot
-    uint32_t* queue;       // slots with a ray to trace
+    EyeQuery* queries;     // kEyeBatch per slot
+    uint32_t* queue;       // queries to trace (slot * kEyeBatch + index)
     uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch
     float4* L_out;
     int* overflow;
@@ -1130,19 +1194,27 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
         EyeSlot& S = w.slots[slot];
         if(S.state == kSlotDone) continue;
         EyeFrame* st = w.frames + static_cast<size_t>(slot) * w.frame_limit;
+        EyeQuery* queries = w.queries + static_cast<size_t>(slot) * kEyeBatch;
         EyeLane ln = S.ln;
         bool have = false;
-        if(S.state == kSlotTracing) {
-            TravState ts;
-            ts.r = Ray{f3{S.qo.x, S.qo.y, S.qo.z}, f3{S.qd.x, S.qd.y, S.qd.z}};
-            ts.any_mode = S.any_mode != 0;
-            ts.best = S.best;
-            ts.closest_so_far = S.closest;
-            ts.best_mesh = S.best_mesh;
-            eye_resume(s, ep, ln, st, w.overflow, ts, w.frame_limit);
+        if(S.state == kSlotTracing) {  // the batch's results, in issue order
+            for(uint32_t q = 0; q < S.nq; ++q) {
+                const EyeQuery& Q = queries[q];
+                ln.query = static_cast<uint8_t>(Q.kind);
+                ln.qa = f3{Q.a.x, Q.a.y, Q.a.z};
+                ln.qpdf = Q.a.w;
+                ln.qlight = Q.light;
+                TravState ts;
+                ts.r = Ray{f3{Q.o.x, Q.o.y, Q.o.z}, f3{Q.d.x, Q.d.y, Q.d.z}};
+                ts.any_mode = Q.any_mode != 0;
+                ts.best = Q.best;
+                ts.closest_so_far = Q.closest;
+                ts.best_mesh = MeshHit{Q.closest, Q.u, Q.v, Q.ref};
+                eye_resume(s, ep, ln, st, w.overflow, ts, w.frame_limit);
+            }
             have = true;
         }
-        uint32_t state = kSlotDone;
+        uint32_t state = kSlotDone, nq = 0;
         while(true) {
             if(!have) {
                 const uint32_t i = atomicAdd(&w.counters[1], 1u);
@@ -1162,12 +1234,12 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
                 have = true;
             }
             TravState ts;
-            if(eye_advance(s, ep, ln, st, heap, w.overflow, ts, w.frame_limit)) {
-                S.qo = make_float4(ts.r.o.x, ts.r.o.y, ts.r.o.z, ts.t_min);
-                S.qd = make_float4(ts.r.d.x, ts.r.d.y, ts.r.d.z, ts.t_max);
-                S.any_mode = ts.any_mode ? 1 : 0;
+            EyeBatch batch{queries, 0};
+            if(eye_advance(s, ep, ln, st, heap, w.overflow, ts, w.frame_limit, batch)) {
                 state = kSlotTracing;
-                w.queue[warp_append(&w.counters[0])] = slot;
+                nq = batch.n;
+                const uint32_t base = atomicAdd(&w.counters[0], nq);
+                for(uint32_t q = 0; q < nq; ++q) w.queue[base + q] = slot * kEyeBatch + q;
                 break;
             }
             w.L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
@@ -1175,9 +1247,12 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
         }
         S.ln = ln;
         S.state = state;
+        S.nq = nq;
     }
 }
 
+// the queued queries with the persistent traversal (closest hit, or any hit for occlusion without a
+// reachable light); results written beside each query
 __global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) {
     const uint32_t n = w.counters[0];
     TravItem stack[kStackSize];
@@ -1185,23 +1260,25 @@ __global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) 
     TravState st;
     TraceCount cnt{0, 0};
     bool active = false, exhausted = n == 0;
-    uint32_t slot = 0;
+    uint32_t entry = 0;
     while(true) {
         if(!exhausted && __popc(__ballot_sync(0xffffffffu, !active)) >= 16) {  // refill half-idle warps
             const uint32_t i = warp_fetch(&w.counters[2], !active, n, exhausted);
             if(!active && i < n) {
-                slot = w.queue[i];
-                const EyeSlot& S = w.slots[slot];
-                trav_begin(st, Ray{f3{S.qo.x, S.qo.y, S.qo.z}, f3{S.qd.x, S.qd.y, S.qd.z}}, S.qo.w, S.qd.w, S.any_mode != 0);
+                entry = w.queue[i];
+                const EyeQuery& Q = w.queries[entry];
+                trav_begin(st, Ray{f3{Q.o.x, Q.o.y, Q.o.z}, f3{Q.d.x, Q.d.y, Q.d.z}}, Q.o.w, Q.d.w, Q.any_mode != 0);
                 active = true;
             }
         }
         if(!__any_sync(0xffffffffu, active)) break;
         if(active && trav_step<false>(s, st, stack, tl_stack, cnt)) {
-            EyeSlot& S = w.slots[slot];
-            S.best = st.best;
-            S.closest = st.closest_so_far;
-            S.best_mesh = st.best_mesh;
+            EyeQuery& Q = w.queries[entry];
+            Q.best = st.best;
+            Q.closest = st.closest_so_far;
+            Q.u = st.best_mesh.u;
+            Q.v = st.best_mesh.v;
+            Q.ref = st.best_mesh.ref;
             active = false;
         }
     }
@@ -1275,18 +1352,21 @@ int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t
     const uint64_t chunk = std::min<uint64_t>(granularity * batches_per_launch, 1ull << 24);
     LRT_CUDA(ctx, ctx->ph_out.ensure(sizeof(lrt_photon) * static_cast<size_t>(requested)));
     LRT_CUDA(ctx, ctx->ph_counts.ensure(4 * chunk));
-    LRT_CUDA(ctx, ctx->ph_offsets.ensure(8 * chunk));
+    LRT_CUDA(ctx, ctx->ph_offsets.ensure(8 * chunk + 4 * chunk));
+    LRT_CUDA(ctx, ctx->ph_stage.ensure(sizeof(lrt_photon) * kStagedPhotons * chunk));
     std::vector<uint32_t> counts(chunk);
     std::vector<uint64_t> offsets(chunk);
+    std::vector<uint32_t> again;
     uint64_t stored = 0, shot = 0, returned = 0, next = 0;
     bool done = false;
-    const int grid = grid_for(ctx, (const void*)k_particles_count, kBlock);
+    const int grid = grid_for(ctx, (const void*)k_particles_trace, kBlock);
+    uint32_t* d_again = reinterpret_cast<uint32_t*>(ctx->ph_offsets.as<uint64_t>() + chunk);
     while(!done) {
         if(next + chunk > 0xffffffffull) return fail(ctx, LRT_ERR_RANGE, "particle index space exhausted");
         const uint32_t first = static_cast<uint32_t>(next);
         const uint32_t n = static_cast<uint32_t>(chunk);
-        k_particles_count<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, n, max_depth, rr_depth,
-                                                            ctx->ph_counts.as<uint32_t>());
+        k_particles_trace<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, n, max_depth, rr_depth,
+                                                            ctx->ph_stage.as<lrt_photon>(), ctx->ph_counts.as<uint32_t>());
         LRT_CUDA(ctx, cudaGetLastError());
         LRT_CUDA(ctx, cudaMemcpyAsync(counts.data(), ctx->ph_counts.ptr, 4 * chunk, cudaMemcpyDeviceToHost, ctx->stream));
         LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1323,10 +1403,22 @@ int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t
         }
         if(taken > 0) {
             LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_offsets.ptr, offsets.data(), 8 * taken, cudaMemcpyHostToDevice, ctx->stream));
-            k_particles_store<<<grid, kBlock, 0, ctx->stream>>>(ctx->ds, kind, first, static_cast<uint32_t>(taken), max_depth,
-                                                                rr_depth, ctx->ph_offsets.as<uint64_t>(), requested,
-                                                                ctx->ph_out.as<lrt_photon>());
+            k_particles_place<<<blocks_for(static_cast<uint32_t>(taken)), kBlock, 0, ctx->stream>>>(
+                ctx->ph_stage.as<lrt_photon>(), ctx->ph_counts.as<uint32_t>(), ctx->ph_offsets.as<uint64_t>(),
+                static_cast<uint32_t>(taken), requested, ctx->ph_out.as<lrt_photon>());
             LRT_CUDA(ctx, cudaGetLastError());
+            again.clear();
+            for(uint64_t i = 0; i < taken; ++i) {
+                if(counts[i] > kStagedPhotons && offsets[i] < requested) again.push_back(static_cast<uint32_t>(i));
+            }
+            if(!again.empty()) {
+                const uint32_t na = static_cast<uint32_t>(again.size());
+                LRT_CUDA(ctx, cudaMemcpyAsync(d_again, again.data(), 4ull * na, cudaMemcpyHostToDevice, ctx->stream));
+                k_particles_store_list<<<blocks_for(na), kBlock, 0, ctx->stream>>>(
+                    ctx->ds, kind, first, d_again, na, max_depth, rr_depth, ctx->ph_offsets.as<uint64_t>(), requested,
+                    ctx->ph_out.as<lrt_photon>());
+                LRT_CUDA(ctx, cudaGetLastError());
+            }
             LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
         next += chunk;
@@ -1619,17 +1711,20 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     const int grid = grid_for(ctx, persistent ? (const void*)k_photon_eye_persistent : (const void*)k_photon_eye, kBlock);
     // wavefront slots: frames up to max_depth deep (a child is pushed only below max_depth)
     const int frame_limit = pp->max_depth;
-    const uint64_t slot_bytes = sizeof(EyeSlot) + sizeof(EyeFrame) * static_cast<uint64_t>(frame_limit);
+    const uint64_t slot_bytes = sizeof(EyeSlot) + sizeof(EyeFrame) * static_cast<uint64_t>(frame_limit) +
+                                (sizeof(EyeQuery) + 4) * kEyeBatch;
     const uint32_t n_slots = static_cast<uint32_t>(std::min<uint64_t>(1u << 20, (2ull << 30) / slot_bytes));
     EyeWave w{};
     if(mode == 2) {
         LRT_CUDA(ctx, ctx->eye_slots.ensure(sizeof(EyeSlot) * n_slots));
         LRT_CUDA(ctx, ctx->eye_frames.ensure(sizeof(EyeFrame) * static_cast<size_t>(n_slots) * frame_limit));
-        LRT_CUDA(ctx, ctx->eye_queue.ensure(4ull * n_slots + 64));
+        LRT_CUDA(ctx, ctx->eye_queue.ensure(4ull * kEyeBatch * n_slots + 64));
+        LRT_CUDA(ctx, ctx->eye_queries.ensure(sizeof(EyeQuery) * kEyeBatch * static_cast<size_t>(n_slots)));
         w.slots = ctx->eye_slots.as<EyeSlot>();
         w.frames = ctx->eye_frames.as<EyeFrame>();
+        w.queries = ctx->eye_queries.as<EyeQuery>();
         w.queue = ctx->eye_queue.as<uint32_t>();
-        w.counters = w.queue + n_slots;
+        w.counters = w.queue + static_cast<size_t>(kEyeBatch) * n_slots;
         w.L_out = L;
         w.overflow = overflow;
         w.frame_limit = frame_limit;
@@ -1665,17 +1760,23 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
                 w.sample_begin = p->sample_offset + sb;
                 LRT_CUDA(ctx, cudaMemsetAsync(w.slots, 0, sizeof(EyeSlot) * w.n_slots, ctx->stream));
                 LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 16, ctx->stream));
+                // rounds of (advance every slot to its next query, trace the queued queries), kEyeRounds at a
+                // time without a host round trip: the trace kernel reads the queue length on the device, and
+                // rounds past the last query find every slot done and launch no work. The host reads the
+                // last round's queue length after each batch: zero means every sample is finished.
+                constexpr int kEyeRounds = 16;
                 while(true) {
-                    LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 4, ctx->stream));
-                    LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 4, ctx->stream));
-                    k_eye_shade<<<g_shade, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
+                    for(int r = 0; r < kEyeRounds; ++r) {
+                        LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 4, ctx->stream));
+                        LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 4, ctx->stream));
+                        k_eye_shade<<<g_shade, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
+                        k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
+                    }
+                    ctx->stats.kernel_launches += 2 * kEyeRounds;
                     uint32_t queued = 0;
                     LRT_CUDA(ctx, cudaMemcpyAsync(&queued, w.counters, 4, cudaMemcpyDeviceToHost, ctx->stream));
                     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-                    ctx->stats.kernel_launches += 1;
                     if(queued == 0) break;
-                    k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
-                    ctx->stats.kernel_launches += 1;
                 }
             } else if(persistent) {
                 LRT_CUDA(ctx, cudaMemsetAsync(fetch, 0, 4, ctx->stream));

@@ -16,6 +16,16 @@ namespace lrt {
 constexpr float kInf = __builtin_huge_valf();
 constexpr int kStackSize = 48;  // sah_kdtree.h:80 (depth limit <= 48 keeps the stack within bounds)
 
+// One deferred far child of the kd traversal. The reference's stack item also holds the child's
+// entry distance (sah_kdtree.h:82-84), but that value always equals the current exit distance at
+// the moment the item is popped: a push sets the near child's maxt to the split distance, which is
+// the far child's mint, and every later push is popped before this one while nothing else changes
+// maxt. So a pop sets mint = maxt, then restores maxt from the item, and an item fits in 8 bytes.
+struct __align__(8) TravItem {
+    uint32_t node;
+    float maxt;
+};
+
 struct Ray {
     f3 o;
     f3 d;
@@ -182,11 +192,7 @@ __device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o
     float closest = t_max;
     bool hit_any = false;
     const float inv_x = 1.0f / r.d.x, inv_y = 1.0f / r.d.y, inv_z = 1.0f / r.d.z;
-    struct Item {
-        uint32_t node;
-        float mint, maxt;
-    };
-    Item stack[kStackSize];
+    TravItem stack[kStackSize];
     int top = 0;
     float mint = t_min;
     float maxt = closest;
@@ -213,12 +219,7 @@ __device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o
             } else if(t_plane < mint) {
                 node = second_child;
             } else {
-                if(top < kStackSize) {
-                    stack[top].node = second_child;
-                    stack[top].mint = t_plane;
-                    stack[top].maxt = maxt;
-                    ++top;
-                }
+                if(top < kStackSize) stack[top++] = TravItem{second_child, maxt};
                 node = first_child;
                 maxt = t_plane;
             }
@@ -243,7 +244,7 @@ __device__ __forceinline__ bool trace_mesh(const DeviceScene& s, const ObjRec& o
         if(top == 0) break;
         --top;
         node = stack[top].node;
-        mint = stack[top].mint;
+        mint = maxt;
         maxt = stack[top].maxt;
     }
     return hit_any;
@@ -471,11 +472,6 @@ __device__ __forceinline__ bool scene_occluded(const DeviceScene& s, const Ray& 
 // analytic shapes on the way), or runs one descend-to-leaf + leaf of the current mesh's traversal. The
 // nodes, triangles and their order per ray are exactly those of trace_mesh / scene_hit; persistent
 // kernels interleave rays so that a lane whose ray finishes takes a new one at once.
-struct TravItem {
-    uint32_t node;
-    float mint, maxt;
-};
-
 struct TravState {
     Ray r;
     float t_min;
@@ -655,12 +651,7 @@ __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, T
         } else if(t_plane < st.mint) {
             st.node = second_child;
         } else {
-            if(st.top < kStackSize) {
-                stack[st.top].node = second_child;
-                stack[st.top].mint = t_plane;
-                stack[st.top].maxt = st.maxt;
-                ++st.top;
-            }
+            if(st.top < kStackSize) stack[st.top++] = TravItem{second_child, st.maxt};
             st.node = first_child;
             st.maxt = t_plane;
         }
@@ -691,7 +682,7 @@ __device__ __forceinline__ bool trav_step(const DeviceScene& s, TravState& st, T
         } else {
             --st.top;
             st.node = stack[st.top].node;
-            st.mint = stack[st.top].mint;
+            st.mint = st.maxt;
             st.maxt = stack[st.top].maxt;
         }
     }
@@ -822,11 +813,14 @@ static __device__ __noinline__ void mesh_light_sample_position(const DeviceScene
 }
 
 // hittable::sample_position of the emitter's shape (rectangle.h:65-69, sphere.h:60-67,
-// triangle_mesh.h:109-138)
+// triangle_mesh.h:109-138). kMeshLights = false compiles the mesh branch out, for kernels that only
+// run on scenes whose lights are rectangles and spheres (the out-of-line mesh call costs registers
+// in every caller that keeps it).
+template <bool kMeshLights = true>
 __device__ __forceinline__ void emitter_sample_position(const DeviceScene& s, const EmitRec& e, float sx, float sy,
                                                         f3& p, f3& n, float& pdf) {
     const ObjRec& o = s.objects[e.object];
-    if(o.kind == LRT_OBJECT_MESH) {
+    if(kMeshLights && o.kind == LRT_OBJECT_MESH) {
         mesh_light_sample_position(s, e, sx, sy, p, n, pdf);
     } else if(o.kind == LRT_OBJECT_RECTANGLE) {
         p = load3(o.corner) + sx * load3(o.edge_u) + sy * load3(o.edge_v);
@@ -845,12 +839,13 @@ __device__ __forceinline__ void emitter_sample_position(const DeviceScene& s, co
 }
 
 // area_emitter::sample (area_emitter.h:17-49)
+template <bool kMeshLights = true>
 __device__ __forceinline__ bool area_sample(const DeviceScene& s, const EmitRec& e, f3 shading_point, float sx,
                                             float sy, DirectSample& out) {
     if(e.area <= 0.0f) return false;
     f3 p, n;
     float pdf_area = 0.0f;
-    emitter_sample_position(s, e, sx, sy, p, n, pdf_area);
+    emitter_sample_position<kMeshLights>(s, e, sx, sy, p, n, pdf_area);
     const f3 to_light = p - shading_point;
     const float dist2 = length_squared(to_light);
     if(dist2 < 1e-8f) return false;
@@ -884,6 +879,7 @@ __device__ __forceinline__ bool env_sample(const EmitRec& e, float sx, float sy,
 }
 
 // scene::sample_emitter_direction (scene.h:73-93): uniform 1/n light pick on sample.x
+template <bool kMeshLights = true>
 __device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f3 shading_point, float sx, float sy,
                                                          DirectSample& out) {
     const int32_t count = s.n_emitters;
@@ -895,7 +891,7 @@ __device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f
     const EmitRec& e = s.emitters[index];
     out.distance = kInf;
     out.pdf = 0.0f;
-    const bool ok = e.kind == LRT_EMITTER_ENV ? env_sample(e, rx, sy, out) : area_sample(s, e, shading_point, rx, sy, out);
+    const bool ok = e.kind == LRT_EMITTER_ENV ? env_sample(e, rx, sy, out) : area_sample<kMeshLights>(s, e, shading_point, rx, sy, out);
     if(!ok) return false;
     out.emitter = index;
     out.pdf *= 1.0f / static_cast<float>(count);
@@ -918,6 +914,7 @@ static __device__ __noinline__ bool mesh_light_hit(const DeviceScene& s, int32_t
 }
 
 // area_emitter::pdf (area_emitter.h:51-72): re-intersects the light shape
+template <bool kMeshLights = true>
 __device__ __forceinline__ float area_pdf(const DeviceScene& s, const EmitRec& e, f3 shading_point, f3 direction) {
     if(e.area <= 0.0f) return 0.0f;
     const f3 dir = normalize(direction);
@@ -926,7 +923,7 @@ __device__ __forceinline__ float area_pdf(const DeviceScene& s, const EmitRec& e
     float t;
     f3 normal;
     if(o.kind == LRT_OBJECT_MESH) {
-        if(!mesh_light_hit(s, e.object, r, t, normal)) return 0.0f;
+        if(!kMeshLights || !mesh_light_hit(s, e.object, r, t, normal)) return 0.0f;
     } else if(o.kind == LRT_OBJECT_RECTANGLE) {
         f3 p;
         if(!hit_rectangle(o, r, 0.001f, kInf, t, p)) return 0.0f;
@@ -952,6 +949,7 @@ __device__ __forceinline__ float env_pdf(const EmitRec& e, f3 direction) {
 }
 
 // scene::pdf_emitter_direction (scene.h:96-108)
+template <bool kMeshLights = true>
 __device__ __forceinline__ float pdf_emitter_direction(const DeviceScene& s, f3 shading_point, f3 direction) {
     const int32_t count = s.n_emitters;
     if(count <= 0) return 0.0f;
@@ -959,7 +957,7 @@ __device__ __forceinline__ float pdf_emitter_direction(const DeviceScene& s, f3 
     float sum = 0.0f;
     for(int32_t i = 0; i < count; ++i) {
         const EmitRec& e = s.emitters[i];
-        const float p = e.kind == LRT_EMITTER_ENV ? env_pdf(e, direction) : area_pdf(s, e, shading_point, direction);
+        const float p = e.kind == LRT_EMITTER_ENV ? env_pdf(e, direction) : area_pdf<kMeshLights>(s, e, shading_point, direction);
         sum += selection * p;
     }
     return sum;

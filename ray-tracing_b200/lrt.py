@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "liblrt.so")
 EXPORTS = [
     "lrt_create", "lrt_destroy", "lrt_last_error", "lrt_status_string", "lrt_rough_transmittance_slice",
     "lrt_fresnel_diffuse_reflectance", "lrt_hosek_state", "lrt_kdtree_build", "lrt_kdtree_build_device", "lrt_scene_upload", "lrt_scene_device_bytes",
+    "lrt_scene_set_camera_frame", "lrt_tonemap", "lrt_tonemap_dev", "lrt_tonemap_table", "lrt_device_allocations",
     "lrt_mesh_tree_info", "lrt_trace", "lrt_trace_dev", "lrt_occluded", "lrt_bsdf_evaluate", "lrt_sky_eval",
     "lrt_sampler_values", "lrt_camera_rays", "lrt_emitter_query", "lrt_render", "lrt_render_dev",
     "lrt_render_dev_noalloc", "lrt_render_batch", "lrt_render_batch_dev",
@@ -36,6 +37,15 @@ EXPORTS = [
     "lrt_photon_irradiance_dev",
     "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
 ]
+
+
+def tonemap_table() -> np.ndarray:
+    """The 256 byte thresholds of the image writer's float-to-byte conversion (host only)."""
+    out = np.zeros(256, dtype=np.float32)
+    st = lib().lrt_tonemap_table(ptr(out, C.c_float))
+    if st != 0:
+        raise LrtError(st, "lrt_tonemap_table")
+    return out
 
 
 class LrtError(RuntimeError):
@@ -71,6 +81,12 @@ def lib():
         L.lrt_scene_upload.argtypes = [vp, P(abi.SceneDesc)]
         L.lrt_scene_device_bytes.restype = u64
         L.lrt_scene_device_bytes.argtypes = [vp]
+        L.lrt_scene_set_camera_frame.argtypes = [vp, P(f32), P(f32), P(f32), P(f32)]
+        L.lrt_device_allocations.restype = u64
+        L.lrt_device_allocations.argtypes = []
+        L.lrt_tonemap.argtypes = [vp, P(f32), u32, u32, C.c_int, P(C.c_uint8)]
+        L.lrt_tonemap_dev.argtypes = [vp, vp, u32, u32, C.c_int, vp]
+        L.lrt_tonemap_table.argtypes = [P(f32)]
         L.lrt_mesh_tree_info.argtypes = [vp, u32, P(u32), P(u32), P(u32)]
         L.lrt_trace.argtypes = [vp, P(abi.Ray), u32, P(abi.Hit)]
         L.lrt_trace_dev.argtypes = [vp, vp, u32, vp]
@@ -244,6 +260,21 @@ class Context:
 
     def scene_bytes(self) -> int:
         return int(lib().lrt_scene_device_bytes(self.handle))
+
+    def tonemap(self, rgb, flip=False):
+        """8-bit RGB of a (height, width, 3) float image as the reference's image writer converts it."""
+        rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+        h, w = rgb.shape[0], rgb.shape[1]
+        out = np.empty((h, w, 3), dtype=np.uint8)
+        self._check(lib().lrt_tonemap(self.handle, ptr(rgb, C.c_float), w, h, int(bool(flip)), ptr(out, C.c_uint8)))
+        return out
+
+    def set_camera_frame(self, origin, lower_left_corner, horizontal, vertical):
+        """Render with a constructed camera's own frame vectors instead of the uploaded camera's."""
+        v = [np.ascontiguousarray(x, dtype=np.float32).reshape(3) for x in
+             (origin, lower_left_corner, horizontal, vertical)]
+        self._check(lib().lrt_scene_set_camera_frame(self.handle, *[ptr(x, C.c_float) for x in v]))
+        return self
 
     def kdtree_build_device(self, meshes):
         """GPU SAH kd-trees of several meshes at once; meshes = [(bmin, bmax), ...] with (n, 3) float32

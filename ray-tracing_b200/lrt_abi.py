@@ -13,8 +13,7 @@ import numpy as np
 LRT_OK = 0
 STATUS_NAMES = {
     0: "LRT_OK", -1: "LRT_ERR_INVALID_ARGUMENT", -2: "LRT_ERR_CUDA", -3: "LRT_ERR_OUT_OF_MEMORY",
-    -4: "LRT_ERR_IO", -5: "LRT_ERR_RANGE", -6: "LRT_ERR_NO_SCENE", -7: "LRT_ERR_QUEUE_OVERFLOW",
-    -8: "LRT_ERR_TIMEOUT", -9: "LRT_ERR_NO_DEVICE", -10: "LRT_ERR_DEVICE_CHECK",
+    -4: "LRT_ERR_IO", -5: "LRT_ERR_RANGE", -6: "LRT_ERR_NO_SCENE", -9: "LRT_ERR_NO_DEVICE",
 }
 for _code, _name in STATUS_NAMES.items():
     globals()[_name] = _code
@@ -42,7 +41,7 @@ class MaterialDesc(C.Structure):
         ("diffuse_reflectance", C.c_float * 3), ("specular_reflectance", C.c_float * 3),
         ("specular_transmittance", C.c_float * 3), ("eta", C.c_float * 3), ("k", C.c_float * 3),
         ("sigma_a", C.c_float * 3), ("trans_table", C.c_float * TRANS_SAMPLES),
-        ("trans_internal_diffuse", C.c_float),
+        ("trans_internal_diffuse", C.c_float), ("eta_pair", C.c_float * 2),
     ]
 
 
@@ -213,6 +212,9 @@ def material_descs(materials, out=None, start=0):
             assert t.size == TRANS_SAMPLES
             d.trans_table = (C.c_float * TRANS_SAMPLES)(*[float(x) for x in t])
         d.trans_internal_diffuse = float(m.get("trans_internal_diffuse", 0.0))
+        pair = m.get("eta_pair")
+        if pair is not None:
+            d.eta_pair = (C.c_float * 2)(float(pair[0]), float(pair[1]))
     return out
 
 

@@ -269,6 +269,32 @@ def light_kat():
     save("light_kat.npz", **out)
 
 
+def image_out_kat():
+    """the image writer's float-to-byte conversion (io/image_write.cpp:10-20) and its vertical flip:
+    special values, the values on either side of every byte boundary ((k/256)^2.2 and its float
+    neighbours), and log-normal radiance, laid out as rows of 23 RGB pixels"""
+    rng = np.random.default_rng(SEED + 13)
+    special = np.array([0.0, -0.0, np.nan, np.inf, -np.inf, -1.0, -1e-30, 1e-45, 1e-38, 1e-30, 1e-10,
+                        1.0, 0.5, 2.0, 1e30, 3.4e38], dtype=np.float32)
+    edges = []
+    for k in range(1, 257):
+        e = np.float32((k / 256.0) ** 2.2)
+        up, down = e, e
+        edges.append(e)
+        for _ in range(3):
+            up = np.nextafter(up, np.float32(np.inf))
+            down = np.nextafter(down, np.float32(-np.inf))
+            edges += [up, down]
+    edges = np.array(edges, dtype=np.float32)
+    lognormal = np.exp(rng.normal(-1.5, 1.5, 6000)).astype(np.float32)
+    values = np.concatenate([special, edges, lognormal])
+    row = 23 * 3
+    pad = (-len(values)) % row
+    values = np.concatenate([values, rng.random(pad, dtype=np.float32)])
+    rgb = values.reshape(-1, 23, 3)
+    save("image_out_kat.npz", rgb=rgb, bytes=oracle.to_bytes(rgb), bytes_flipped=oracle.to_bytes(rgb, flip=True))
+
+
 def main():
     if len(sys.argv) > 1:  # only the named fixtures, e.g. `make_golden.py light_kat`
         for name in sys.argv[1:]:
@@ -285,6 +311,7 @@ def main():
     photon_kat(rng)
     image_kat()
     light_kat()
+    image_out_kat()
 
 
 if __name__ == "__main__":
