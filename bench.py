@@ -716,11 +716,14 @@ def measure_batch(gpu, oracle, args, steps, warmup):
         for j in jobs:
             ctx.render_batch_dev([j], DEPTH, RR, out.data_ptr())
 
-    arms = {"batched": batched, "per_job_plain": per_job_plain, "per_job_wavefront": per_job_wavefront}
+    arms = {"batched": batched, "per_job_plain": per_job_plain, "per_job_wavefront": per_job_wavefront,
+            "persistent_queue": batched}
     results, images = {}, {}
     for name, fn in arms.items():
         if name == "per_job_wavefront":
             ctx.set_option("batch_graph", 0)
+        # one persistent megakernel launch pulling (job, 32-pixel tile) items from a device queue
+        ctx.set_option("batch_queue", 1 if name == "persistent_queue" else 0)
         for _ in range(warmup):
             fn()
         gpu.sync()
@@ -730,6 +733,7 @@ def measure_batch(gpu, oracle, args, steps, warmup):
             gpu.flush()
             secs.append(gpu.time(fn))
         ctx.set_option("batch_graph", 1)
+        ctx.set_option("batch_queue", 0)
         total = sum(secs)
         results[name] = {"jobs_per_s": len(jobs) * steps / total, "ms_per_step": 1000 * total / steps,
                          "mpaths_per_s": n_paths * steps / total / 1e6,
@@ -754,6 +758,7 @@ def measure_batch(gpu, oracle, args, steps, warmup):
                       "l2": "flushed (256 MB write) between timed steps"},
            "arms": results, "batched_over_per_job_plain": b["jobs_per_s"] / results["per_job_plain"]["jobs_per_s"],
            "batched_over_per_job_wavefront": b["jobs_per_s"] / results["per_job_wavefront"]["jobs_per_s"],
+           "batched_over_persistent_queue": b["jobs_per_s"] / results["persistent_queue"]["jobs_per_s"],
            "images_identical_across_arms": same, "nonfinite_floats": nonfinite, **tuned,
            "e2e": {"value": e2e, "unit": "jobs/s", "h2d_bytes_per_step": 80 * len(jobs),
                    "d2h_bytes_per_step": 4 * floats, "path": "lrt_render_batch (host output buffer)"},

@@ -501,7 +501,12 @@ int lrt_render_stats_reset(lrt_context* ctx);
 /* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26;
  * 0, the default: 2^24 for forward renders, 2^21 for adjoint renders; a wave never holds more paths than
  * its call renders),
- * "photon_tree_device" (0/1), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
+ * "batch_queue" (0, the default: batches as shared path waves; 1: one persistent megakernel that pulls
+ * (job, 32-pixel tile) items from a device queue, costliest jobs first -- identical images),
+ * "photon_tree_device" (1, the default: photon maps' kd-trees built on the GPU; 0: on the host cores with
+ * std::nth_element; the trees are identical), "photon_tree_depth_limit" (-1, the default: the partition
+ * budget std::nth_element gives a node, 2*floor(log2(n)); k >= 0: k partitions, then the heap selection
+ * -- a test setting for that path), "batch_graph" (1: one CUDA graph per wave sequence, 0: direct launches),
  * "adjoint_megakernel" (1: the one-thread-per-path adjoint instead of the wavefront one),
  * "blocks_per_sm" (cap on resident blocks per SM of every grid, 0: occupancy's maximum),
  * "pixel_tile" (batch path order: bands of this many rows walked column by column; 1: row-major),
@@ -523,6 +528,12 @@ int lrt_photon_trace_particles(lrt_context* ctx, int32_t kind, uint32_t first, u
                                lrt_photon* photons_out, uint32_t* counts_out);
 int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photons, uint32_t n,
                          float scale);
+/* The built map's tree (photon_map.h:74-81): order[i] = the index (in the array given to the build) of
+ * the photon at tree position i; nodes: 4 words per node in depth-first order -- interior {left,
+ * right, axis, split as float bits}, leaf {first photon, count, 3, 0}. n_nodes gets the node count
+ * (max_nodes too small: LRT_ERR_RANGE). */
+int lrt_photon_map_tree(lrt_context* ctx, int32_t map, uint32_t* order, int32_t* nodes, uint64_t max_nodes,
+                        uint32_t* n_nodes);
 /* k nearest photons within squared radius r2 (photon_map.h:117-165). Indices refer to the array
  * given to lrt_photon_map_build; each query's results are sorted by (d2, index) descending as the
  * reference pops its max-heap. */

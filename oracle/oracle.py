@@ -61,6 +61,10 @@ def _load(path):
         lib.ref_photon_map_create.restype = vp
         lib.ref_photon_map_create.argtypes = [P(abi.Photon), u32, f32]
         lib.ref_photon_map_destroy.argtypes = [vp]
+        lib.ref_photon_map_tree.restype = i32
+        lib.ref_photon_map_tree.argtypes = [vp, P(u32), P(i32), C.c_uint64, P(u32)]
+        lib.ref_photon_tree_limited.restype = i32
+        lib.ref_photon_tree_limited.argtypes = [P(f32), u32, C.c_int, P(u32), P(i32), C.c_uint64, P(u32)]
         lib.ref_photon_map_knn.argtypes = [vp, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
         lib.ref_photon_map_irradiance.argtypes = [vp, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
         lib.ref_rough_transmittance.restype = i32
@@ -233,6 +237,17 @@ class RefPhotonMap:
         self.photons = np.ascontiguousarray(photons, dtype=abi.PHOTON_DTYPE)
         self.handle = ref_lib().ref_photon_map_create(_p(self.photons, abi.Photon), len(self.photons), scale)
 
+    def tree(self):
+        """(order, nodes) of the reference's build in lrt_photon_map_tree's layout"""
+        n = len(self.photons)
+        order = np.zeros(max(1, n), dtype=np.uint32)
+        cap = max(1, n // 2 + 16)
+        nodes = np.zeros((cap, 4), dtype=np.int32)
+        nn = C.c_uint32(0)
+        assert ref_lib().ref_photon_map_tree(self.handle, _p(order, C.c_uint32), _p(nodes, C.c_int32), cap,
+                                             C.byref(nn)) == 0
+        return order[:n], nodes[: nn.value]
+
     def knn(self, points, r2, k):
         points = np.ascontiguousarray(points, dtype=np.float32)
         n = len(points)
@@ -316,6 +331,20 @@ def hosek_state(sun_direction, turbidity, albedo):
     rad = np.zeros(3, dtype=np.float64)
     ref_lib().ref_hosek_state(_p(sd), turbidity, albedo, _p(cfg, C.c_double), _p(rad, C.c_double))
     return cfg.reshape(3, 9), rad
+
+
+def photon_tree_limited(positions, limit):
+    """photon_map::build_range over positions with libstdc++'s introselect given `limit` partitions per
+    node (-1: std::nth_element's own budget); (order, nodes) in lrt_photon_map_tree's layout"""
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    n = len(pos)
+    order = np.zeros(max(1, n), dtype=np.uint32)
+    cap = max(1, n // 2 + 16)
+    nodes = np.zeros((cap, 4), dtype=np.int32)
+    nn = C.c_uint32(0)
+    assert ref_lib().ref_photon_tree_limited(_p(pos), n, limit, _p(order, C.c_uint32), _p(nodes, C.c_int32), cap,
+                                             C.byref(nn)) == 0
+    return order[:n], nodes[: nn.value]
 
 
 def to_bytes(rgb, flip=False):

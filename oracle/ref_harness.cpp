@@ -586,6 +586,81 @@ void* ref_photon_map_create(const lrt_photon* photons, uint32_t n, float scale) 
 
 void ref_photon_map_destroy(void* handle) { delete static_cast<ref_photon_map*>(handle); }
 
+// the built tree (photon_map.h:74-81, 83-114): order[i] = caller index of the photon at position i;
+// nodes as 4 words, interior {left, right, axis, split bits}, leaf {start, count, 3, 0}
+int ref_photon_map_tree(void* handle, uint32_t* order, int32_t* nodes, uint64_t max_nodes, uint32_t* n_nodes) {
+    const auto* pm = static_cast<ref_photon_map*>(handle);
+    *n_nodes = static_cast<uint32_t>(pm->map.nodes.size());
+    if(pm->map.nodes.size() > max_nodes) return -1;
+    std::copy(pm->original.begin(), pm->original.end(), order);
+    for(size_t i = 0; i < pm->map.nodes.size(); ++i) {
+        const auto& nd = pm->map.nodes[i];
+        int32_t* o = nodes + 4 * i;
+        if(nd.leaf) {
+            o[0] = nd.start;
+            o[1] = nd.count;
+            o[2] = 3;
+            o[3] = 0;
+        } else {
+            o[0] = nd.left;
+            o[1] = nd.right;
+            o[2] = nd.axis;
+            std::memcpy(&o[3], &nd.split, 4);
+        }
+    }
+    return 0;
+}
+
+// photon_map::build_range's recursion (photon_map.h:83-114) over bare positions with libstdc++'s
+// introselect given an explicit partition budget per node (std::nth_element's is 2*floor(log2(n))), so
+// that a small budget drives its heap-selection path. Test infrastructure for the device build.
+namespace {
+struct limited_item {
+    float p[3];
+    uint32_t index;
+};
+int limited_build(std::vector<limited_item>& v, int start, int count, int limit, std::vector<std::array<int32_t, 4>>& out) {
+    const int index = static_cast<int>(out.size());
+    out.push_back({start, count, 3, 0});
+    if(count <= 8) return index;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for(int i = 0; i < count; ++i) {
+        for(int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], v[start + i].p[a]);
+            hi[a] = std::max(hi[a], v[start + i].p[a]);
+        }
+    }
+    const float ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    int axis = 0;
+    if(ext[1] > ext[axis]) axis = 1;
+    if(ext[2] > ext[axis]) axis = 2;
+    const int mid = start + count / 2;
+    auto cmp = [axis](const limited_item& a, const limited_item& b) { return a.p[axis] < b.p[axis]; };
+    const int budget = limit >= 0 ? limit : 2 * std::__lg(count);
+    std::__introselect(v.begin() + start, v.begin() + mid, v.begin() + start + count, budget,
+                       __gnu_cxx::__ops::__iter_comp_iter(cmp));
+    const int left = limited_build(v, start, mid - start, limit, out);
+    const int right = limited_build(v, mid, start + count - mid, limit, out);
+    int32_t split_bits;
+    std::memcpy(&split_bits, &v[mid].p[axis], 4);
+    out[index] = {left, right, axis, split_bits};
+    return index;
+}
+}  // namespace
+
+int ref_photon_tree_limited(const float* positions, uint32_t n, int limit, uint32_t* order, int32_t* nodes,
+                            uint64_t max_nodes, uint32_t* n_nodes) {
+    std::vector<limited_item> v(n);
+    for(uint32_t i = 0; i < n; ++i) v[i] = limited_item{{positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]}, i};
+    std::vector<std::array<int32_t, 4>> out;
+    if(n > 0) limited_build(v, 0, static_cast<int>(n), limit, out);
+    *n_nodes = static_cast<uint32_t>(out.size());
+    if(out.size() > max_nodes) return -1;
+    for(uint32_t i = 0; i < n; ++i) order[i] = v[i].index;
+    for(size_t i = 0; i < out.size(); ++i) std::memcpy(nodes + 4 * i, out[i].data(), 16);
+    return 0;
+}
+
 // photon_map::nearest (photon_map.h:117-130): results in max-heap pop order (descending (d2, index)).
 void ref_photon_map_knn(void* handle, const float* points, uint32_t n, float r2, uint32_t k, uint32_t* idx,
                         float* d2, uint32_t* count) {

@@ -1134,6 +1134,7 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
     unsigned long long total = 0, out_floats = 0;
     const int jst = job_records(ctx, jobs, n_jobs, recs, total, out_floats);
     if(jst != LRT_OK) return jst;
+    if(ctx->batch_queue) return render_batch_queue(ctx, recs, total, max_depth, rr_depth, rgb_dev);
     WaveArgs a;
     const int st = batch_wave_args(ctx, recs, total, max_depth, rr_depth, false, a);
     if(st != LRT_OK) return st;
@@ -1755,6 +1756,10 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->pixel_tile = static_cast<uint32_t>(value);
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
+    } else if(strcmp(name, "batch_queue") == 0) {
+        ctx->batch_queue = value != 0;
+    } else if(strcmp(name, "photon_tree_depth_limit") == 0) {
+        ctx->photon_tree_depth_limit = value < 0 ? -1 : static_cast<int>(std::min<int64_t>(value, 64));
     } else if(strcmp(name, "wave_capacity") == 0) {
         if(value != 0 && (value < 1024 || value > (1ll << 26))) {
             return fail(ctx, LRT_ERR_RANGE, "wave_capacity must be 0 (the defaults) or in [1024, 2^26]");

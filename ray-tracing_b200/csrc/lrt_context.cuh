@@ -126,7 +126,9 @@ struct lrt_context {
     std::vector<cudaEvent_t> events;
     std::vector<int> event_stage;
     // photons
-    bool photon_tree_device = false;  // false: reference-identical tree built on the host
+    bool batch_queue = false;  // true: a batch as one persistent megakernel over (job, tile) items
+    bool photon_tree_device = true;  // the reference's photon tree built on the GPU (false: on the host cores)
+    int photon_tree_depth_limit = -1;  // introselect's partition budget per node (-1: 2*floor(log2(n)), as std::nth_element)
     bool shade_per_key = true;  // one shading kernel per material type present (false: one for all)
     uint32_t shade_keys = 3u;    // bit k: shading key k can occur in the uploaded scene
     bool has_mesh_lights = false;  // a mesh is an area light: the one all-keys shading kernel runs
@@ -161,6 +163,16 @@ inline int fail(lrt_context* ctx, int code, const char* fmt, ...) {
                                "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);          \
         }                                                                                                     \
     } while(0)
+
+// A batch's jobs as one persistent megakernel launch pulling (job, tile) items from a device queue
+// (lrt_plain.cu, option batch_queue); images identical to the per-job plain launches.
+int render_batch_queue(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned long long total, int32_t max_depth,
+                       int32_t rr_depth, float* rgb_dev);
+
+// The photon map's kd-tree of photons_dev built on the GPU, identical to photon_map::build's
+// (lrt_photon_tree.cu); fills pm's search arrays and nodes.
+int photon_tree_build_device(lrt_context* ctx, PhotonMap& pm, const lrt_photon* photons_dev, uint32_t n,
+                             int depth_limit);
 
 // Validates a batch's jobs and lays out their path ranges (pixel-major, samples inner) and outputs;
 // total = the batch's paths, out_floats = the output floats the jobs reach.

@@ -303,97 +303,6 @@ __global__ void k_photon_gather_attrs(const lrt_photon* in, const uint32_t* orde
 }
 
 // ---------------------------------------------------------------------------------------------
-// photon map build on the device (option photon_tree_device): same topology, every node range sorted
-// on its axis, split = the median value. A valid partition, so the search finds the exact k nearest
-// photons within the radius; the reference's tree can miss some of them (see above).
-
-struct HostNode {
-    int32_t start, count, left, right, depth;
-};
-
-int build_topology(int32_t start, int32_t count, int32_t depth, std::vector<HostNode>& nodes) {
-    const int32_t index = static_cast<int32_t>(nodes.size());
-    nodes.push_back(HostNode{start, count, -1, -1, depth});
-    if(count <= 8) return index;
-    const int32_t mid = start + count / 2;
-    const int32_t left = build_topology(start, mid - start, depth + 1, nodes);
-    const int32_t right = build_topology(mid, start + count - mid, depth + 1, nodes);
-    nodes[index].left = left;
-    nodes[index].right = right;
-    return index;
-}
-
-__global__ void k_photon_positions(const lrt_photon* in, uint32_t n, float4* pos) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= n) return;
-    pos[i] = make_float4(in[i].position[0], in[i].position[1], in[i].position[2], __uint_as_float(i));
-}
-
-// one block per node: bounds of its photons -> largest-extent axis (photon_map.h:94-100); then the sort keys
-__global__ void __launch_bounds__(256) k_node_axis(const float4* pos, const int2* segs, const int32_t* seg_node,
-                                                   PhotonNode* nodes, float* keys, uint32_t* vals) {
-    __shared__ float lo[3][256];
-    __shared__ float hi[3][256];
-    __shared__ int axis_s;
-    const int2 seg = segs[blockIdx.x];
-    float l0 = kInf, l1 = kInf, l2 = kInf, h0 = -kInf, h1 = -kInf, h2 = -kInf;
-    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) {
-        const float4 p = pos[i];
-        l0 = smin(l0, p.x); l1 = smin(l1, p.y); l2 = smin(l2, p.z);
-        h0 = smax(h0, p.x); h1 = smax(h1, p.y); h2 = smax(h2, p.z);
-    }
-    lo[0][threadIdx.x] = l0; lo[1][threadIdx.x] = l1; lo[2][threadIdx.x] = l2;
-    hi[0][threadIdx.x] = h0; hi[1][threadIdx.x] = h1; hi[2][threadIdx.x] = h2;
-    __syncthreads();
-    for(int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
-        if(threadIdx.x < stride) {
-            for(int a = 0; a < 3; ++a) {
-                lo[a][threadIdx.x] = smin(lo[a][threadIdx.x], lo[a][threadIdx.x + stride]);
-                hi[a][threadIdx.x] = smax(hi[a][threadIdx.x], hi[a][threadIdx.x + stride]);
-            }
-        }
-        __syncthreads();
-    }
-    if(threadIdx.x == 0) {
-        const f3 extent = f3{hi[0][0], hi[1][0], hi[2][0]} - f3{lo[0][0], lo[1][0], lo[2][0]};
-        int axis = 0;
-        if(extent.y > comp(extent, axis)) axis = 1;
-        if(extent.z > comp(extent, axis)) axis = 2;
-        axis_s = axis;
-        nodes[seg_node[blockIdx.x]].axis = axis;
-    }
-    __syncthreads();
-    const int axis = axis_s;
-    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) {
-        const float4 p = pos[i];
-        keys[i] = axis == 0 ? p.x : (axis == 1 ? p.y : p.z);
-        vals[i] = static_cast<uint32_t>(i);
-    }
-}
-
-// reorder each node range by the sorted permutation and read the split at the median (photon_map.h:102-110)
-__global__ void __launch_bounds__(256) k_node_permute(const float4* pos, float4* out, const int2* segs,
-                                                      const int32_t* seg_node, const uint32_t* perm, PhotonNode* nodes) {
-    const int2 seg = segs[blockIdx.x];
-    for(int i = seg.x + threadIdx.x; i < seg.y; i += blockDim.x) out[i] = pos[perm[i]];
-    if(threadIdx.x == 0) {
-        PhotonNode& nd = nodes[seg_node[blockIdx.x]];
-        const int mid = seg.x + (seg.y - seg.x) / 2;
-        const float4 p = pos[perm[mid]];
-        nd.split = nd.axis == 0 ? p.x : (nd.axis == 1 ? p.y : p.z);
-    }
-}
-
-__global__ void k_photon_attrs(const lrt_photon* in, const float4* pos, uint32_t n, float4* dir, float4* nrm, float4* pw) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= n) return;
-    const lrt_photon& p = in[__float_as_uint(pos[i].w)];
-    dir[i] = make_float4(p.direction[0], p.direction[1], p.direction[2], __int_as_float(static_cast<int>(p.depth)));
-    nrm[i] = make_float4(p.normal[0], p.normal[1], p.normal[2], 0.0f);
-    pw[i] = make_float4(p.power[0], p.power[1], p.power[2], 0.0f);
-}
-
-// ---------------------------------------------------------------------------------------------
 // k-NN gather
 
 struct MapView {
@@ -565,7 +474,7 @@ __global__ void __launch_bounds__(kBlock) k_irradiance(MapView m, const float* p
 // (the reference multiplies the child's returned radiance instead: same terms, other rounding).
 
 constexpr int kEyeFrames = 128;  // one frame per recursion level: max_depth <= 128
-enum EyeStage : uint8_t { kEyeStart = 0, kEyeSpecular = 1, kEyeEmitters = 2, kEyeBsdf = 3 };
+enum EyeStage : uint8_t { kEyeStart = 0, kEyeSpecular = 1, kEyeEmitters = 2, kEyeBsdf = 3, kEyeLookup = 4 };
 
 struct EyeFrame {
     f3 ro, rd;       // the ray li was called with
@@ -815,7 +724,7 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye(DeviceScene s, EyeParams 
 // (trav_step, the persistent traversal of the path tracer), and a lane whose ray is done resumes its
 // walk with the result; a lane whose camera sample is done takes the next one. Samples, sampler
 // draws, rays and additions to L are those of eye_sample, in the same order.
-enum EyeQueryKind : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, kQueryBsdf = 3 };
+enum EyeQueryKind : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, kQueryBsdf = 3, kQueryIrradiance = 4 };
 
 // A ray query of the wavefront eye pass, in device memory with its result. A lane's walk issues the
 // shadow rays of a frame's emitter samples, and the rays of its BSDF samples when they do not recurse,
@@ -824,10 +733,14 @@ enum EyeQueryKind : uint8_t { kQueryNone = 0, kQueryHit = 1, kQueryShadow = 2, k
 // are those of one query at a time. A frame's own ray and a BSDF sample that recurses go alone.
 constexpr uint32_t kEyeBatch = 16;
 
+// A photon lookup (kQueryIrradiance) uses the record as: o = (point, radius), d = (normal, -), a =
+// (diffuse reflectance / pi, -), b = (frame weight, -), light = map (0 global, 1 caustic), any_mode =
+// photon depth limit; the estimate comes back in (closest, u, v).
 struct EyeQuery {
     float4 o;          // origin, t_min
     float4 d;          // direction, t_max
     float4 a;          // shadow: what L gains when the light is visible; BSDF sample: weight (xyz), pdf (w)
+    float4 b;          // photon lookup: the frame's weight
     int32_t kind;      // EyeQueryKind
     int32_t light;     // shadow: the light
     int32_t any_mode;
@@ -920,6 +833,10 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
             }
             const uint32_t flags = s.materials[m].flags;
             const bool diffuse = (flags & (kDiffuse | kGlossy | kSpecular)) == kDiffuse;
+            if(diffuse && dot(F.n, F.rd) < 0.0f && batch.q) {  // the lookups go into the batch
+                F.stage = kEyeLookup;
+                continue;
+            }
             if(diffuse && dot(F.n, F.rd) < 0.0f) {  // photon lookups (photon_integrator.h:95-106)
                 const int photon_depth = ep.max_depth - F.depth;
                 const f3 reflectance = bsdf_diffuse_reflectance(s.materials, m) * (1.0f / kPi);
@@ -934,6 +851,28 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
             }
             F.stage = kEyeSpecular;
             F.iter = 0;
+            continue;
+        }
+        if(F.stage == kEyeLookup) {  // the photon lookups as queries of the batch, global map first
+            const int need = (ep.global.n > 0 ? 1 : 0) + (ep.caustic.n > 0 ? 1 : 0);
+            if(batch.n + need > kEyeBatch) return true;  // the batch is not empty: resume here
+            const int32_t m = s.objects[F.obj].material;
+            const int photon_depth = ep.max_depth - F.depth;
+            const f3 reflectance = bsdf_diffuse_reflectance(s.materials, m) * (1.0f / kPi);
+            for(int map = 0; map < 2; ++map) {
+                if((map == 0 ? ep.global.n : ep.caustic.n) == 0) continue;
+                EyeQuery& Q = batch.q[batch.n++];
+                Q.o = make_float4(F.p.x, F.p.y, F.p.z, map == 0 ? ep.global_radius : ep.caustic_radius);
+                Q.d = make_float4(F.n.x, F.n.y, F.n.z, 0.0f);
+                Q.a = make_float4(reflectance.x, reflectance.y, reflectance.z, 0.0f);
+                Q.b = make_float4(F.tp.x, F.tp.y, F.tp.z, 0.0f);
+                Q.kind = kQueryIrradiance;
+                Q.light = map;
+                Q.any_mode = photon_depth;
+            }
+            F.stage = kEyeSpecular;
+            F.iter = 0;
+            if(batch.n == kEyeBatch) return true;  // full: the walk resumes at the specular lobes
             continue;
         }
         const int32_t mid = s.objects[F.obj].material;
@@ -1179,7 +1118,8 @@ struct EyeWave {
     EyeFrame* frames;      // frame_limit frames per slot
     EyeQuery* queries;     // kEyeBatch per slot
     uint32_t* queue;       // queries to trace (slot * kEyeBatch + index)
-    uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch
+    uint32_t* lookups;     // photon lookups (slot * kEyeBatch + index)
+    uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch, [3] lookups
     float4* L_out;
     int* overflow;
     uint32_t n_slots;
@@ -1200,6 +1140,10 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
         if(S.state == kSlotTracing) {  // the batch's results, in issue order
             for(uint32_t q = 0; q < S.nq; ++q) {
                 const EyeQuery& Q = queries[q];
+                if(Q.kind == kQueryIrradiance) {  // L += tp * (estimate * reflectance), as the walk would
+                    ln.L += f3{Q.b.x, Q.b.y, Q.b.z} * (f3{Q.closest, Q.u, Q.v} * f3{Q.a.x, Q.a.y, Q.a.z});
+                    continue;
+                }
                 ln.query = static_cast<uint8_t>(Q.kind);
                 ln.qa = f3{Q.a.x, Q.a.y, Q.a.z};
                 ln.qpdf = Q.a.w;
@@ -1238,8 +1182,17 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
             if(eye_advance(s, ep, ln, st, heap, w.overflow, ts, w.frame_limit, batch)) {
                 state = kSlotTracing;
                 nq = batch.n;
-                const uint32_t base = atomicAdd(&w.counters[0], nq);
-                for(uint32_t q = 0; q < nq; ++q) w.queue[base + q] = slot * kEyeBatch + q;
+                uint32_t n_lookups = 0;
+                for(uint32_t q = 0; q < nq; ++q) n_lookups += queries[q].kind == kQueryIrradiance ? 1u : 0u;
+                const uint32_t tbase = nq > n_lookups ? atomicAdd(&w.counters[0], nq - n_lookups) : 0u;
+                const uint32_t kbase = n_lookups > 0 ? atomicAdd(&w.counters[3], n_lookups) : 0u;
+                for(uint32_t q = 0, t = 0, k = 0; q < nq; ++q) {
+                    if(queries[q].kind == kQueryIrradiance) {
+                        w.lookups[kbase + k++] = slot * kEyeBatch + q;
+                    } else {
+                        w.queue[tbase + t++] = slot * kEyeBatch + q;
+                    }
+                }
                 break;
             }
             w.L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
@@ -1281,6 +1234,21 @@ __global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) 
             Q.ref = st.best_mesh.ref;
             active = false;
         }
+    }
+}
+
+// the queued photon lookups, one per thread (photon_map::estimate_irradiance); the estimate is written
+// beside each query
+__global__ void __launch_bounds__(kBlock) k_eye_lookup(EyeParams ep, EyeWave w) {
+    const uint32_t n = w.counters[3];
+    KnnHeap heap;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        EyeQuery& Q = w.queries[w.lookups[i]];
+        const f3 E = estimate_irradiance(Q.light == 0 ? ep.global : ep.caustic, f3{Q.o.x, Q.o.y, Q.o.z},
+                                         f3{Q.d.x, Q.d.y, Q.d.z}, Q.o.w, Q.any_mode, ep.lookup_size, heap);
+        Q.closest = E.x;
+        Q.u = E.y;
+        Q.v = E.z;
     }
 }
 
@@ -1335,8 +1303,13 @@ int lrt_photon_trace_particles(lrt_context* ctx, int32_t kind, uint32_t first, u
     return LRT_OK;
 }
 
-int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t max_depth, int32_t rr_depth,
-                     lrt_photon* photons_out, uint32_t* n_out, uint64_t* shot_out) {
+}  // extern "C"
+
+namespace {
+
+// photon_gather::run; photons_out == nullptr leaves the photons in ctx->ph_out (device)
+int photon_trace_impl(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t max_depth, int32_t rr_depth,
+                      lrt_photon* photons_out, uint32_t* n_out, uint64_t* shot_out) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
     if(!n_out || !shot_out || (kind != LRT_GATHER_SURFACE && kind != LRT_GATHER_CAUSTIC)) {
@@ -1345,7 +1318,6 @@ int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t
     *n_out = 0;
     *shot_out = 0;
     if(requested == 0 || max_depth < 1) return LRT_OK;  // photon_gather.h:20-22
-    if(!photons_out) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photon buffer");
     // work items of `granularity` particles as with one worker (photon_gather.h:26-28)
     const uint64_t granularity = std::max<uint64_t>(1, requested / 16);
     const uint64_t batches_per_launch = std::max<uint64_t>(1, (1ull << 21) / granularity);
@@ -1423,7 +1395,7 @@ int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t
         }
         next += chunk;
     }
-    if(stored > 0) {
+    if(stored > 0 && photons_out) {
         LRT_CUDA(ctx, cudaMemcpyAsync(photons_out, ctx->ph_out.ptr, sizeof(lrt_photon) * stored, cudaMemcpyDeviceToHost,
                                       ctx->stream));
         LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1433,10 +1405,12 @@ int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t
     return LRT_OK;
 }
 
-int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photons, uint32_t n, float scale) {
+// photon_map::build (photon_map.h:26-33) of photons given on the host or (photons_dev) on the device
+int photon_map_build_impl(lrt_context* ctx, int32_t map, const lrt_photon* photons, const lrt_photon* photons_dev,
+                          uint32_t n, float scale) {
     if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
     if(map < 0 || map >= kMaxPhotonMaps) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "photon map id out of range");
-    if(n > 0 && !photons) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photons");
+    if(n > 0 && !photons && !photons_dev) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photons");
     if(n >= (1u << 30)) return fail(ctx, LRT_ERR_RANGE, "too many photons");
     LRT_CUDA(ctx, cudaSetDevice(ctx->device));
     PhotonMap& pm = ctx->maps[map];
@@ -1445,7 +1419,15 @@ int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photon
     pm.n_nodes = 0;
     if(n == 0) return LRT_OK;
     cudaStream_t s = ctx->stream;
-    if(!ctx->photon_tree_device) {
+    std::vector<lrt_photon> host_copy;
+    if(!ctx->photon_tree_device && !photons) {
+        host_copy.resize(n);
+        LRT_CUDA(ctx, cudaMemcpyAsync(host_copy.data(), photons_dev, sizeof(lrt_photon) * static_cast<size_t>(n),
+                                      cudaMemcpyDeviceToHost, s));
+        LRT_CUDA(ctx, cudaStreamSynchronize(s));
+        photons = host_copy.data();
+    }
+    if(!ctx->photon_tree_device) {  // the same tree built on the host cores with std::nth_element itself
         std::vector<HostPhoton> ph(n);
         for(uint32_t i = 0; i < n; ++i) {
             ph[i] = HostPhoton{{photons[i].position[0], photons[i].position[1], photons[i].position[2]}, i};
@@ -1480,90 +1462,51 @@ int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photon
         pm.depth = max_depth;
         return LRT_OK;
     }
-    // topology (depends only on n) in the reference's depth-first node order
-    std::vector<HostNode> topo;
-    topo.reserve(n / 4 + 16);
-    build_topology(0, static_cast<int32_t>(n), 0, topo);
-    std::vector<PhotonNode> nodes(topo.size());
-    int32_t max_level = 0;
-    for(size_t i = 0; i < topo.size(); ++i) {
-        const HostNode& h = topo[i];
-        if(h.left < 0) {
-            nodes[i] = PhotonNode{h.start, h.count, 3, 0.0f};
-        } else {
-            nodes[i] = PhotonNode{h.left, h.right, 0, 0.0f};
-            max_level = std::max(max_level, h.depth);
-        }
+    if(!photons_dev) {
+        LRT_CUDA(ctx, ctx->ph_tmp.ensure(sizeof(lrt_photon) * static_cast<size_t>(n)));
+        LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_tmp.ptr, photons, sizeof(lrt_photon) * static_cast<size_t>(n),
+                                      cudaMemcpyHostToDevice, s));
+        photons_dev = ctx->ph_tmp.as<lrt_photon>();
     }
-    pm.depth = static_cast<uint32_t>(max_level + 1);
-    LRT_CUDA(ctx, pm.pos.ensure(16ull * n));
-    LRT_CUDA(ctx, pm.dir.ensure(16ull * n));
-    LRT_CUDA(ctx, pm.nrm.ensure(16ull * n));
-    LRT_CUDA(ctx, pm.pow.ensure(16ull * n));
-    LRT_CUDA(ctx, pm.nodes.ensure(sizeof(PhotonNode) * nodes.size()));
-    LRT_CUDA(ctx, ctx->ph_tmp.ensure(sizeof(lrt_photon) * static_cast<size_t>(n)));
-    LRT_CUDA(ctx, ctx->ph_keys.ensure(8ull * n));
-    LRT_CUDA(ctx, ctx->ph_vals.ensure(8ull * n));
-    LRT_CUDA(ctx, ctx->scratch_b.ensure(16ull * n));
-    LRT_CUDA(ctx, cudaMemcpyAsync(ctx->ph_tmp.ptr, photons, sizeof(lrt_photon) * static_cast<size_t>(n),
-                                  cudaMemcpyHostToDevice, s));
-    LRT_CUDA(ctx, cudaMemcpyAsync(pm.nodes.ptr, nodes.data(), sizeof(PhotonNode) * nodes.size(), cudaMemcpyHostToDevice, s));
-    k_photon_positions<<<blocks_for(n), kBlock, 0, s>>>(ctx->ph_tmp.as<lrt_photon>(), n, pm.pos.as<float4>());
-    LRT_CUDA(ctx, cudaGetLastError());
-    // per level: the interior nodes as sort segments
-    std::vector<std::vector<int32_t>> levels(max_level + 1);
-    for(size_t i = 0; i < topo.size(); ++i) {
-        if(topo[i].left >= 0) levels[topo[i].depth].push_back(static_cast<int32_t>(i));
+    return photon_tree_build_device(ctx, pm, photons_dev, n, ctx->photon_tree_depth_limit);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_photon_trace(lrt_context* ctx, int32_t kind, uint32_t requested, int32_t max_depth, int32_t rr_depth,
+                     lrt_photon* photons_out, uint32_t* n_out, uint64_t* shot_out) {
+    if(ctx && requested > 0 && max_depth >= 1 && !photons_out) {
+        return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photon buffer");
     }
-    float* keys_in = ctx->ph_keys.as<float>();
-    float* keys_out = keys_in + n;
-    uint32_t* vals_in = ctx->ph_vals.as<uint32_t>();
-    uint32_t* vals_out = vals_in + n;
-    float4* pos = pm.pos.as<float4>();
-    float4* pos_tmp = ctx->scratch_b.as<float4>();
-    for(int32_t level = 0; level <= max_level; ++level) {
-        const std::vector<int32_t>& ids = levels[level];
-        if(ids.empty()) continue;
-        const int32_t nseg = static_cast<int32_t>(ids.size());
-        std::vector<int2> segs(nseg);
-        std::vector<int32_t> begin(nseg), end(nseg);
-        for(int32_t j = 0; j < nseg; ++j) {
-            const HostNode& h = topo[ids[j]];
-            segs[j] = make_int2(h.start, h.start + h.count);
-            begin[j] = h.start;
-            end[j] = h.start + h.count;
-        }
-        const size_t seg_bytes = sizeof(int2) * nseg + 3 * sizeof(int32_t) * nseg;
-        LRT_CUDA(ctx, ctx->ph_seg.ensure(seg_bytes));
-        char* sb = ctx->ph_seg.as<char>();
-        int2* d_segs = reinterpret_cast<int2*>(sb);
-        int32_t* d_node = reinterpret_cast<int32_t*>(sb + sizeof(int2) * nseg);
-        int32_t* d_begin = d_node + nseg;
-        int32_t* d_end = d_begin + nseg;
-        LRT_CUDA(ctx, cudaMemcpyAsync(d_segs, segs.data(), sizeof(int2) * nseg, cudaMemcpyHostToDevice, s));
-        LRT_CUDA(ctx, cudaMemcpyAsync(d_node, ids.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
-        LRT_CUDA(ctx, cudaMemcpyAsync(d_begin, begin.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
-        LRT_CUDA(ctx, cudaMemcpyAsync(d_end, end.data(), 4ull * nseg, cudaMemcpyHostToDevice, s));
-        k_node_axis<<<nseg, 256, 0, s>>>(pos, d_segs, d_node, pm.nodes.as<PhotonNode>(), keys_in, vals_in);
-        LRT_CUDA(ctx, cudaGetLastError());
-        size_t temp = 0;
-        LRT_CUDA(ctx, cub::DeviceSegmentedRadixSort::SortPairs(nullptr, temp, keys_in, keys_out, vals_in, vals_out,
-                                                               static_cast<int>(n), nseg, d_begin, d_end, 0, 32, s));
-        LRT_CUDA(ctx, ctx->ph_cub.ensure(temp));
-        LRT_CUDA(ctx, cub::DeviceSegmentedRadixSort::SortPairs(ctx->ph_cub.ptr, temp, keys_in, keys_out, vals_in,
-                                                               vals_out, static_cast<int>(n), nseg, d_begin, d_end, 0,
-                                                               32, s));
-        LRT_CUDA(ctx, cudaMemcpyAsync(pos_tmp, pos, 16ull * n, cudaMemcpyDeviceToDevice, s));
-        k_node_permute<<<nseg, 256, 0, s>>>(pos, pos_tmp, d_segs, d_node, vals_out, pm.nodes.as<PhotonNode>());
-        LRT_CUDA(ctx, cudaGetLastError());
-        LRT_CUDA(ctx, cudaMemcpyAsync(pos, pos_tmp, 16ull * n, cudaMemcpyDeviceToDevice, s));
-        LRT_CUDA(ctx, cudaStreamSynchronize(s));  // the segment arrays are rewritten next level
+    return photon_trace_impl(ctx, kind, requested, max_depth, rr_depth, photons_out, n_out, shot_out);
+}
+
+int lrt_photon_map_build(lrt_context* ctx, int32_t map, const lrt_photon* photons, uint32_t n, float scale) {
+    if(ctx && n > 0 && !photons) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "null photons");
+    return photon_map_build_impl(ctx, map, photons, nullptr, n, scale);
+}
+
+int lrt_photon_map_tree(lrt_context* ctx, int32_t map, uint32_t* order, int32_t* nodes, uint64_t max_nodes,
+                        uint32_t* n_nodes) {
+    if(!ctx) return LRT_ERR_INVALID_ARGUMENT;
+    if(map < 0 || map >= kMaxPhotonMaps || !n_nodes) return fail(ctx, LRT_ERR_INVALID_ARGUMENT, "bad photon map query");
+    const PhotonMap& pm = ctx->maps[map];
+    *n_nodes = pm.n_nodes;
+    if(pm.n == 0) return LRT_OK;
+    if(!order || !nodes || max_nodes < pm.n_nodes) return fail(ctx, LRT_ERR_RANGE, "photon map tree: output too small");
+    LRT_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::vector<float4> pos(pm.n);
+    LRT_CUDA(ctx, cudaMemcpyAsync(pos.data(), pm.pos.ptr, 16ull * pm.n, cudaMemcpyDeviceToHost, ctx->stream));
+    static_assert(sizeof(PhotonNode) == 16, "4 words per node");
+    LRT_CUDA(ctx, cudaMemcpyAsync(nodes, pm.nodes.ptr, sizeof(PhotonNode) * pm.n_nodes, cudaMemcpyDeviceToHost, ctx->stream));
+    LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for(uint32_t i = 0; i < pm.n; ++i) {
+        uint32_t bits;
+        std::memcpy(&bits, &pos[i].w, 4);
+        order[i] = bits;
     }
-    k_photon_attrs<<<blocks_for(n), kBlock, 0, s>>>(ctx->ph_tmp.as<lrt_photon>(), pos, n, pm.dir.as<float4>(),
-                                                     pm.nrm.as<float4>(), pm.pow.as<float4>());
-    LRT_CUDA(ctx, cudaGetLastError());
-    LRT_CUDA(ctx, cudaStreamSynchronize(s));
-    pm.n_nodes = static_cast<uint32_t>(nodes.size());
     return LRT_OK;
 }
 
@@ -1718,13 +1661,14 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     if(mode == 2) {
         LRT_CUDA(ctx, ctx->eye_slots.ensure(sizeof(EyeSlot) * n_slots));
         LRT_CUDA(ctx, ctx->eye_frames.ensure(sizeof(EyeFrame) * static_cast<size_t>(n_slots) * frame_limit));
-        LRT_CUDA(ctx, ctx->eye_queue.ensure(4ull * kEyeBatch * n_slots + 64));
+        LRT_CUDA(ctx, ctx->eye_queue.ensure(8ull * kEyeBatch * n_slots + 64));
         LRT_CUDA(ctx, ctx->eye_queries.ensure(sizeof(EyeQuery) * kEyeBatch * static_cast<size_t>(n_slots)));
         w.slots = ctx->eye_slots.as<EyeSlot>();
         w.frames = ctx->eye_frames.as<EyeFrame>();
         w.queries = ctx->eye_queries.as<EyeQuery>();
         w.queue = ctx->eye_queue.as<uint32_t>();
         w.counters = w.queue + static_cast<size_t>(kEyeBatch) * n_slots;
+        w.lookups = w.counters + 16;
         w.L_out = L;
         w.overflow = overflow;
         w.frame_limit = frame_limit;
@@ -1733,6 +1677,7 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     }
     const int g_shade = grid_for(ctx, (const void*)k_eye_shade, kBlock);
     const int g_trace = grid_for(ctx, (const void*)k_eye_trace, kBlock);
+    const int g_lookup = grid_for(ctx, (const void*)k_eye_lookup, kBlock);
     const uint32_t spp = p->spp;
     // the wavefront form keeps refilling its slots from one large pool of samples, so that the slow drain
     // of the longest walks happens once per pool rather than once per 2^20 samples
@@ -1768,15 +1713,16 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
                 while(true) {
                     for(int r = 0; r < kEyeRounds; ++r) {
                         LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 4, ctx->stream));
-                        LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 4, ctx->stream));
+                        LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 8, ctx->stream));
                         k_eye_shade<<<g_shade, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
                         k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
+                        k_eye_lookup<<<g_lookup, kBlock, 0, ctx->stream>>>(ep, w);
                     }
-                    ctx->stats.kernel_launches += 2 * kEyeRounds;
-                    uint32_t queued = 0;
-                    LRT_CUDA(ctx, cudaMemcpyAsync(&queued, w.counters, 4, cudaMemcpyDeviceToHost, ctx->stream));
+                    ctx->stats.kernel_launches += 3 * kEyeRounds;
+                    uint32_t queued[4] = {0, 0, 0, 0};
+                    LRT_CUDA(ctx, cudaMemcpyAsync(queued, w.counters, 16, cudaMemcpyDeviceToHost, ctx->stream));
                     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-                    if(queued == 0) break;
+                    if(queued[0] == 0 && queued[3] == 0) break;
                 }
             } else if(persistent) {
                 LRT_CUDA(ctx, cudaMemsetAsync(fetch, 0, 4, ctx->stream));
@@ -1843,14 +1789,14 @@ int lrt_photon_preprocess(lrt_context* ctx, uint32_t global_photons, uint32_t ca
     for(int m = 0; m < 2; ++m) {
         if(shots) shots[m] = 0;
         if(requested[m] == 0) continue;
-        std::vector<lrt_photon> photons(requested[m]);
         uint32_t n = 0;
         uint64_t shot = 0;
-        int st = lrt_photon_trace(ctx, kinds[m], requested[m], max_depth - 1, rr_depth, photons.data(), &n, &shot);
+        // the photons stay on the device (ctx->ph_out) for the map build
+        int st = photon_trace_impl(ctx, kinds[m], requested[m], max_depth - 1, rr_depth, nullptr, &n, &shot);
         if(st != LRT_OK) return st;
         if(shots) shots[m] = shot;
         if(n != requested[m]) continue;  // not full: the reference leaves the map empty
-        st = lrt_photon_map_build(ctx, m, photons.data(), n, 1.0f / static_cast<float>(shot));
+        st = photon_map_build_impl(ctx, m, nullptr, ctx->ph_out.as<lrt_photon>(), n, 1.0f / static_cast<float>(shot));
         if(st != LRT_OK) return st;
         if(m == 0) {
             out->global_map = 0;

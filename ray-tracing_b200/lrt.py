@@ -33,7 +33,7 @@ EXPORTS = [
     "lrt_rough_transmittance_at_alpha", "lrt_scene_update_materials", "lrt_diff_setup", "lrt_render_adjoint",
     "lrt_render_adjoint_dev",
     "lrt_render_stats_get", "lrt_render_stats_reset", "lrt_set_option", "lrt_photon_trace",
-    "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_knn", "lrt_photon_irradiance",
+    "lrt_photon_trace_particles", "lrt_photon_map_build", "lrt_photon_map_tree", "lrt_photon_knn", "lrt_photon_irradiance",
     "lrt_photon_irradiance_dev",
     "lrt_photon_preprocess", "lrt_render_photon", "lrt_render_photon_dev",
 ]
@@ -118,6 +118,7 @@ def lib():
         L.lrt_photon_trace.argtypes = [vp, i32, u32, i32, i32, P(abi.Photon), P(u32), P(u64)]
         L.lrt_photon_trace_particles.argtypes = [vp, i32, u32, u32, i32, i32, u32, P(abi.Photon), P(u32)]
         L.lrt_photon_map_build.argtypes = [vp, i32, P(abi.Photon), u32, f32]
+        L.lrt_photon_map_tree.argtypes = [vp, i32, P(u32), P(i32), u64, P(u32)]
         L.lrt_photon_knn.argtypes = [vp, i32, P(f32), u32, f32, u32, P(u32), P(f32), P(u32)]
         L.lrt_photon_irradiance.argtypes = [vp, i32, P(f32), P(f32), u32, f32, i32, u32, P(f32)]
         L.lrt_photon_irradiance_dev.argtypes = [vp, i32, vp, vp, u32, f32, i32, u32, vp]
@@ -449,6 +450,17 @@ class Context:
     def photon_map_build(self, map_id: int, photons: np.ndarray, scale: float):
         photons = np.ascontiguousarray(photons, dtype=abi.PHOTON_DTYPE)
         self._check(lib().lrt_photon_map_build(self.handle, map_id, ptr(photons, abi.Photon), len(photons), scale))
+
+    def photon_map_tree(self, map_id: int, n_photons: int):
+        """(order, nodes): the built map's photon order (indices into the build's array) and its nodes,
+        (n_nodes, 4) int32 in depth-first order (interior: left, right, axis, split bits; leaf: first, count, 3, 0)"""
+        order = np.zeros(max(1, n_photons), dtype=np.uint32)
+        cap = max(1, n_photons // 2 + 16)
+        nodes = np.zeros((cap, 4), dtype=np.int32)
+        nn = C.c_uint32(0)
+        self._check(lib().lrt_photon_map_tree(self.handle, map_id, ptr(order, C.c_uint32), ptr(nodes, C.c_int32), cap,
+                                              C.byref(nn)))
+        return order[:n_photons], nodes[: nn.value]
 
     def photon_knn(self, map_id: int, points, r2: float, k: int):
         points = np.ascontiguousarray(points, dtype=np.float32)

@@ -151,6 +151,13 @@ def test_plain_path_tracer_equals_batch(ctx, library):
     plain = ctx.render_plain(jobs, DEPTH, RR)
     batch = ctx.render_batch(jobs, DEPTH, RR)
     assert np.array_equal(plain, batch)
+    # the persistent megakernel over the (job, tile) queue: the same images
+    ctx.set_option("batch_queue", 1)
+    try:
+        queued = ctx.render_batch(jobs, DEPTH, RR)
+    finally:
+        ctx.set_option("batch_queue", 0)
+    assert np.array_equal(plain, queued)
 
 
 def test_launch_knobs_keep_images(ctx, library, tmp_path):
