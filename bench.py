@@ -1028,6 +1028,8 @@ def run_profile_case(args):
     bounce extend, hit records, shadow and one shading kernel per shading key present; about 0.5 GB.
     With the defaults, k_extend launch number 9 (0-based) is bounce 1 of the last frame.
     eye: the large photon-mapping scene, `photons` photons, one photon-mapper image of size x size x 1.
+    eye_box: the closed box with `material` on the sphere, 1M photons per map (k = 64), one photon-mapper
+    image of size x size x spp.
     adjoint: the seven-material scene at size x size x spp per material, one render and one adjoint.
     batch: 16 seeded jobs of the batched workload with spp scaled down.
     kdbuild: the SAH kd-trees of the large scene's 257 meshes built on the GPU in one call.
@@ -1036,12 +1038,23 @@ def run_profile_case(args):
     import lrt
     import lrt_abi as abi
     ctx = lrt.Context(0)
+    for opt in args.option:  # library options, e.g. --option photon_eye_tail=0
+        name, value = opt.split("=", 1)
+        ctx.set_option(name, int(value))
     if args.case == "eye":
         ctx.upload(scenes.large_scene())
         pp, shots = ctx.photon_preprocess(args.photons, 0, max_depth=8, rr_depth=5, radius_cap=0.05, lookup_size=100)
         img = ctx.render_photon(scenes.render_params(args.size, args.size, 1, 8, 3), pp)
         out = {"photons": args.photons, "shot": shots[0], "launches": ctx.stats()["kernel_launches"],
                "mean": float(img.mean())}
+    elif args.case == "eye_box":
+        ctx.upload(scenes.cornell_box(material=args.material))
+        pp, shots = ctx.photon_preprocess(PHOTONS, PHOTONS, max_depth=128, rr_depth=5, lookup_size=KNN_K)
+        ctx.reset_stats()
+        t0 = time.perf_counter()
+        img = ctx.render_photon(scenes.render_params(args.size, args.size, args.spp, DEPTH, RR), pp)
+        out = {"material": args.material, "shots": list(shots), "seconds": time.perf_counter() - t0,
+               "launches": ctx.stats()["kernel_launches"], "mean": float(img.mean())}
     elif args.case == "adjoint":
         import diff
         scene, sphere, index = scenes.open_box_library()
@@ -1129,8 +1142,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: default launch shapes")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--large-spp", type=int, default=0, help="large workload: spp (0: the configuration's 32)")
-    ap.add_argument("--case", default="render", choices=["render", "eye", "adjoint", "batch", "kdbuild", "knn"])
+    ap.add_argument("--case", default="render", choices=["render", "eye", "eye_box", "adjoint", "batch", "kdbuild", "knn"])
     ap.add_argument("--material", default="rough_plastic", choices=scenes.MATERIAL_NAMES)
+    ap.add_argument("--option", action="append", default=[], help="profile workload: a library option name=value")
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--spp", type=int, default=4)
     ap.add_argument("--frames", type=int, default=2)

@@ -126,6 +126,8 @@ struct lrt_context {
     std::vector<cudaEvent_t> events;
     std::vector<int> event_stage;
     // photons
+    uint32_t photon_eye_tail = 65536;  // queued queries below which the eye pass finishes its walks in place
+    bool knn_shared_heap = true;  // photon lookups keep their k-NN heaps in shared memory (false: local memory)
     bool batch_queue = false;  // true: a batch as one persistent megakernel over (job, tile) items
     bool photon_tree_device = true;  // the reference's photon tree built on the GPU (false: on the host cores)
     int photon_tree_depth_limit = -1;  // introselect's partition budget per node (-1: 2*floor(log2(n)), as std::nth_element)

@@ -320,41 +320,62 @@ __device__ __forceinline__ bool pair_less(float da, uint32_t ia, float db, uint3
     return da < db || (!(db < da) && ia < ib);
 }
 
+// The k nearest photons found so far: a max-heap of (d2 bits, index) pairs under pair_less. Element j of
+// a thread's heap sits at e[j * stride]: a local array (stride 1), or the thread's column of a shared
+// array interleaved across the block (stride = threads per block), where the threads of a warp at the
+// same heap position touch consecutive words and the heap stays on chip (a local heap of 1 KB per
+// thread is far beyond what L1 holds for a full SM).
 struct KnnHeap {
-    float d[kMaxKnn];
-    uint32_t i[kMaxKnn];
+    uint2* e;
+    uint32_t stride;
     uint32_t size;
+
+    __device__ __forceinline__ uint2 at(uint32_t j) const { return e[j * stride]; }
+    __device__ __forceinline__ void put(uint32_t j, uint2 v) { e[j * stride] = v; }
+    __device__ __forceinline__ float top_d() const { return __uint_as_float(e[0].x); }
+    __device__ __forceinline__ uint32_t top_i() const { return e[0].y; }
 
     __device__ __forceinline__ void pop() {  // remove the maximum
         --size;
         if(size == 0) return;
-        const float dl = d[size];
-        const uint32_t il = i[size];
+        const uint2 last = at(size);
+        const float dl = __uint_as_float(last.x);
         uint32_t k = 0;
         while(true) {
             uint32_t c = 2 * k + 1;
             if(c >= size) break;
-            if(c + 1 < size && pair_less(d[c], i[c], d[c + 1], i[c + 1])) ++c;
-            if(!pair_less(dl, il, d[c], i[c])) break;
-            d[k] = d[c];
-            i[k] = i[c];
+            uint2 cv = at(c);
+            if(c + 1 < size) {
+                const uint2 c2 = at(c + 1);
+                if(pair_less(__uint_as_float(cv.x), cv.y, __uint_as_float(c2.x), c2.y)) {
+                    ++c;
+                    cv = c2;
+                }
+            }
+            if(!pair_less(dl, last.y, __uint_as_float(cv.x), cv.y)) break;
+            put(k, cv);
             k = c;
         }
-        d[k] = dl;
-        i[k] = il;
+        put(k, last);
     }
     __device__ __forceinline__ void push(float dv, uint32_t iv) {
         uint32_t k = size++;
         while(k > 0) {
             const uint32_t parent = (k - 1) / 2;
-            if(!pair_less(d[parent], i[parent], dv, iv)) break;
-            d[k] = d[parent];
-            i[k] = i[parent];
+            const uint2 pv = at(parent);
+            if(!pair_less(__uint_as_float(pv.x), pv.y, dv, iv)) break;
+            put(k, pv);
             k = parent;
         }
-        d[k] = dv;
-        i[k] = iv;
+        put(k, make_uint2(__float_as_uint(dv), iv));
     }
+};
+
+// threads per block of the kernels that keep their heaps in shared memory: kCap heap entries of 8 bytes
+// per thread, 32 KB per block (kCap = 0: heaps in local memory, the library's usual block)
+template <uint32_t kCap>
+struct HeapBlock {
+    static constexpr int kThreads = kCap == 0 ? kBlock : static_cast<int>(4096 / kCap);
 };
 
 // per-query work of a k-NN search (algorithmic-bytes accounting); compiled out unless requested
@@ -375,7 +396,7 @@ __device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2,
         const PhotonNode nd = m.nodes[stack[--top]];
         if(kCount) ++cnt->nodes;
         float limit = r2;
-        if(heap.size == k) limit = smin(limit, heap.d[0]);
+        if(heap.size == k) limit = smin(limit, heap.top_d());
         if(nd.axis == 3) {
             for(int32_t j = 0; j < nd.b; ++j) {
                 const uint32_t pi = static_cast<uint32_t>(nd.a + j);
@@ -385,7 +406,7 @@ __device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2,
                 if(distance > limit) continue;
                 if(heap.size == k) heap.pop();
                 heap.push(distance, pi);
-                if(heap.size == k) limit = smin(r2, heap.d[0]);
+                if(heap.size == k) limit = smin(r2, heap.top_d());
             }
             continue;
         }
@@ -400,13 +421,14 @@ __device__ __forceinline__ void knn_search(const MapView& m, f3 point, float r2,
 __global__ void __launch_bounds__(kBlock) k_knn(MapView m, const float* points, uint32_t n, float r2, uint32_t k,
                                                 uint32_t* idx_out, float* d2_out, uint32_t* cnt_out) {
     for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        KnnHeap heap;
+        uint2 heap_store[kMaxKnn];
+        KnnHeap heap{heap_store, 1u, 0u};
         knn_search(m, load3(points + 3ull * q), r2, k, heap);
         const uint32_t found = heap.size;
         cnt_out[q] = found;
         for(uint32_t j = 0; j < found; ++j) {  // max-heap pop order
-            idx_out[static_cast<size_t>(q) * k + j] = __float_as_uint(m.pos[heap.i[0]].w);
-            d2_out[static_cast<size_t>(q) * k + j] = heap.d[0];
+            idx_out[static_cast<size_t>(q) * k + j] = __float_as_uint(m.pos[heap.top_i()].w);
+            d2_out[static_cast<size_t>(q) * k + j] = heap.top_d();
             heap.pop();
         }
     }
@@ -424,8 +446,8 @@ __device__ __forceinline__ f3 estimate_irradiance(const MapView& m, f3 point, f3
     if(kCount) *found += heap.size;
     const float inverse_squared_radius = 1.0f / squared_radius;
     while(heap.size > 0) {
-        const uint32_t pi = heap.i[0];
-        const float d2 = heap.d[0];
+        const uint32_t pi = heap.top_i();
+        const float d2 = heap.top_d();
         heap.pop();
         const float4 dir = m.dir[pi];
         if(__float_as_int(dir.w) > max_depth) continue;
@@ -446,14 +468,20 @@ __device__ __forceinline__ f3 estimate_irradiance(const MapView& m, f3 point, f3
 }
 
 // one query per thread; kCount adds the queries' nodes, photons tested and photons found to work[0..3]
-template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_irradiance(MapView m, const float* points, const float* normals, uint32_t n,
-                                                       float radius, int32_t max_depth, uint32_t k, float* rgb,
-                                                       unsigned long long* work) {
+// kCap > 0: heaps of kCap entries in shared memory (k <= kCap); 0: in local memory
+template <bool kCount, uint32_t kCap>
+__global__ void __launch_bounds__(HeapBlock<kCap>::kThreads) k_irradiance(MapView m, const float* points,
+                                                                         const float* normals, uint32_t n, float radius,
+                                                                         int32_t max_depth, uint32_t k, float* rgb,
+                                                                         unsigned long long* work) {
+    constexpr int kThreads = HeapBlock<kCap>::kThreads;
+    __shared__ uint2 shared_heaps[kCap == 0 ? 1 : kCap * kThreads];
+    uint2 local_heap[kCap == 0 ? kMaxKnn : 1];
     KnnCount cnt{0, 0};
     uint32_t found = 0, queries = 0;
     for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        KnnHeap heap;
+        KnnHeap heap = kCap == 0 ? KnnHeap{local_heap, 1u, 0u}
+                                 : KnnHeap{shared_heaps + threadIdx.x, static_cast<uint32_t>(kThreads), 0u};
         store3(rgb + 3ull * q, estimate_irradiance<kCount>(m, load3(points + 3ull * q), load3(normals + 3ull * q),
                                                            radius, max_depth, k, heap, &cnt, &found));
         ++queries;
@@ -702,7 +730,8 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye(DeviceScene s, EyeParams 
                                                        uint32_t pixel_begin, uint32_t n_pixels, uint32_t sample_begin,
                                                        uint32_t n_samples, float4* L_out, int* overflow) {
     EyeFrame frames[kEyeFrames];
-    KnnHeap heap;
+    uint2 heap_store[kMaxKnn];
+    KnnHeap heap{heap_store, 1u, 0u};
     const uint32_t n = n_pixels * n_samples;
     for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
         const uint32_t pix = pixel_begin + slot / n_samples;
@@ -854,11 +883,24 @@ __device__ bool eye_advance(const DeviceScene& s, const EyeParams& ep, EyeLane& 
             continue;
         }
         if(F.stage == kEyeLookup) {  // the photon lookups as queries of the batch, global map first
-            const int need = (ep.global.n > 0 ? 1 : 0) + (ep.caustic.n > 0 ? 1 : 0);
-            if(batch.n + need > kEyeBatch) return true;  // the batch is not empty: resume here
             const int32_t m = s.objects[F.obj].material;
             const int photon_depth = ep.max_depth - F.depth;
             const f3 reflectance = bsdf_diffuse_reflectance(s.materials, m) * (1.0f / kPi);
+            if(!batch.q) {  // a walk continued one query at a time (the wave's tail): the lookups inline
+                if(ep.global.n > 0) {
+                    ln.L += F.tp * (estimate_irradiance(ep.global, F.p, F.n, ep.global_radius, photon_depth, ep.lookup_size,
+                                                        heap) * reflectance);
+                }
+                if(ep.caustic.n > 0) {
+                    ln.L += F.tp * (estimate_irradiance(ep.caustic, F.p, F.n, ep.caustic_radius, photon_depth,
+                                                        ep.lookup_size, heap) * reflectance);
+                }
+                F.stage = kEyeSpecular;
+                F.iter = 0;
+                continue;
+            }
+            const int need = (ep.global.n > 0 ? 1 : 0) + (ep.caustic.n > 0 ? 1 : 0);
+            if(batch.n + need > kEyeBatch) return true;  // the batch is not empty: resume here
             for(int map = 0; map < 2; ++map) {
                 if((map == 0 ? ep.global.n : ep.caustic.n) == 0) continue;
                 EyeQuery& Q = batch.q[batch.n++];
@@ -1051,7 +1093,8 @@ __global__ void __launch_bounds__(kBlock) k_photon_eye_persistent(DeviceScene s,
                                                                   uint32_t n_samples, float4* L_out, int* overflow,
                                                                   uint32_t* fetch) {
     EyeFrame frames[kEyeFrames];
-    KnnHeap heap;
+    uint2 heap_store[kMaxKnn];
+    KnnHeap heap{heap_store, 1u, 0u};
     TravItem stack[kStackSize];
     int32_t tl_stack[kTlasStack];
     TravState ts;
@@ -1128,8 +1171,33 @@ struct EyeWave {
     uint32_t width, height, pixel_begin, n_samples, sample_begin;
 };
 
+// A slot's finished batch handed to its walk, in issue order: a photon lookup adds tp * (estimate *
+// reflectance) to L as the walk would have, a ray query goes through eye_resume.
+__device__ __forceinline__ void eye_apply_batch(const DeviceScene& s, const EyeParams& ep, EyeLane& ln, EyeFrame* st,
+                                                const EyeQuery* queries, uint32_t nq, int* overflow, int frame_limit) {
+    for(uint32_t q = 0; q < nq; ++q) {
+        const EyeQuery& Q = queries[q];
+        if(Q.kind == kQueryIrradiance) {
+            ln.L += f3{Q.b.x, Q.b.y, Q.b.z} * (f3{Q.closest, Q.u, Q.v} * f3{Q.a.x, Q.a.y, Q.a.z});
+            continue;
+        }
+        ln.query = static_cast<uint8_t>(Q.kind);
+        ln.qa = f3{Q.a.x, Q.a.y, Q.a.z};
+        ln.qpdf = Q.a.w;
+        ln.qlight = Q.light;
+        TravState ts;
+        ts.r = Ray{f3{Q.o.x, Q.o.y, Q.o.z}, f3{Q.d.x, Q.d.y, Q.d.z}};
+        ts.any_mode = Q.any_mode != 0;
+        ts.best = Q.best;
+        ts.closest_so_far = Q.closest;
+        ts.best_mesh = MeshHit{Q.closest, Q.u, Q.v, Q.ref};
+        eye_resume(s, ep, ln, st, overflow, ts, frame_limit);
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams ep, EyeWave w) {
-    KnnHeap heap;
+    uint2 heap_store[kMaxKnn];
+    KnnHeap heap{heap_store, 1u, 0u};
     for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
         EyeSlot& S = w.slots[slot];
         if(S.state == kSlotDone) continue;
@@ -1137,25 +1205,8 @@ __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams e
         EyeQuery* queries = w.queries + static_cast<size_t>(slot) * kEyeBatch;
         EyeLane ln = S.ln;
         bool have = false;
-        if(S.state == kSlotTracing) {  // the batch's results, in issue order
-            for(uint32_t q = 0; q < S.nq; ++q) {
-                const EyeQuery& Q = queries[q];
-                if(Q.kind == kQueryIrradiance) {  // L += tp * (estimate * reflectance), as the walk would
-                    ln.L += f3{Q.b.x, Q.b.y, Q.b.z} * (f3{Q.closest, Q.u, Q.v} * f3{Q.a.x, Q.a.y, Q.a.z});
-                    continue;
-                }
-                ln.query = static_cast<uint8_t>(Q.kind);
-                ln.qa = f3{Q.a.x, Q.a.y, Q.a.z};
-                ln.qpdf = Q.a.w;
-                ln.qlight = Q.light;
-                TravState ts;
-                ts.r = Ray{f3{Q.o.x, Q.o.y, Q.o.z}, f3{Q.d.x, Q.d.y, Q.d.z}};
-                ts.any_mode = Q.any_mode != 0;
-                ts.best = Q.best;
-                ts.closest_so_far = Q.closest;
-                ts.best_mesh = MeshHit{Q.closest, Q.u, Q.v, Q.ref};
-                eye_resume(s, ep, ln, st, w.overflow, ts, w.frame_limit);
-            }
+        if(S.state == kSlotTracing) {
+            eye_apply_batch(s, ep, ln, st, queries, S.nq, w.overflow, w.frame_limit);
             have = true;
         }
         uint32_t state = kSlotDone, nq = 0;
@@ -1237,11 +1288,48 @@ __global__ void __launch_bounds__(kBlock) k_eye_trace(DeviceScene s, EyeWave w) 
     }
 }
 
+// The wave's tail: once no sample is left to start and few slots still have queries, each remaining slot
+// applies its finished batch and runs the rest of its walk alone, one query at a time traced in place
+// (the persistent form's step), so that the last, deepest walks do not each cost a round of three
+// launches per query. The walk, its draws and its additions are those of the other forms.
+__global__ void __launch_bounds__(kBlock) k_eye_finish(DeviceScene s, EyeParams ep, EyeWave w) {
+    uint2 heap_store[kMaxKnn];
+    KnnHeap heap{heap_store, 1u, 0u};
+    TravItem stack[kStackSize];
+    int32_t tl_stack[kTlasStack];
+    TraceCount cnt{0, 0};
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
+        EyeSlot& S = w.slots[slot];
+        if(S.state != kSlotTracing) continue;
+        EyeFrame* st = w.frames + static_cast<size_t>(slot) * w.frame_limit;
+        EyeLane ln = S.ln;
+        eye_apply_batch(s, ep, ln, st, w.queries + static_cast<size_t>(slot) * kEyeBatch, S.nq, w.overflow,
+                        w.frame_limit);
+        while(true) {
+            TravState ts;
+            EyeBatch one{nullptr, 0};
+            if(!eye_advance(s, ep, ln, st, heap, w.overflow, ts, w.frame_limit, one)) break;
+            while(!trav_step<false>(s, ts, stack, tl_stack, cnt)) {
+            }
+            eye_resume(s, ep, ln, st, w.overflow, ts, w.frame_limit);
+        }
+        w.L_out[ln.slot] = make_float4(ln.L.x, ln.L.y, ln.L.z, 0.0f);
+        S.ln = ln;
+        S.state = kSlotDone;
+        S.nq = 0;
+    }
+}
+
 // the queued photon lookups, one per thread (photon_map::estimate_irradiance); the estimate is written
 // beside each query
-__global__ void __launch_bounds__(kBlock) k_eye_lookup(EyeParams ep, EyeWave w) {
+template <uint32_t kCap>
+__global__ void __launch_bounds__(HeapBlock<kCap>::kThreads) k_eye_lookup(EyeParams ep, EyeWave w) {
+    constexpr int kThreads = HeapBlock<kCap>::kThreads;
+    __shared__ uint2 shared_heaps[kCap == 0 ? 1 : kCap * kThreads];
+    uint2 local_heap[kCap == 0 ? kMaxKnn : 1];
+    KnnHeap heap = kCap == 0 ? KnnHeap{local_heap, 1u, 0u}
+                             : KnnHeap{shared_heaps + threadIdx.x, static_cast<uint32_t>(kThreads), 0u};
     const uint32_t n = w.counters[3];
-    KnnHeap heap;
     for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         EyeQuery& Q = w.queries[w.lookups[i]];
         const f3 E = estimate_irradiance(Q.light == 0 ? ep.global : ep.caustic, f3{Q.o.x, Q.o.y, Q.o.z},
@@ -1539,24 +1627,37 @@ int lrt_photon_knn(lrt_context* ctx, int32_t map, const float* points, uint32_t 
 namespace {
 
 // the irradiance queries on device buffers; with count_work their k-NN work goes into the stats
+// k_irradiance with the heap placement the option knn_shared_heap and k call for
+template <bool kCount>
+int irradiance_kernel(lrt_context* ctx, const MapView& view, const float* points, const float* normals, uint32_t n,
+                      float radius, int32_t max_depth, uint32_t k, float* rgb, unsigned long long* work) {
+    if(!ctx->knn_shared_heap) {
+        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 0>, HeapBlock<0>::kThreads);
+        k_irradiance<kCount, 0><<<grid, HeapBlock<0>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
+                                                                                 max_depth, k, rgb, work);
+    } else if(k <= 64) {
+        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 64>, HeapBlock<64>::kThreads);
+        k_irradiance<kCount, 64><<<grid, HeapBlock<64>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
+                                                                                   max_depth, k, rgb, work);
+    } else {
+        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 128>, HeapBlock<128>::kThreads);
+        k_irradiance<kCount, 128><<<grid, HeapBlock<128>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
+                                                                                     max_depth, k, rgb, work);
+    }
+    LRT_CUDA(ctx, cudaGetLastError());
+    ctx->stats.kernel_launches += 1;
+    return LRT_OK;
+}
+
 int irradiance_launch(lrt_context* ctx, int32_t map, const float* points, const float* normals, uint32_t n,
                       float radius, int32_t max_depth, uint32_t k, float* rgb) {
     const MapView view = view_of(ctx->maps[map]);
-    if(!ctx->count_work) {
-        const int grid = grid_for(ctx, (const void*)k_irradiance<false>, kBlock);
-        k_irradiance<false><<<grid, kBlock, 0, ctx->stream>>>(view, points, normals, n, radius, max_depth, k, rgb,
-                                                              nullptr);
-        LRT_CUDA(ctx, cudaGetLastError());
-        ctx->stats.kernel_launches += 1;
-        return LRT_OK;
-    }
+    if(!ctx->count_work) return irradiance_kernel<false>(ctx, view, points, normals, n, radius, max_depth, k, rgb, nullptr);
     LRT_CUDA(ctx, ctx->knn_work.ensure(4 * sizeof(unsigned long long)));
     unsigned long long* work = ctx->knn_work.as<unsigned long long>();
     LRT_CUDA(ctx, cudaMemsetAsync(work, 0, 4 * sizeof(unsigned long long), ctx->stream));
-    const int grid = grid_for(ctx, (const void*)k_irradiance<true>, kBlock);
-    k_irradiance<true><<<grid, kBlock, 0, ctx->stream>>>(view, points, normals, n, radius, max_depth, k, rgb, work);
-    LRT_CUDA(ctx, cudaGetLastError());
-    ctx->stats.kernel_launches += 1;
+    const int st = irradiance_kernel<true>(ctx, view, points, normals, n, radius, max_depth, k, rgb, work);
+    if(st != LRT_OK) return st;
     unsigned long long h[4];
     LRT_CUDA(ctx, cudaMemcpyAsync(h, work, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1677,7 +1778,14 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     }
     const int g_shade = grid_for(ctx, (const void*)k_eye_shade, kBlock);
     const int g_trace = grid_for(ctx, (const void*)k_eye_trace, kBlock);
-    const int g_lookup = grid_for(ctx, (const void*)k_eye_lookup, kBlock);
+    // photon lookups: heaps in shared memory unless the option knn_shared_heap is off
+    const uint32_t heap_cap = !ctx->knn_shared_heap ? 0u : (pp->lookup_size <= 64 ? 64u : 128u);
+    const void* lookup_kernel = heap_cap == 0 ? (const void*)k_eye_lookup<0> :
+                                (heap_cap == 64 ? (const void*)k_eye_lookup<64> : (const void*)k_eye_lookup<128>);
+    const int lookup_threads = heap_cap == 0 ? HeapBlock<0>::kThreads :
+                               (heap_cap == 64 ? HeapBlock<64>::kThreads : HeapBlock<128>::kThreads);
+    const int g_lookup = grid_for(ctx, lookup_kernel, lookup_threads);
+    const int g_finish = grid_for(ctx, (const void*)k_eye_finish, kBlock);
     const uint32_t spp = p->spp;
     // the wavefront form keeps refilling its slots from one large pool of samples, so that the slow drain
     // of the longest walks happens once per pool rather than once per 2^20 samples
@@ -1716,13 +1824,26 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
                         LRT_CUDA(ctx, cudaMemsetAsync(w.counters + 2, 0, 8, ctx->stream));
                         k_eye_shade<<<g_shade, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
                         k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
-                        k_eye_lookup<<<g_lookup, kBlock, 0, ctx->stream>>>(ep, w);
+                        if(heap_cap == 0) {
+                            k_eye_lookup<0><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
+                        } else if(heap_cap == 64) {
+                            k_eye_lookup<64><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
+                        } else {
+                            k_eye_lookup<128><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
+                        }
                     }
                     ctx->stats.kernel_launches += 3 * kEyeRounds;
                     uint32_t queued[4] = {0, 0, 0, 0};
                     LRT_CUDA(ctx, cudaMemcpyAsync(queued, w.counters, 16, cudaMemcpyDeviceToHost, ctx->stream));
                     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
                     if(queued[0] == 0 && queued[3] == 0) break;
+                    // the tail: every sample started and few queries left -- finish the walks in place
+                    if(queued[1] >= w.n_total && queued[0] + queued[3] <= ctx->photon_eye_tail) {
+                        k_eye_finish<<<g_finish, kBlock, 0, ctx->stream>>>(ctx->ds, ep, w);
+                        LRT_CUDA(ctx, cudaGetLastError());
+                        ctx->stats.kernel_launches += 1;
+                        break;
+                    }
                 }
             } else if(persistent) {
                 LRT_CUDA(ctx, cudaMemsetAsync(fetch, 0, 4, ctx->stream));

@@ -193,8 +193,16 @@ def test_eye_pass_kernels_agree(ctx, material):
         for mode in (0, 1, 2):
             ctx.set_option("photon_eye_kernel", mode)
             images.append(ctx.render_photon(params, pp))
+        # the wavefront form without its in-place tail (every query through the rounds), and with the
+        # lookups' heaps in local memory
+        ctx.set_option("photon_eye_tail", 0)
+        ctx.set_option("knn_shared_heap", 0)
+        images.append(ctx.render_photon(params, pp))
     finally:
         ctx.set_option("photon_eye_kernel", 2)
+        ctx.set_option("photon_eye_tail", 65536)
+        ctx.set_option("knn_shared_heap", 1)
     assert np.array_equal(images[0], images[1], equal_nan=True)
     assert np.array_equal(images[0], images[2], equal_nan=True)
+    assert np.array_equal(images[0], images[3], equal_nan=True)
     assert images[2].mean() > 0
