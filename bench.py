@@ -1044,9 +1044,11 @@ def run_profile_case(args):
     if args.case == "eye":
         ctx.upload(scenes.large_scene())
         pp, shots = ctx.photon_preprocess(args.photons, 0, max_depth=8, rr_depth=5, radius_cap=0.05, lookup_size=100)
+        ctx.reset_stats()
+        t0 = time.perf_counter()
         img = ctx.render_photon(scenes.render_params(args.size, args.size, 1, 8, 3), pp)
-        out = {"photons": args.photons, "shot": shots[0], "launches": ctx.stats()["kernel_launches"],
-               "mean": float(img.mean())}
+        out = {"photons": args.photons, "shot": shots[0], "seconds": time.perf_counter() - t0,
+               "launches": ctx.stats()["kernel_launches"], "mean": float(img.mean())}
     elif args.case == "eye_box":
         ctx.upload(scenes.cornell_box(material=args.material))
         pp, shots = ctx.photon_preprocess(PHOTONS, PHOTONS, max_depth=128, rr_depth=5, lookup_size=KNN_K)

@@ -501,9 +501,11 @@ int lrt_render_stats_reset(lrt_context* ctx);
 /* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26;
  * 0, the default: 2^24 for forward renders, 2^21 for adjoint renders; a wave never holds more paths than
  * its call renders),
+ * "photon_eye_sort" (1, the default: the wavefront eye pass shades its slots grouped by the material type of
+ * the surface each walk resumes on; 0: in slot order -- same images),
  * "photon_eye_tail" (65536: once every sample of a wavefront eye pass has started and at most this many
  * queries are queued, the remaining walks finish in place, one thread each; 0: never -- same images),
- * "knn_shared_heap" (1, the default: the irradiance lookups keep their k-nearest heaps in shared memory;
+ * "knn_shared_heap" (1, the default: irradiance lookups with k <= 64 keep their k-nearest heaps in shared memory;
  * 0: in local memory -- same results),
  * "batch_queue" (0, the default: batches as shared path waves; 1: one persistent megakernel that pulls
  * (job, 32-pixel tile) items from a device queue, costliest jobs first -- identical images),

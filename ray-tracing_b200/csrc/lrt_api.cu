@@ -1756,6 +1756,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->pixel_tile = static_cast<uint32_t>(value);
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
+    } else if(strcmp(name, "photon_eye_sort") == 0) {
+        ctx->photon_eye_sort = value != 0;
     } else if(strcmp(name, "photon_eye_tail") == 0) {
         ctx->photon_eye_tail = static_cast<uint32_t>(std::max<int64_t>(0, std::min<int64_t>(value, 1ll << 30)));
     } else if(strcmp(name, "knn_shared_heap") == 0) {

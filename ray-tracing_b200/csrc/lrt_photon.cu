@@ -1162,7 +1162,10 @@ struct EyeWave {
     EyeQuery* queries;     // kEyeBatch per slot
     uint32_t* queue;       // queries to trace (slot * kEyeBatch + index)
     uint32_t* lookups;     // photon lookups (slot * kEyeBatch + index)
-    uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch, [3] lookups
+    uint32_t* counters;    // [0] queue length, [1] next sample, [2] trace fetch, [3] lookups, [4] slots in
+                           // `order`, [5] order valid, [8, 8 + kEyeKeys) slots per key, then the key cursors
+    uint32_t* order;       // the slots to shade next round, grouped by key (when counters[5] is set)
+    uint32_t* slot_key;    // each slot's key for the grouping
     float4* L_out;
     int* overflow;
     uint32_t n_slots;
@@ -1195,10 +1198,65 @@ __device__ __forceinline__ void eye_apply_batch(const DeviceScene& s, const EyeP
     }
 }
 
+// Slots waiting for their batch are shaded grouped by the surface their walk resumes on: the key is
+// 2 + the material type of the object the batch's last hit or BSDF ray found, or of the current frame's
+// object for a batch of shadow rays and lookups (0: nothing hit, 1: no material). Warps then run one
+// material's code, as the path tracer's per-key shading does; each slot's walk is unchanged.
+constexpr int kEyeKeys = 10;
+constexpr int kEyeKeyCounts = 8;  // counters[8..] per-key counts, then per-key cursors
+
+__device__ __forceinline__ int eye_slot_key(const DeviceScene& s, const EyeSlot& S, const EyeFrame* st,
+                                            const EyeQuery* queries) {
+    int32_t obj = st[S.ln.top].obj;
+    if(S.nq > 0) {
+        const EyeQuery& Q = queries[S.nq - 1];
+        if(Q.kind == kQueryHit || Q.kind == kQueryBsdf) obj = Q.best;
+    }
+    if(obj < 0) return 0;
+    const int32_t m = s.objects[obj].material;
+    return m < 0 ? 1 : 2 + static_cast<int>(s.materials[m].type);
+}
+
+__global__ void __launch_bounds__(kBlock) k_eye_order_count(DeviceScene s, EyeWave w) {
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
+        const EyeSlot& S = w.slots[slot];
+        if(S.state != kSlotTracing) continue;
+        const int key = eye_slot_key(s, S, w.frames + static_cast<size_t>(slot) * w.frame_limit,
+                                     w.queries + static_cast<size_t>(slot) * kEyeBatch);
+        w.slot_key[slot] = static_cast<uint32_t>(key);
+        warp_append_keyed(w.counters + kEyeKeyCounts, key);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eye_order_scatter(EyeWave w) {
+    __shared__ uint32_t prefix[kEyeKeys + 1];
+    if(threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for(int k = 0; k < kEyeKeys; ++k) {
+            prefix[k] = acc;
+            acc += w.counters[kEyeKeyCounts + k];
+        }
+        prefix[kEyeKeys] = acc;
+        if(blockIdx.x == 0) {
+            w.counters[4] = acc;
+            w.counters[5] = 1;
+        }
+    }
+    __syncthreads();
+    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
+        if(w.slots[slot].state != kSlotTracing) continue;
+        const int key = static_cast<int>(w.slot_key[slot]);
+        w.order[prefix[key] + warp_append_keyed(w.counters + kEyeKeyCounts + kEyeKeys, key)] = slot;
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_eye_shade(DeviceScene s, EyeParams ep, EyeWave w) {
     uint2 heap_store[kMaxKnn];
     KnnHeap heap{heap_store, 1u, 0u};
-    for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n_slots; slot += gridDim.x * blockDim.x) {
+    const bool ordered = w.counters[5] != 0;
+    const uint32_t n = ordered ? w.counters[4] : w.n_slots;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ordered ? w.order[i] : i;
         EyeSlot& S = w.slots[slot];
         if(S.state == kSlotDone) continue;
         EyeFrame* st = w.frames + static_cast<size_t>(slot) * w.frame_limit;
@@ -1631,18 +1689,16 @@ namespace {
 template <bool kCount>
 int irradiance_kernel(lrt_context* ctx, const MapView& view, const float* points, const float* normals, uint32_t n,
                       float radius, int32_t max_depth, uint32_t k, float* rgb, unsigned long long* work) {
-    if(!ctx->knn_shared_heap) {
-        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 0>, HeapBlock<0>::kThreads);
-        k_irradiance<kCount, 0><<<grid, HeapBlock<0>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
-                                                                                 max_depth, k, rgb, work);
-    } else if(k <= 64) {
+    // shared-memory heaps only for k <= 64: a 128-entry heap leaves 32 threads per 32 KB block, 7 warps
+    // per SM, and ran slower than local heaps (the large scene's eye pass, k = 100: 2.37 against 2.08 s)
+    if(ctx->knn_shared_heap && k <= 64) {
         const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 64>, HeapBlock<64>::kThreads);
         k_irradiance<kCount, 64><<<grid, HeapBlock<64>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
                                                                                    max_depth, k, rgb, work);
     } else {
-        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 128>, HeapBlock<128>::kThreads);
-        k_irradiance<kCount, 128><<<grid, HeapBlock<128>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
-                                                                                     max_depth, k, rgb, work);
+        const int grid = grid_for(ctx, (const void*)k_irradiance<kCount, 0>, HeapBlock<0>::kThreads);
+        k_irradiance<kCount, 0><<<grid, HeapBlock<0>::kThreads, 0, ctx->stream>>>(view, points, normals, n, radius,
+                                                                                 max_depth, k, rgb, work);
     }
     LRT_CUDA(ctx, cudaGetLastError());
     ctx->stats.kernel_launches += 1;
@@ -1762,14 +1818,16 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     if(mode == 2) {
         LRT_CUDA(ctx, ctx->eye_slots.ensure(sizeof(EyeSlot) * n_slots));
         LRT_CUDA(ctx, ctx->eye_frames.ensure(sizeof(EyeFrame) * static_cast<size_t>(n_slots) * frame_limit));
-        LRT_CUDA(ctx, ctx->eye_queue.ensure(8ull * kEyeBatch * n_slots + 64));
+        LRT_CUDA(ctx, ctx->eye_queue.ensure(8ull * kEyeBatch * n_slots + 256 + 8ull * n_slots));
         LRT_CUDA(ctx, ctx->eye_queries.ensure(sizeof(EyeQuery) * kEyeBatch * static_cast<size_t>(n_slots)));
         w.slots = ctx->eye_slots.as<EyeSlot>();
         w.frames = ctx->eye_frames.as<EyeFrame>();
         w.queries = ctx->eye_queries.as<EyeQuery>();
         w.queue = ctx->eye_queue.as<uint32_t>();
         w.counters = w.queue + static_cast<size_t>(kEyeBatch) * n_slots;
-        w.lookups = w.counters + 16;
+        w.lookups = w.counters + 64;
+        w.order = w.lookups + static_cast<size_t>(kEyeBatch) * n_slots;
+        w.slot_key = w.order + n_slots;
         w.L_out = L;
         w.overflow = overflow;
         w.frame_limit = frame_limit;
@@ -1778,14 +1836,13 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     }
     const int g_shade = grid_for(ctx, (const void*)k_eye_shade, kBlock);
     const int g_trace = grid_for(ctx, (const void*)k_eye_trace, kBlock);
-    // photon lookups: heaps in shared memory unless the option knn_shared_heap is off
-    const uint32_t heap_cap = !ctx->knn_shared_heap ? 0u : (pp->lookup_size <= 64 ? 64u : 128u);
-    const void* lookup_kernel = heap_cap == 0 ? (const void*)k_eye_lookup<0> :
-                                (heap_cap == 64 ? (const void*)k_eye_lookup<64> : (const void*)k_eye_lookup<128>);
-    const int lookup_threads = heap_cap == 0 ? HeapBlock<0>::kThreads :
-                               (heap_cap == 64 ? HeapBlock<64>::kThreads : HeapBlock<128>::kThreads);
+    // photon lookups: heaps in shared memory for k <= 64 (option knn_shared_heap), else in local memory
+    const uint32_t heap_cap = ctx->knn_shared_heap && pp->lookup_size <= 64 ? 64u : 0u;
+    const void* lookup_kernel = heap_cap == 0 ? (const void*)k_eye_lookup<0> : (const void*)k_eye_lookup<64>;
+    const int lookup_threads = heap_cap == 0 ? HeapBlock<0>::kThreads : HeapBlock<64>::kThreads;
     const int g_lookup = grid_for(ctx, lookup_kernel, lookup_threads);
     const int g_finish = grid_for(ctx, (const void*)k_eye_finish, kBlock);
+    const int g_order = grid_for(ctx, (const void*)k_eye_order_count, kBlock);
     const uint32_t spp = p->spp;
     // the wavefront form keeps refilling its slots from one large pool of samples, so that the slow drain
     // of the longest walks happens once per pool rather than once per 2^20 samples
@@ -1812,7 +1869,7 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
                 w.n_samples = ns;
                 w.sample_begin = p->sample_offset + sb;
                 LRT_CUDA(ctx, cudaMemsetAsync(w.slots, 0, sizeof(EyeSlot) * w.n_slots, ctx->stream));
-                LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 16, ctx->stream));
+                LRT_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 256, ctx->stream));
                 // rounds of (advance every slot to its next query, trace the queued queries), kEyeRounds at a
                 // time without a host round trip: the trace kernel reads the queue length on the device, and
                 // rounds past the last query find every slot done and launch no work. The host reads the
@@ -1826,13 +1883,16 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
                         k_eye_trace<<<g_trace, kBlock, 0, ctx->stream>>>(ctx->ds, w);
                         if(heap_cap == 0) {
                             k_eye_lookup<0><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
-                        } else if(heap_cap == 64) {
-                            k_eye_lookup<64><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
                         } else {
-                            k_eye_lookup<128><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
+                            k_eye_lookup<64><<<g_lookup, lookup_threads, 0, ctx->stream>>>(ep, w);
+                        }
+                        if(ctx->photon_eye_sort) {  // next round's shading order, grouped by key
+                            LRT_CUDA(ctx, cudaMemsetAsync(w.counters + kEyeKeyCounts, 0, 8 * kEyeKeys, ctx->stream));
+                            k_eye_order_count<<<g_order, kBlock, 0, ctx->stream>>>(ctx->ds, w);
+                            k_eye_order_scatter<<<g_order, kBlock, 0, ctx->stream>>>(w);
                         }
                     }
-                    ctx->stats.kernel_launches += 3 * kEyeRounds;
+                    ctx->stats.kernel_launches += (ctx->photon_eye_sort ? 5 : 3) * kEyeRounds;
                     uint32_t queued[4] = {0, 0, 0, 0};
                     LRT_CUDA(ctx, cudaMemcpyAsync(queued, w.counters, 16, cudaMemcpyDeviceToHost, ctx->stream));
                     LRT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

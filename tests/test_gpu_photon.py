@@ -193,15 +193,17 @@ def test_eye_pass_kernels_agree(ctx, material):
         for mode in (0, 1, 2):
             ctx.set_option("photon_eye_kernel", mode)
             images.append(ctx.render_photon(params, pp))
-        # the wavefront form without its in-place tail (every query through the rounds), and with the
-        # lookups' heaps in local memory
+        # the wavefront form without its in-place tail (every query through the rounds), with the
+        # lookups' heaps in local memory and the slots shaded in slot order
         ctx.set_option("photon_eye_tail", 0)
         ctx.set_option("knn_shared_heap", 0)
+        ctx.set_option("photon_eye_sort", 0)
         images.append(ctx.render_photon(params, pp))
     finally:
         ctx.set_option("photon_eye_kernel", 2)
         ctx.set_option("photon_eye_tail", 65536)
         ctx.set_option("knn_shared_heap", 1)
+        ctx.set_option("photon_eye_sort", 1)
     assert np.array_equal(images[0], images[1], equal_nan=True)
     assert np.array_equal(images[0], images[2], equal_nan=True)
     assert np.array_equal(images[0], images[3], equal_nan=True)
