@@ -904,6 +904,72 @@ void collect_stage_times(lrt_context* ctx) {
     ctx->event_stage.clear();
 }
 
+// The wave plan of one render -- the pixel range [pix0, pix1) x the sample range, at most `cap` slots
+// per wave -- and its launches: ray generation, per bounce extend, hit records, shading and shadow rays,
+// then the accumulation. Shared by lrt_render(_dev) and the allocation-free entry point, which differ
+// only in where the wave's arrays live; `stages` records the stage events of the option stage_timing.
+int run_render_waves(lrt_context* ctx, WaveArgs& a, const lrt_render_params* p, uint32_t pix0, uint32_t pix1,
+                     uint32_t cap, size_t counters_bytes, bool cnt, bool stages, float* rgb_dev, uint64_t& launches) {
+    const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
+    const int g_extend =
+        grid_for(ctx, cnt ? (const void*)k_extend_persistent<true> : (const void*)k_extend_persistent<false>, kBlock);
+    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
+    const ShadeLaunch shade = shade_launch(ctx);
+    const int g_shadow =
+        grid_for(ctx, cnt ? (const void*)k_shadow_persistent<true> : (const void*)k_shadow_persistent<false>, kBlock);
+    const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
+    auto stage = [&](int which, bool begin) {
+        if(stages) record_stage(ctx, which, begin);
+    };
+    const uint32_t spp = p->spp;
+    const uint32_t samples_per_wave = std::min(spp, cap);
+    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
+    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
+        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
+        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
+            const uint32_t ns = std::min(samples_per_wave, spp - sb);
+            a.pixel_begin = pb;
+            a.n_pixels = np;
+            a.sample_begin = p->sample_offset + sb;
+            a.n_samples = ns;
+            LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
+            stage(LRT_STAGE_RAYGEN, true);
+            k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
+            stage(LRT_STAGE_RAYGEN, false);
+            launches += 1;
+            for(int depth = 0; depth < p->max_depth; ++depth) {
+                stage(LRT_STAGE_EXTEND, true);
+                if(cnt) {
+                    k_extend_persistent<true><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                } else {
+                    k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
+                }
+                stage(LRT_STAGE_EXTEND, false);
+                stage(LRT_STAGE_SORT, true);
+                k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
+                stage(LRT_STAGE_SORT, false);
+                stage(LRT_STAGE_SHADE, true);
+                launch_shade(shade, a, depth, ctx->stream);
+                stage(LRT_STAGE_SHADE, false);
+                stage(LRT_STAGE_SHADOW, true);
+                if(cnt) {
+                    k_shadow_persistent<true><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                } else {
+                    k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+                }
+                stage(LRT_STAGE_SHADOW, false);
+                launches += 3 + shade_launch_count(shade);
+            }
+            stage(LRT_STAGE_ACCUM, true);
+            k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
+            stage(LRT_STAGE_ACCUM, false);
+            launches += 1;
+            LRT_CUDA(ctx, cudaGetLastError());
+        }
+    }
+    return LRT_OK;
+}
+
 int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     if(!ctx->has_scene) return fail(ctx, LRT_ERR_NO_SCENE, "no scene uploaded");
     if(!p || p->width < 2 || p->height < 2 || p->spp == 0 || p->max_depth < 1 || p->max_depth > 1024) {
@@ -953,65 +1019,12 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     a.work = work;
 
     const bool cnt = ctx->count_work;
-    const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
-    const int g_extend =
-        grid_for(ctx, cnt ? (const void*)k_extend_persistent<true> : (const void*)k_extend_persistent<false>, kBlock);
-    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const ShadeLaunch shade = shade_launch(ctx);
-    const int g_shadow =
-        grid_for(ctx, cnt ? (const void*)k_shadow_persistent<true> : (const void*)k_shadow_persistent<false>, kBlock);
-    const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
-
-    // wave plan: a pixel range x a sample range, at most `cap` slots
-    const uint32_t spp = p->spp;
-    const uint32_t samples_per_wave = std::min(spp, cap);
-    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
     const uint32_t pix0 = row_begin * p->width;
     const uint32_t pix1 = row_end * p->width;
+    const uint32_t spp = p->spp;
     uint64_t launches = 0;
-    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
-        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
-        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
-            const uint32_t ns = std::min(samples_per_wave, spp - sb);
-            a.pixel_begin = pb;
-            a.n_pixels = np;
-            a.sample_begin = p->sample_offset + sb;
-            a.n_samples = ns;
-            LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
-            record_stage(ctx, LRT_STAGE_RAYGEN, true);
-            k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
-            record_stage(ctx, LRT_STAGE_RAYGEN, false);
-            launches += 1;
-            for(int depth = 0; depth < p->max_depth; ++depth) {
-                record_stage(ctx, LRT_STAGE_EXTEND, true);
-                if(cnt) {
-                    k_extend_persistent<true><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
-                } else {
-                    k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
-                }
-                record_stage(ctx, LRT_STAGE_EXTEND, false);
-                record_stage(ctx, LRT_STAGE_SORT, true);
-                k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
-                record_stage(ctx, LRT_STAGE_SORT, false);
-                record_stage(ctx, LRT_STAGE_SHADE, true);
-                launch_shade(shade, a, depth, ctx->stream);
-                record_stage(ctx, LRT_STAGE_SHADE, false);
-                record_stage(ctx, LRT_STAGE_SHADOW, true);
-                if(cnt) {
-                    k_shadow_persistent<true><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
-                } else {
-                    k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
-                }
-                record_stage(ctx, LRT_STAGE_SHADOW, false);
-                launches += 3 + shade_launch_count(shade);
-            }
-            record_stage(ctx, LRT_STAGE_ACCUM, true);
-            k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
-            record_stage(ctx, LRT_STAGE_ACCUM, false);
-            launches += 1;
-            LRT_CUDA(ctx, cudaGetLastError());
-        }
-    }
+    st = run_render_waves(ctx, a, p, pix0, pix1, cap, counters_bytes, cnt, true, rgb_dev, launches);
+    if(st != LRT_OK) return st;
     ctx->stats.paths += static_cast<uint64_t>(pix1 - pix0) * spp;
     ctx->stats.kernel_launches += launches;
     if(ctx->stage_timing || cnt) {
@@ -1892,39 +1905,12 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
     a.rr_depth = p->rr_depth;
     const size_t counters_bytes = sizeof(BounceCounters) * (p->max_depth + 1);
 
-    const int g_raygen = grid_for(ctx, (const void*)k_raygen, kBlock);
-    const int g_extend = grid_for(ctx, (const void*)k_extend_persistent<false>, kBlock);
-    const int g_hitrec = grid_for(ctx, (const void*)k_hitrec, kBlock);
-    const ShadeLaunch shade = shade_launch(ctx);
-    const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
-    const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
     const uint32_t spp = p->spp;
-    const uint32_t samples_per_wave = std::min(spp, cap);
-    const uint32_t pixels_per_wave = std::max(1u, cap / samples_per_wave);
     const uint32_t pix0 = row_begin * p->width;
     const uint32_t pix1 = row_end * p->width;
     uint64_t launches = 0;
-    for(uint32_t pb = pix0; pb < pix1; pb += pixels_per_wave) {
-        const uint32_t np = std::min(pixels_per_wave, pix1 - pb);
-        for(uint32_t sb = 0; sb < spp; sb += samples_per_wave) {
-            const uint32_t ns = std::min(samples_per_wave, spp - sb);
-            a.pixel_begin = pb;
-            a.n_pixels = np;
-            a.sample_begin = p->sample_offset + sb;
-            a.n_samples = ns;
-            LRT_CUDA(ctx, cudaMemsetAsync(a.counters, 0, counters_bytes, ctx->stream));
-            k_raygen<<<g_raygen, kBlock, 0, ctx->stream>>>(a);
-            for(int depth = 0; depth < p->max_depth; ++depth) {
-                k_extend_persistent<false><<<g_extend, kBlock, 0, ctx->stream>>>(a, depth);
-                k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
-                launch_shade(shade, a, depth, ctx->stream);
-                k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
-            }
-            k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
-            launches += 2 + (3ull + shade_launch_count(shade)) * p->max_depth;
-            LRT_CUDA(ctx, cudaGetLastError());
-        }
-    }
+    const int rst = run_render_waves(ctx, a, p, pix0, pix1, cap, counters_bytes, false, false, rgb_dev, launches);
+    if(rst != LRT_OK) return rst;
     ctx->stats.paths += static_cast<uint64_t>(pix1 - pix0) * spp;
     ctx->stats.kernel_launches += launches;
     return LRT_OK;
