@@ -205,7 +205,8 @@ struct WaveArgs {
     uint32_t* keyed; // kKeys segments of `capacity`
     float4* sh_o;    // shadow origin, tmax
     float4* sh_d;    // shadow direction, light index bits
-    float4* sh_c;    // contribution rgb, path id bits
+    float4* sh_c;    // contribution rgb, path id bits (a sky sample: the contribution before its radiance)
+    float* sh_s;     // a sky sample: the factor w / light_pdf applied after the radiance
     BounceCounters* counters;
     unsigned long long* work;  // [0] nodes, [1] triangles, [2] shading events, [3] extension rays, [4] shadow rays
     float* sum;      // per-pixel running sums (3 floats per pixel of the wave)
@@ -350,6 +351,35 @@ __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
     }
 }
 
+// A shadow record's light index carries two flags: a sky sample whose radiance waits for the ray's
+// visibility, and that ray found unoccluded. The shading kernels sample the sky's direction only; the
+// FP64 sky model (env_emitter::eval) then runs in k_shadow_sky for the unoccluded rays alone, and the
+// contribution is ((throughput * f) * radiance) * (w / light_pdf), the expression of path_integrator.h:118.
+constexpr int32_t kShadowSkyDeferred = 1 << 30;
+constexpr int32_t kShadowSkyVisible = 1 << 29;
+constexpr int32_t kShadowLightMask = kShadowSkyVisible - 1;
+
+__global__ void __launch_bounds__(kBlock) k_shadow_sky(WaveArgs a, int depth) {
+    const BounceCounters& bc = a.counters[depth];
+    const uint32_t n0 = bc.shadow[0];
+    const uint32_t n = n0 + bc.shadow[1];
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t k = i < n0 ? i : a.capacity + (i - n0);
+        const float4 d = a.sh_d[k];
+        const int32_t bits = __float_as_int(d.w);
+        if((bits & (kShadowSkyDeferred | kShadowSkyVisible)) != (kShadowSkyDeferred | kShadowSkyVisible)) continue;
+        const f3 radiance = env_eval(a.s.emitters[bits & kShadowLightMask], f3{d.x, d.y, d.z});
+        const float4 c = a.sh_c[k];
+        const f3 contrib = f3{c.x, c.y, c.z} * radiance * a.sh_s[k];
+        const uint32_t p = __float_as_uint(c.w);
+        float4 L = a.L[p];
+        L.x += contrib.x;
+        L.y += contrib.y;
+        L.z += contrib.z;
+        a.L[p] = L;
+    }
+}
+
 // shadow rays with ray replacement: any-hit unless the light's own shape is reachable (then the
 // closest hit decides, scene_occluded)
 template <bool kCount, bool kVis = false>
@@ -371,7 +401,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
             if(!active && i < n) {
                 k = i < n0 ? i : a.capacity + (i - n0);
                 const float4 o = a.sh_o[k], d = a.sh_d[k];
-                light = __float_as_int(d.w);
+                light = __float_as_int(d.w) & kShadowLightMask;
                 const Ray r{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}};
                 bool any_mode = true;
                 const EmitRec& e = a.s.emitters[light];
@@ -385,7 +415,10 @@ __global__ void __launch_bounds__(kBlock, 8) k_shadow_persistent(WaveArgs a, int
         if(active && trav_step<kCount, true>(a.s, st, stack, tl_stack, cnt)) {
             const bool blocked = st.any_mode ? st.best >= 0 : (st.best >= 0 && a.s.objects[st.best].emitter != light);
             if(kVis) a.adj_sh_vis[k] = blocked ? 0 : 1;
-            if(!blocked) {
+            const int32_t bits = __float_as_int(a.sh_d[k].w);
+            if(!blocked && (bits & kShadowSkyDeferred)) {  // k_shadow_sky adds it with the sky's radiance
+                reinterpret_cast<int32_t*>(a.sh_d + k)[3] = bits | kShadowSkyVisible;
+            } else if(!blocked) {
                 const float4 c = a.sh_c[k];
                 const uint32_t p = __float_as_uint(c.w);
                 float4 L = a.L[p];
@@ -411,6 +444,7 @@ template <bool kAdj, int kKey = -1>
 __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_t* prefix) {
     constexpr int kType = kKey >= 2 ? kKey - 2 : -1;
     constexpr bool kMeshLights = kKey < 0;  // the per-key kernels run only on scenes without mesh lights
+    constexpr bool kDeferSky = !kAdj;       // the adjoint needs the sky radiance of every NEE sample here
     BounceCounters& bc = a.counters[depth];
     if(kKey < 0 && threadIdx.x == 0) {
         uint32_t acc = 0;
@@ -508,7 +542,8 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
         if((mat.flags & (kDiffuse | kGlossy)) != 0) {  // NEE (path_integrator.h:86-128)
             DirectSample light{};
             light.distance = kInf;
-            if(sample_emitter_direction<kMeshLights>(s, p, light_uv.x, light_uv.y, light)) {
+            if(sample_emitter_direction<kMeshLights, !kDeferSky>(s, p, light_uv.x, light_uv.y, light)) {
+                const bool sky = kDeferSky && s.emitters[light.emitter].kind == LRT_EMITTER_ENV;
                 const f3 shadow_origin = p + normal * 1e-4f;
                 f3 shadow_dir = light.direction;
                 float tmax = kInf;
@@ -531,12 +566,16 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
                         const float light_pdf = pdf_emitter_direction<kMeshLights>(s, p, shadow_dir);
                         if(light_pdf > 0.0f) {
                             const float w = power_heuristic(light_pdf, bsdf_pdf_v);
-                            const f3 contrib = throughput * f_cos * light.radiance * (w / light_pdf);
+                            // a sky sample leaves radiance and w / light_pdf to k_shadow_sky
+                            const f3 contrib = sky ? throughput * f_cos
+                                                   : throughput * f_cos * light.radiance * (w / light_pdf);
                             const int seg = heavy_key(s, Ray{shadow_origin, shadow_dir}, 0.001f, tmax);
                             const size_t si = static_cast<size_t>(seg) * a.capacity + warp_append_keyed(bc.shadow, seg);
                             a.sh_o[si] = make_float4(shadow_origin.x, shadow_origin.y, shadow_origin.z, tmax);
-                            a.sh_d[si] = make_float4(shadow_dir.x, shadow_dir.y, shadow_dir.z, __int_as_float(light.emitter));
+                            a.sh_d[si] = make_float4(shadow_dir.x, shadow_dir.y, shadow_dir.z,
+                                                     __int_as_float(light.emitter | (sky ? kShadowSkyDeferred : 0)));
                             a.sh_c[si] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(pid));
+                            if(sky) a.sh_s[si] = w / light_pdf;
                             if(kAdj) {  // delta x dNEE per group, kept until the shadow ray's visibility is known
                                 int32_t smid = -1;
                                 if(!is_zero(delta)) {
@@ -874,6 +913,7 @@ int ensure_wave(lrt_context* ctx, uint32_t cap) {
     LRT_CUDA(ctx, w.sh_o.ensure(c * 32));
     LRT_CUDA(ctx, w.sh_d.ensure(c * 32));
     LRT_CUDA(ctx, w.sh_c.ensure(c * 32));
+    LRT_CUDA(ctx, w.sh_s.ensure(c * 8));
     LRT_CUDA(ctx, w.sum.ensure(c * 12));
     w.capacity = cap;
     return LRT_OK;
@@ -918,6 +958,7 @@ int run_render_waves(lrt_context* ctx, WaveArgs& a, const lrt_render_params* p, 
     const int g_shadow =
         grid_for(ctx, cnt ? (const void*)k_shadow_persistent<true> : (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate, kBlock);
+    const int g_sky = grid_for(ctx, (const void*)k_shadow_sky, kBlock);
     auto stage = [&](int which, bool begin) {
         if(stages) record_stage(ctx, which, begin);
     };
@@ -957,8 +998,9 @@ int run_render_waves(lrt_context* ctx, WaveArgs& a, const lrt_render_params* p, 
                 } else {
                     k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
                 }
+                if(ctx->has_sky) k_shadow_sky<<<g_sky, kBlock, 0, ctx->stream>>>(a, depth);
                 stage(LRT_STAGE_SHADOW, false);
-                launches += 3 + shade_launch_count(shade);
+                launches += 3 + shade_launch_count(shade) + (ctx->has_sky ? 1 : 0);
             }
             stage(LRT_STAGE_ACCUM, true);
             k_accumulate<<<g_accum, kBlock, 0, ctx->stream>>>(a, rgb_dev, spp, sb == 0 ? 1 : 0, sb + ns >= spp ? 1 : 0);
@@ -1002,6 +1044,7 @@ int render_impl(lrt_context* ctx, const lrt_render_params* p, float* rgb_dev) {
     a.sh_o = w.sh_o.as<float4>();
     a.sh_d = w.sh_d.as<float4>();
     a.sh_c = w.sh_c.as<float4>();
+    a.sh_s = w.sh_s.as<float>();
     a.counters = ctx->counters.as<BounceCounters>();
     a.sum = w.sum.as<float>();
     a.capacity = cap;
@@ -1057,6 +1100,7 @@ void launch_batch_wave(lrt_context* ctx, const WaveArgs& a, size_t counters_byte
         k_hitrec<<<g_hitrec, kBlock, 0, ctx->stream>>>(a, depth);
         launch_shade(shade, a, depth, ctx->stream);
         k_shadow_persistent<false><<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
+        if(ctx->has_sky) k_shadow_sky<<<g_shadow, kBlock, 0, ctx->stream>>>(a, depth);
     }
     k_accumulate_batch<<<g_accum, kBlock, 0, ctx->stream>>>(a);
     k_wave_advance<<<1, 32, 0, ctx->stream>>>(a);
@@ -1094,6 +1138,7 @@ int batch_wave_args(lrt_context* ctx, const std::vector<JobRec>& recs, unsigned 
     a.sh_o = w.sh_o.as<float4>();
     a.sh_d = w.sh_d.as<float4>();
     a.sh_c = w.sh_c.as<float4>();
+    a.sh_s = w.sh_s.as<float>();
     a.counters = ctx->counters.as<BounceCounters>();
     a.sum = w.sum.as<float>();
     a.capacity = cap;
@@ -1162,7 +1207,7 @@ int render_batch_impl(lrt_context* ctx, const lrt_job_desc* jobs, uint32_t n_job
     const int g_shadow = grid_for(ctx, (const void*)k_shadow_persistent<false>, kBlock);
     const int g_accum = grid_for(ctx, (const void*)k_accumulate_batch, kBlock);
     const unsigned long long waves = (total + a.capacity - 1) / a.capacity;
-    const uint64_t per_wave = 3 + (3ull + shade_launch_count(shade)) * max_depth;
+    const uint64_t per_wave = 3 + (3ull + shade_launch_count(shade) + (ctx->has_sky ? 1 : 0)) * max_depth;
     const int rst = run_waves(ctx, waves, [&]() {
         launch_batch_wave(ctx, a, counters_bytes, g_raygen, g_extend, g_hitrec, shade, g_shadow, g_accum);
     });
@@ -1505,6 +1550,8 @@ int lrt_scene_upload(lrt_context* ctx, const lrt_scene_desc* desc) {
     // shading keys a hit can carry: misses, hits without a BSDF, and 2 + each material type present
     ctx->shade_keys = 3u;
     for(const MatRec& m : h.materials) ctx->shade_keys |= 1u << (2 + m.type);
+    ctx->has_sky = false;
+    for(const EmitRec& e : h.emitters) ctx->has_sky |= e.kind == LRT_EMITTER_ENV;
     ctx->has_mesh_lights = false;
     for(const EmitRec& e : h.emitters) {
         ctx->has_mesh_lights |= e.kind == LRT_EMITTER_AREA && e.shape == LRT_OBJECT_MESH;
@@ -1819,11 +1866,12 @@ std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {nullptr};
 
 // bytes of wavefront state per path slot: o, d, tp, L, hit_p, hit_n, sh_o, sh_d, sh_c (float4 each),
-// misc (float2), id (uint2), two queues, kKeys shading segments and the per-pixel sum (3 floats)
-constexpr size_t kNoAllocSlotBytes = 6 * 16 + 3 * 32 + 8 + 8 + 2 * 8 + kKeys * 4 + 12;
+// sh_s (float), misc (float2), id (uint2), two queues, kKeys shading segments and the per-pixel sum
+// (3 floats); the shadow arrays have two entries per slot
+constexpr size_t kNoAllocSlotBytes = 6 * 16 + 3 * 32 + 2 * 4 + 8 + 8 + 2 * 8 + kKeys * 4 + 12;
 constexpr size_t kNoAllocHeaderBytes = (sizeof(BounceCounters) * (kNoAllocMaxDepth + 1) + 255) / 256 * 256;
 constexpr uint32_t kNoAllocCapacity =
-    static_cast<uint32_t>((kNoAllocScratchBytes - kNoAllocHeaderBytes - 16 * 256) / kNoAllocSlotBytes);
+    static_cast<uint32_t>((kNoAllocScratchBytes - kNoAllocHeaderBytes - 17 * 256) / kNoAllocSlotBytes);
 
 int noalloc_scratch(lrt_context* ctx, unsigned char** base) {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -1890,6 +1938,7 @@ extern "C" int lrt_render_dev_noalloc(lrt_context* ctx, const lrt_render_params*
     a.sh_o = reinterpret_cast<float4*>(take(32ull * cap));
     a.sh_d = reinterpret_cast<float4*>(take(32ull * cap));
     a.sh_c = reinterpret_cast<float4*>(take(32ull * cap));
+    a.sh_s = reinterpret_cast<float*>(take(8ull * cap));
     a.misc = reinterpret_cast<float2*>(take(8ull * cap));
     a.id = reinterpret_cast<uint2*>(take(8ull * cap));
     a.q0 = reinterpret_cast<uint32_t*>(take(8ull * cap));

@@ -65,7 +65,7 @@ static_assert(sizeof(BounceCounters) == 64, "counter layout");
 
 struct WaveState {
     uint32_t capacity = 0;
-    DevBuf o, d, tp, L, misc, id, hit_p, hit_n, q0, q1, keyed, sh_o, sh_d, sh_c, sum;
+    DevBuf o, d, tp, L, misc, id, hit_p, hit_n, q0, q1, keyed, sh_o, sh_d, sh_c, sh_s, sum;
 };
 
 // photon map in tree order: positions carry the caller's index in w (bits)
@@ -134,7 +134,8 @@ struct lrt_context {
     int photon_tree_depth_limit = -1;  // introselect's partition budget per node (-1: 2*floor(log2(n)), as std::nth_element)
     bool shade_per_key = true;  // one shading kernel per material type present (false: one for all)
     uint32_t shade_keys = 3u;    // bit k: shading key k can occur in the uploaded scene
-    bool has_mesh_lights = false;  // a mesh is an area light: the one all-keys shading kernel runs
+    bool has_mesh_lights = false;
+    bool has_sky = false;  // an env emitter: the path tracer's sky NEE radiance is evaluated after visibility  // a mesh is an area light: the one all-keys shading kernel runs
     int kd_build_device = 2;  // lrt_scene_upload's kd-trees: 0 host cores, 1 GPU, 2 GPU from 2^15 triangles
     int photon_eye_kernel = 2;  // 0: one sample per thread; 1: persistent lanes; 2: wavefront slots
     lrt::DevBuf eye_slots, eye_frames, eye_queue, eye_L, eye_queries;

@@ -861,7 +861,9 @@ __device__ __forceinline__ bool area_sample(const DeviceScene& s, const EmitRec&
     return true;
 }
 
-// env_emitter::sample (env_emitter.h:33-53)
+// env_emitter::sample (env_emitter.h:33-53); kRadiance = false leaves out.radiance to the caller (the
+// path tracer evaluates the sky only for shadow rays that turn out unoccluded)
+template <bool kRadiance = true>
 __device__ __forceinline__ bool env_sample(const EmitRec& e, float sx, float sy, DirectSample& out) {
     if(!e.sun_active) return false;
     const float cos_theta = (1.0f - sx) + sx * e.cos_cutoff;
@@ -873,13 +875,13 @@ __device__ __forceinline__ bool env_sample(const EmitRec& e, float sx, float sy,
     const f3 a0 = load3(e.frame[0]), a1 = load3(e.frame[1]), a2 = load3(e.frame[2]);
     out.direction = a0 * local.x + a1 * local.y + a2 * local.z;
     out.pdf = e.cone_pdf;
-    out.radiance = env_eval(e, out.direction);
+    out.radiance = kRadiance ? env_eval(e, out.direction) : mk(0.0f);
     out.distance = kInf;
     return true;
 }
 
 // scene::sample_emitter_direction (scene.h:73-93): uniform 1/n light pick on sample.x
-template <bool kMeshLights = true>
+template <bool kMeshLights = true, bool kEnvRadiance = true>
 __device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f3 shading_point, float sx, float sy,
                                                          DirectSample& out) {
     const int32_t count = s.n_emitters;
@@ -891,7 +893,8 @@ __device__ __forceinline__ bool sample_emitter_direction(const DeviceScene& s, f
     const EmitRec& e = s.emitters[index];
     out.distance = kInf;
     out.pdf = 0.0f;
-    const bool ok = e.kind == LRT_EMITTER_ENV ? env_sample(e, rx, sy, out) : area_sample<kMeshLights>(s, e, shading_point, rx, sy, out);
+    const bool ok = e.kind == LRT_EMITTER_ENV ? env_sample<kEnvRadiance>(e, rx, sy, out)
+                                              : area_sample<kMeshLights>(s, e, shading_point, rx, sy, out);
     if(!ok) return false;
     out.emitter = index;
     out.pdf *= 1.0f / static_cast<float>(count);

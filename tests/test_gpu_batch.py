@@ -110,15 +110,17 @@ def test_batch_stats_count_paths(ctx, library):
     ctx.render_batch(jobs, DEPTH, RR)
     st = ctx.stats()
     assert st["paths"] == 16 * 16 * 3 + 8 * 12 * 5
-    # one wave: raygen, accumulate, advance; per bounce extend, hit records, shadow and one shading
-    # kernel per key the scene can produce (misses, hits without a BSDF, each material type)
+    # one wave: raygen, accumulate, advance; per bounce extend, hit records, shadow, the sky samples'
+    # radiance (the scene has a sky) and one shading kernel per key the scene can produce (misses, hits
+    # without a BSDF, each material type)
     keys = 2 + len({m["type"] for m in scene.materials})
-    assert st["kernel_launches"] == 3 + (3 + keys) * DEPTH
+    sky = int(any(e["kind"] == abi.EMITTER_ENV for e in scene.emitters))
+    assert st["kernel_launches"] == 3 + (3 + sky + keys) * DEPTH
     ctx.set_option("shade_per_key", 0)
     try:
         ctx.reset_stats()
         ctx.render_batch(jobs, DEPTH, RR)
-        assert ctx.stats()["kernel_launches"] == 3 + 4 * DEPTH
+        assert ctx.stats()["kernel_launches"] == 3 + (4 + sky) * DEPTH
     finally:
         ctx.set_option("shade_per_key", 1)
 
