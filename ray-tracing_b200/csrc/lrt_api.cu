@@ -658,8 +658,10 @@ __global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
     shade_wave<true>(a, depth, prefix);
 }
 
+// The forward kernels of misses, hits without a BSDF and the diffuse material are held to 80 registers
+// (6 resident blocks per SM instead of 4, no spills): the diffuse walls are most of the shading.
 template <int kKey, bool kAdj = false>
-__global__ void __launch_bounds__(kBlock) k_shade_key(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(kBlock, (!kAdj && kKey >= 0 && kKey <= 2) ? 6 : 1) k_shade_key(WaveArgs a, int depth) {
     shade_wave<kAdj, kKey>(a, depth, nullptr);
 }
 

@@ -738,14 +738,27 @@ __device__ __forceinline__ void hit_record_of(const DeviceScene& s, const Ray& r
 }
 
 // ---- sky: env_emitter::eval (env_emitter.h:71-88) + ArHosekSkyModel_GetRadianceInternal (double) ----
-__device__ __forceinline__ double hosek_radiance(const double* cfg, double theta, double gamma) {
-    const double cos_gamma = cos(gamma);
-    const double expM = exp(cfg[4] * gamma);
-    const double rayM = cos_gamma * cos_gamma;
-    const double mieM = (1.0 + cos_gamma * cos_gamma) / pow((1.0 + cfg[8] * cfg[8] - 2.0 * cfg[8] * cos_gamma), 1.5);
-    const double zenith = sqrt(cos(theta));
-    return (1.0 + cfg[0] * exp(cfg[1] / (cos(theta) + 0.01))) *
-           (cfg[2] + cfg[3] * expM + cfg[5] * rayM + cfg[6] * mieM + cfg[7] * zenith);
+// The terms of ArHosekSkyModel_GetRadianceInternal that do not depend on the channel, computed once per
+// direction (the same double values the per-channel evaluation computes).
+struct HosekAngles {
+    double gamma, cos_gamma, cos_theta, zenith;
+};
+
+__device__ __forceinline__ HosekAngles hosek_angles(double theta, double gamma) {
+    HosekAngles h;
+    h.gamma = gamma;
+    h.cos_gamma = cos(gamma);
+    h.cos_theta = cos(theta);
+    h.zenith = sqrt(h.cos_theta);
+    return h;
+}
+
+__device__ __forceinline__ double hosek_radiance(const double* cfg, const HosekAngles& h) {
+    const double expM = exp(cfg[4] * h.gamma);
+    const double rayM = h.cos_gamma * h.cos_gamma;
+    const double mieM = (1.0 + h.cos_gamma * h.cos_gamma) / pow((1.0 + cfg[8] * cfg[8] - 2.0 * cfg[8] * h.cos_gamma), 1.5);
+    return (1.0 + cfg[0] * exp(cfg[1] / (h.cos_theta + 0.01))) *
+           (cfg[2] + cfg[3] * expM + cfg[5] * rayM + cfg[6] * mieM + cfg[7] * h.zenith);
 }
 
 __device__ __forceinline__ f3 env_eval(const EmitRec& e, f3 direction) {
@@ -753,9 +766,10 @@ __device__ __forceinline__ f3 env_eval(const EmitRec& e, f3 direction) {
     if(dir.y <= 0.0f) return mk(1.0f);
     const float theta = acos_rn(sclamp(dir.y, 0.0f, 1.0f));
     const float gamma = acos_rn(sclamp(dot(dir, load3(e.sun)), -1.0f, 1.0f));
-    const f3 c{static_cast<float>(hosek_radiance(e.cfg[0], theta, gamma) * e.rad[0]),
-               static_cast<float>(hosek_radiance(e.cfg[1], theta, gamma) * e.rad[1]),
-               static_cast<float>(hosek_radiance(e.cfg[2], theta, gamma) * e.rad[2])};
+    const HosekAngles h = hosek_angles(theta, gamma);
+    const f3 c{static_cast<float>(hosek_radiance(e.cfg[0], h) * e.rad[0]),
+               static_cast<float>(hosek_radiance(e.cfg[1], h) * e.rad[1]),
+               static_cast<float>(hosek_radiance(e.cfg[2], h) * e.rad[2])};
     return c * e.scale;
 }
 
