@@ -73,22 +73,27 @@ def measured_peaks():
 def source_digest(names):
     """first 16 hex digits of the SHA-256 of the named library sources (ties a capture to its kernel). A
     name "file:marker" takes only the text of file from the line holding marker to the next line that is
-    a lone closing brace (one function), so that edits elsewhere in a large file leave the digest alone."""
+    a lone closing brace (one function), so that edits elsewhere in a large file leave the digest alone;
+    "file@marker" takes the text of file up to marker (its leading part)."""
     h = hashlib.sha256()
     for n in names:
         path, _, marker = n.partition(":")
+        path, _, until = path.partition("@")
         with open(os.path.join(ROOT, "ray-tracing_b200", "csrc", path), "rb") as f:
             text = f.read()
         if marker:
             i = text.index(marker.encode())
             i = text.rindex(b"\n", 0, i) + 1
             text = text[i:text.index(b"\n}\n", i) + 3]
+        if until:
+            text = text[:text.index(until.encode())]
         h.update(text)
     return h.hexdigest()[:16]
 
 
-# the closest-hit kernel: its traversal headers and its own function in lrt_api.cu
-EXTEND_SOURCES = ["lrt_scene.cuh", "lrt_math.cuh", "lrt_types.h",
+# the closest-hit kernel: the traversal part of lrt_scene.cuh (everything before the hit-record and
+# emitter code), its other headers and its own function in lrt_api.cu
+EXTEND_SOURCES = ["lrt_scene.cuh@// The hit record of a finished closest-hit traversal", "lrt_math.cuh", "lrt_types.h",
                   "lrt_api.cu:__global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(",
                   "lrt_api.cu:constexpr int kRefillLanes"]
 
