@@ -659,9 +659,11 @@ __global__ void __launch_bounds__(kBlock) k_shade_adj(WaveArgs a, int depth) {
 }
 
 // The forward kernels of misses, hits without a BSDF and the diffuse material are held to 80 registers
-// (6 resident blocks per SM instead of 4, no spills): the diffuse walls are most of the shading.
+// (6 resident blocks per SM, no spills): the diffuse walls are most of the shading. The others keep 4
+// blocks per SM (128 registers); with no floor the material kernels grew to 162-172 registers and the
+// adjoint's shading slowed by 14%.
 template <int kKey, bool kAdj = false>
-__global__ void __launch_bounds__(kBlock, (!kAdj && kKey >= 0 && kKey <= 2) ? 6 : 1) k_shade_key(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(kBlock, (!kAdj && kKey >= 0 && kKey <= 2) ? 6 : 4) k_shade_key(WaveArgs a, int depth) {
     shade_wave<kAdj, kKey>(a, depth, nullptr);
 }
 
