@@ -324,7 +324,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(WaveArgs a, int
     }
 }
 
-// hit records of the raw results, in queue order (coherent), and the material-type shading queues
+// the material-type shading queues of the raw results, in queue order; each shading kernel computes the
+// full hit record of its own hits (hit_p / hit_n keep the raw result: t, u, v, object; leaf reference)
 __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
     const uint32_t* queue = (depth & 1) ? a.q1 : a.q0;
     BounceCounters& bc = a.counters[depth];
@@ -336,15 +337,8 @@ __global__ void __launch_bounds__(kBlock) k_hitrec(WaveArgs a, int depth) {
         const int32_t best = __float_as_int(raw.w);
         int key = 0;
         if(best >= 0) {
-            const float4 o = a.o[pid];
-            const float4 d = a.d[pid];
-            const MeshHit mh{raw.x, raw.y, raw.z, __float_as_uint(a.hit_n[pid].x)};
-            HitInfo h;
-            hit_record_of(a.s, Ray{f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}}, best, raw.x, mh, h);
             const int32_t mat = effective_material(a, pid, best);
             key = mat < 0 ? 1 : 2 + a.s.materials[mat].type;
-            a.hit_p[pid] = make_float4(h.p.x, h.p.y, h.p.z, __int_as_float(h.object));
-            a.hit_n[pid] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.front_face ? 1.0f : 0.0f);
         }
         const uint32_t slot = warp_append_keyed(bc.key_count, key);
         a.keyed[static_cast<size_t>(key) * a.capacity + slot] = pid;
@@ -498,11 +492,15 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
             a.L[pid] = make_float4(result.x, result.y, result.z, 0.0f);
             continue;
         }
-        const float4 hp = a.hit_p[pid], hn = a.hit_n[pid];
-        const f3 p{hp.x, hp.y, hp.z};
-        const f3 normal{hn.x, hn.y, hn.z};
-        const bool front_face = hn.w != 0.0f;
-        const ObjRec& obj = s.objects[__float_as_int(hp.w)];
+        // the hit record of the raw closest hit (hittable_list::hit's record)
+        const float4 raw = a.hit_p[pid];
+        HitInfo hrec;
+        hit_record_of(s, Ray{ro, rd}, __float_as_int(raw.w), raw.x,
+                      MeshHit{raw.x, raw.y, raw.z, __float_as_uint(a.hit_n[pid].x)}, hrec);
+        const f3 p = hrec.p;
+        const f3 normal = hrec.normal;
+        const bool front_face = hrec.front_face;
+        const ObjRec& obj = s.objects[hrec.object];
         if(obj.emitter >= 0 && front_face) {  // path_integrator.h:47-59
             const f3 outgoing = -normalize(rd);
             const f3 Le = area_emitted(s.emitters[obj.emitter], normal, outgoing);
@@ -521,7 +519,7 @@ __device__ __forceinline__ void shade_wave(const WaveArgs& a, int depth, uint32_
             continue;
         }
         ++shading;
-        const int32_t mid = effective_material(a, pid, __float_as_int(hp.w));
+        const int32_t mid = effective_material(a, pid, hrec.object);
         const Onb basis = onb_from_normal(normal);
         BRec rec{};
         rec.wi = to_local(basis, -normalize(rd));
