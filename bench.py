@@ -625,7 +625,7 @@ def measure_photon_mapper(gpu, oracle, args, spp=4, knn_steps=10):
         pp, shots = ctx.photon_preprocess(PHOTONS, PHOTONS, max_depth=128, rr_depth=5, lookup_size=KNN_K)
         gpu.sync()
         t_pre = time.perf_counter() - t0
-        ctx.render_photon_dev(scenes.render_params(64, 64, 1, DEPTH, RR), pp, out.data_ptr())  # warm
+        ctx.render_photon_dev(params, pp, out.data_ptr())  # warm: the eye pass's slots sized for this image
         gpu.flush()
         gpu.sync()
         ctx.reset_stats()

@@ -501,6 +501,7 @@ int lrt_render_stats_reset(lrt_context* ctx);
 /* options: "stage_timing", "count_work" (0/1), "wave_capacity" (paths per wave, 1024..2^26;
  * 0, the default: 2^24 for forward renders, 2^21 for adjoint renders; a wave never holds more paths than
  * its call renders),
+ * "photon_eye_slot_mb" (8192: device memory for the wavefront eye pass's sample slots, up to 2^20 slots),
  * "photon_eye_sort" (1, the default: the wavefront eye pass shades its slots grouped by the material type of
  * the surface each walk resumes on; 0: in slot order -- same images),
  * "photon_eye_tail" (65536: once every sample of a wavefront eye pass has started and at most this many

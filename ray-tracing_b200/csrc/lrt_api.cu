@@ -1818,6 +1818,8 @@ int lrt_set_option(lrt_context* ctx, const char* name, int64_t value) {
         ctx->pixel_tile = static_cast<uint32_t>(value);
     } else if(strcmp(name, "photon_tree_device") == 0) {
         ctx->photon_tree_device = value != 0;
+    } else if(strcmp(name, "photon_eye_slot_mb") == 0) {
+        ctx->photon_eye_slot_mb = static_cast<uint64_t>(std::max<int64_t>(16, std::min<int64_t>(value, 1ll << 20)));
     } else if(strcmp(name, "photon_eye_sort") == 0) {
         ctx->photon_eye_sort = value != 0;
     } else if(strcmp(name, "photon_eye_tail") == 0) {

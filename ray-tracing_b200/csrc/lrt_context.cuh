@@ -126,6 +126,7 @@ struct lrt_context {
     std::vector<cudaEvent_t> events;
     std::vector<int> event_stage;
     // photons
+    uint64_t photon_eye_slot_mb = 8192;  // device memory for the wavefront eye pass's slots (frames, queries)
     bool photon_eye_sort = true;  // the wavefront eye pass shades slots grouped by the surface's material type
     uint32_t photon_eye_tail = 65536;  // queued queries below which the eye pass finishes its walks in place
     bool knn_shared_heap = true;  // photon lookups keep their k-NN heaps in shared memory (false: local memory)

@@ -1813,7 +1813,14 @@ int photon_render_impl(lrt_context* ctx, const lrt_render_params* p, const lrt_p
     const int frame_limit = pp->max_depth;
     const uint64_t slot_bytes = sizeof(EyeSlot) + sizeof(EyeFrame) * static_cast<uint64_t>(frame_limit) +
                                 (sizeof(EyeQuery) + 4) * kEyeBatch;
-    const uint32_t n_slots = static_cast<uint32_t>(std::min<uint64_t>(1u << 20, (2ull << 30) / slot_bytes));
+    // up to 2^20 slots within a budget of the option photon_eye_slot_mb (8 GB by default): with the
+    // reference's 128-deep walks a slot holds ~11 KB of frames, and more slots in flight mean fewer
+    // rounds for the same samples
+    // rounds for the same samples; never more slots than the render has samples
+    const uint64_t slot_budget = static_cast<uint64_t>(ctx->photon_eye_slot_mb) << 20;
+    const uint64_t render_samples = static_cast<uint64_t>(row_end - row_begin) * p->width * p->spp;
+    const uint32_t n_slots = static_cast<uint32_t>(std::max<uint64_t>(
+        1, std::min<uint64_t>(render_samples, std::max<uint64_t>(1024, std::min<uint64_t>(1u << 20, slot_budget / slot_bytes)))));
     EyeWave w{};
     if(mode == 2) {
         LRT_CUDA(ctx, ctx->eye_slots.ensure(sizeof(EyeSlot) * n_slots));
