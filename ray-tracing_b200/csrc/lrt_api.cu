@@ -273,13 +273,14 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs a) {
 
 // ---- persistent traversal: every lane keeps a ray and idle lanes take new ones from the queue inside
 // the traversal loop (ray replacement), so a warp's lanes stay busy while its rays need very different
-// numbers of nodes: occlusion rays are fetched as soon as a lane is idle, closest-hit rays once half the
-// warp is (a fetch per finished ray cost more than the idle lanes). The per-ray work is the state
-// machine of trav_step.
+// numbers of nodes: occlusion rays are fetched as soon as a lane is idle, closest-hit rays once three
+// quarters of the warp are (a fetch, one atomic and the new rays' loads, stalls the warp's busy lanes
+// too: on the seven-material step's extension rays 12 idle lanes gave 210 ms, 16 205 ms, 20 201 ms,
+// 24 200 ms). The per-ray work is the state machine of trav_step.
 
 
 // closest hits of the active queue; writes the raw result (t, u, v, object) and the leaf reference
-constexpr int kRefillLanes = 16;  // idle lanes of a warp before k_extend_persistent fetches new rays
+constexpr int kRefillLanes = 24;  // idle lanes of a warp before k_extend_persistent fetches new rays
 
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock, 8) k_extend_persistent(WaveArgs a, int depth) {
