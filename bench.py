@@ -118,6 +118,12 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a second or more to start: wait (at most 10 s) for its first sample, so that the
+        # samples cover the whole timed region that follows
+        deadline = time.monotonic() + 10.0
+        while time.monotonic() < deadline and self.proc.poll() is None and os.path.getsize(self.file.name) == 0:
+            time.sleep(0.05)
         return self
 
     def stop(self):
